@@ -1,0 +1,143 @@
+/*
+ * pacman_b200 -- C ABI of the B200 (sm_100a) RBF-PUM transfer.
+ *
+ * Drop-in engine for PACMAN's RBF-PUM path (messahelramzi/pacman).  Plain C
+ * types only: no C++, CUDA or torch types cross this boundary, no exception
+ * crosses it, every entry point returns 0 or a negative PACMAN_B200_ERR_*
+ * code, and pacman_b200_last_error() gives the calling thread's message
+ * (the convention of the reference's C shim, src/fortran_interface.cpp:84-90).
+ *
+ * Pointers may be host memory or CUDA device memory of the selected device;
+ * each one is classified with cudaPointerGetAttributes.  Points are row-major
+ * [count x dim] doubles, values are row-major [n_source x n_fields] doubles,
+ * outputs are row-major [n_target x n_fields] doubles.  Inputs are never
+ * modified.  Targets outside every patch receive 0 (the reference zero-fills,
+ * src/common/transfer.hxx:101-110).
+ */
+#ifndef PACMAN_B200_H
+#define PACMAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PACMAN_B200_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PACMAN_B200_API __attribute__((visibility("default")))
+#else
+#define PACMAN_B200_API
+#endif
+
+/* Error codes. */
+#define PACMAN_B200_OK 0
+#define PACMAN_B200_ERR_INVALID (-1)    /* bad argument (std::invalid_argument in the reference) */
+#define PACMAN_B200_ERR_DIMENSION (-2)  /* dim not in {1,2,3} (std::runtime_error in the reference) */
+#define PACMAN_B200_ERR_CUDA (-3)       /* CUDA runtime error or no usable device */
+#define PACMAN_B200_ERR_NOMEM (-4)      /* device allocation failed */
+#define PACMAN_B200_ERR_DEGENERATE (-5) /* zero or non-finite patch radius */
+#define PACMAN_B200_ERR_LIMIT (-6)      /* a documented size limit was exceeded */
+
+/* Basis selector bytes, identical to PACMAN::RbfFunctions (src/interface.hpp:25-31). */
+#define PACMAN_B200_WENDLAND_C0 0x10
+#define PACMAN_B200_WENDLAND_C2 0x11
+#define PACMAN_B200_WENDLAND_C4 0x12
+#define PACMAN_B200_WENDLAND_C6 0x13
+#define PACMAN_B200_WENDLAND_C8 0x14
+
+/* Execution-space selector bytes of PACMAN::ExecSpaces
+ * (src/common/execspaces.hpp:17-24).  All of them select the B200 path. */
+#define PACMAN_B200_EXEC_SERIAL 0x00
+#define PACMAN_B200_EXEC_OPENMP 0x01
+#define PACMAN_B200_EXEC_THREADS 0x02
+#define PACMAN_B200_EXEC_CUDA 0x03
+#define PACMAN_B200_EXEC_HIP 0x04
+#define PACMAN_B200_EXEC_SYCL 0x05
+
+/* Precision of the per-patch solves. */
+#define PACMAN_B200_FP64 0  /* the reference algorithm: unpivoted LU in FP64 */
+#define PACMAN_B200_MIXED 1 /* FP32 factor + FP64 refinement where the patch is
+                               well conditioned, FP64 Cholesky elsewhere */
+
+typedef struct pacman_b200_options {
+  int32_t nodes_per_cluster; /* 50: RbfPumInterpolator default, src/rbf_pum/interpolator.hxx:39 */
+  double relative_overlap;   /* 0.15: interpolator.hxx:40 */
+  double support_radius;     /* 0.1: interpolator.hxx:41 (absolute basis support) */
+  int32_t precision;         /* PACMAN_B200_FP64 or PACMAN_B200_MIXED */
+  int32_t device;            /* CUDA device ordinal, -1 = the current device */
+  void *stream;              /* cudaStream_t to run on, NULL = a library-owned stream */
+} pacman_b200_options;
+
+typedef struct pacman_b200_stats {
+  double radius;            /* patch radius (clusters_radius.hpp:121-124) */
+  int64_t num_candidates;   /* candidate centres before pruning */
+  int64_t num_patches;      /* K, surviving centres */
+  int64_t sum_n, sum_m;     /* total patch sources / targets */
+  int64_t max_n;            /* largest patch */
+  int64_t patches_fp32;     /* patches solved by FP32 factor + FP64 refinement */
+  int64_t patches_fp64;     /* patches solved by an FP64 factorisation */
+  int64_t patches_fallback; /* FP32 attempts that fell back to FP64 */
+  int64_t dropped_axis_patches; /* patches whose linear polynomial lost an axis */
+  double ms_geometry;       /* device time of radius + centres + membership */
+  double ms_solve;          /* device time of the patch solves */
+  double ms_total;          /* device time of the whole call */
+  int64_t kernel_launches;  /* this library's kernel launches in the call */
+  double ms_factor;         /* device time of the dense factorisations */
+  double factor_flops;      /* algorithmic FLOPs of those factorisations */
+} pacman_b200_stats;
+
+/* Fills the reference's defaults (50, 0.15, 0.1, FP64, current device). */
+PACMAN_B200_API void pacman_b200_options_init(pacman_b200_options *opts);
+
+/*
+ * One RBF-PUM transfer, the engine behind PACMAN::rbf_interpolate
+ * (replaces src/rbf_interface.cpp:101-130 -> RbfPumInterpolator,
+ * src/rbf_pum/interpolator.hpp:58-94) for n_fields fields at once.
+ * opts may be NULL (defaults); stats may be NULL.
+ */
+PACMAN_B200_API int pacman_b200_rbf_interpolate(int32_t dim, int32_t rbf_function,
+                                 const double *source_points, int64_t n_source,
+                                 const double *source_values, int32_t n_fields,
+                                 const double *target_points, int64_t n_target,
+                                 double *target_values,
+                                 const pacman_b200_options *opts,
+                                 pacman_b200_stats *stats);
+
+/* Reusable transfer plan: the geometry (patch radius, centre cover, patch
+ * membership lists; src/rbf_pum/interpolator.hpp:76-92 and solver.hpp:45-66)
+ * is built once and each execute solves for new source values.  The plan
+ * copies the points to the device; the caller may free them afterwards. */
+typedef struct pacman_b200_plan pacman_b200_plan;
+
+PACMAN_B200_API int pacman_b200_plan_create(int32_t dim, const double *source_points, int64_t n_source,
+                            const double *target_points, int64_t n_target,
+                            const pacman_b200_options *opts, pacman_b200_plan **plan);
+PACMAN_B200_API int pacman_b200_plan_execute(pacman_b200_plan *plan, int32_t rbf_function,
+                             const double *source_values, int32_t n_fields,
+                             double *target_values, pacman_b200_stats *stats);
+PACMAN_B200_API void pacman_b200_plan_destroy(pacman_b200_plan *plan);
+
+/* Geometry of a plan, for inspection and parity tests.
+ * info[0] = K, info[1] = candidates, info[2] = total source memberships,
+ * info[3] = total target memberships; *radius = patch radius. */
+PACMAN_B200_API int pacman_b200_plan_info(const pacman_b200_plan *plan, double *radius, int64_t info[4]);
+/* Patch centres, K x dim row-major (host or device buffer). */
+PACMAN_B200_API int pacman_b200_plan_centers(const pacman_b200_plan *plan, double *centers);
+/* Membership lists in CSR form (ascending point ids within a patch):
+ * which = 0 sources, 1 targets; offsets has K+1 entries. */
+PACMAN_B200_API int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, int32_t which,
+                                 int64_t *offsets, int32_t *indices);
+/* Per (patch, target) local interpolant values of the last execute, in the
+ * order of the target membership lists, times n_fields. */
+PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local);
+
+/* Message of the last error on the calling thread ("" if none). */
+PACMAN_B200_API const char *pacman_b200_last_error(void);
+PACMAN_B200_API int32_t pacman_b200_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PACMAN_B200_H */

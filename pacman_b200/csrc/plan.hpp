@@ -1,0 +1,109 @@
+// Internal host-side state of one RBF-PUM transfer on one GPU.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pacman_b200.h"
+#include "common.cuh"
+
+namespace pacman_b200 {
+
+// Error carried from the kernels' host wrappers to the C ABI.
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define PB_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      throw ::pacman_b200::Error{PACMAN_B200_ERR_CUDA,                         \
+                                 std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+// Stream-ordered device allocation owned by a plan.
+struct DevMem {
+  void *p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t s = nullptr;
+  DevMem() = default;
+  DevMem(const DevMem &) = delete;
+  DevMem &operator=(const DevMem &) = delete;
+  ~DevMem() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t nbytes, cudaStream_t stream) {
+    if (nbytes <= bytes && p) return;
+    release();
+    s = stream;
+    if (nbytes == 0) nbytes = 16;
+    cudaError_t e = cudaMallocAsync(&p, nbytes, stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      throw Error{PACMAN_B200_ERR_NOMEM,
+                  "device allocation of " + std::to_string(nbytes) + " bytes failed"};
+    }
+    bytes = nbytes;
+  }
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+struct DevGrid {
+  GridView view{};
+  DevMem start, items;
+};
+
+struct Plan {
+  int dim = 3;
+  int64_t n = 0, m = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  pacman_b200_options opts{};
+
+  DevMem src4, tgt4;  // double4 AoS, zero padded
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  double radius = 0.0;
+  int64_t ncand = 0;
+  int K = 0;
+  DevMem centers;  // double4[K]
+  DevMem soff, sidx, toff, tidx;  // int64 offsets, int32 ids
+  int64_t snnz = 0, tnnz = 0;
+  std::vector<int> n_host, m_host;  // per patch sizes
+  DevGrid cgrid;                    // grid of centres (weights)
+  DevMem scratch;                   // solver workspace
+  DevMem local;                     // per (patch, target) local values
+  DevMem status;                    // per patch status words
+  double ms_geometry = 0.0;
+  int64_t dropped_axis_patches = 0;
+  int64_t launches_geometry = 0;  // kernel launches of the geometry phase
+  int64_t launches = 0;           // kernel launches of the current execute
+};
+
+// Launch counter of this library's own kernels on the calling thread.
+int64_t &launch_counter();
+inline void note_launch(int k = 1) { launch_counter() += k; }
+
+// geometry.cu
+void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev);
+void pu_gather(Plan &p, const double *local, int F, double *out_dev);
+
+// solve.cu
+struct SolveReport {
+  int64_t patches_fp32 = 0, patches_fp64 = 0, patches_fallback = 0, dropped = 0;
+  double ms_factor = 0.0;     // device time of the factorisation launches
+  double factor_flops = 0.0;  // their algorithmic FLOPs
+};
+void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
+                   double *local_dev, SolveReport &rep);
+
+}  // namespace pacman_b200

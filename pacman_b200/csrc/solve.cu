@@ -1,0 +1,593 @@
+// Per-patch solves of the B200 RBF-PUM transfer
+// (src/rbf_pum/solver/solver.hpp:180-286 and solver/utils/*.hpp).
+//
+// One CTA per patch.  The patch's points, the Wendland matrix A (with the
+// right-hand sides as extra columns) and all reductions live in shared
+// memory when they fit; larger patches use a global workspace (the same code
+// with a different base pointer) or the blocked engine of blocked.cu.
+//
+// Modes:
+//   kLU    the reference algorithm: unpivoted Doolittle LU (KokkosBatched
+//          SerialLU<Unblocked>, serial_solve.hpp:76-84) in FP64;
+//   kChol  FP64 Cholesky of the symmetric positive definite A (half the flops),
+//          with a per-patch breakdown flag that sends the patch back to kLU.
+//
+// The polynomial block (serial_ops.hpp:108-139, serial_solve.hpp:46-67) is
+// solved from one reduction pass: the Gram matrix of the patch-centred
+// monomials [1, x - c] gives the least-squares fit and, through its Cholesky
+// factor times the change of basis back to [1, x], the singular values of the
+// reference's uncentred Q for the condition test.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace pacman_b200 {
+
+enum SolveMode { kLU = 0, kChol = 1 };
+
+enum PatchStatus : int {
+  kStatusDropped = 1,     // the polynomial block lost at least one axis
+  kStatusNonFinite = 2,   // a non-finite local value
+  kStatusBreakdown = 4,   // non-positive Cholesky pivot
+};
+
+struct PatchArgs {
+  const double4 *src;
+  const double4 *tgt;
+  const double *vals;
+  const int64_t *soff;
+  const int *sidx;
+  const int64_t *toff;
+  const int *tidx;
+  const double4 *centers;
+  double *local;
+  int *status;
+  double *gA;             // global workspace (patches whose A does not fit in smem)
+  const int64_t *gAoff;   // per list entry offset into gA, or nullptr
+  double rinv;            // 1 / support radius
+  int F;
+  int dim;
+  int basis;
+};
+
+constexpr int kSolveThreads = 256;
+constexpr int kWarps = kSolveThreads / 32;
+constexpr int kMaxF = 8;
+constexpr int kRedVals = 10 + 4 * kMaxF + 6;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Singular values (descending) of a pv x pv upper-triangular-ish matrix by
+// one-sided Jacobi.
+__device__ void small_svd(double M[4][4], int pv, double *sig) {
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    bool rot = false;
+    for (int i = 0; i < pv; ++i)
+      for (int j = i + 1; j < pv; ++j) {
+        double al = 0, be = 0, ga = 0;
+        for (int r = 0; r < pv; ++r) {
+          al += M[r][i] * M[r][i];
+          be += M[r][j] * M[r][j];
+          ga += M[r][i] * M[r][j];
+        }
+        if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
+        rot = true;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int r = 0; r < pv; ++r) {
+          const double x = M[r][i], y = M[r][j];
+          M[r][i] = cs * x - sn * y;
+          M[r][j] = sn * x + cs * y;
+        }
+      }
+    if (!rot) break;
+  }
+  for (int j = 0; j < pv; ++j) {
+    double s = 0;
+    for (int r = 0; r < pv; ++r) s += M[r][j] * M[r][j];
+    sig[j] = sqrt(s);
+  }
+  for (int i = 1; i < pv; ++i) {
+    const double x = sig[i];
+    int j = i - 1;
+    while (j >= 0 && sig[j] < x) {
+      sig[j + 1] = sig[j];
+      --j;
+    }
+    sig[j + 1] = x;
+  }
+}
+
+// Cholesky of the pv x pv SPD matrix G (upper factor R, G = R^T R).
+__device__ bool small_chol(const double G[4][4], int pv, double R[4][4]) {
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) R[i][j] = 0.0;
+  for (int j = 0; j < pv; ++j) {
+    double d = G[j][j];
+    for (int k = 0; k < j; ++k) d -= R[k][j] * R[k][j];
+    if (!(d > 0.0)) return false;
+    d = sqrt(d);
+    R[j][j] = d;
+    for (int i = j + 1; i < pv; ++i) {
+      double s = G[j][i];
+      for (int k = 0; k < j; ++k) s -= R[k][j] * R[k][i];
+      R[j][i] = s / d;
+    }
+  }
+  return true;
+}
+
+// Polynomial block of one patch from the reduced moments (one thread).
+// red: [0]=n, [1..3]=sum dx, [4..9]=sum dx_a dx_b (aa,ab,ac,bb,bc,cc),
+//      [10 + 4f + c] = sum q_c b_f, [10+4F .. +6] = min x,y,z, max x,y,z.
+// Writes beta[4 x F] (uncentred basis, zero for dropped axes), act[0..2]
+// (active axis ids, -1 terminated) and returns the dropped flag.
+__device__ int poly_block(const double *red, int F, int dim, const double *shift,
+                          double *beta, int *act) {
+  double G[4][4];
+  G[0][0] = red[0];
+  G[0][1] = G[1][0] = red[1];
+  G[0][2] = G[2][0] = red[2];
+  G[0][3] = G[3][0] = red[3];
+  G[1][1] = red[4];
+  G[1][2] = G[2][1] = red[5];
+  G[1][3] = G[3][1] = red[6];
+  G[2][2] = red[7];
+  G[2][3] = G[3][2] = red[8];
+  G[3][3] = red[9];
+  const double *mn = red + 10 + 4 * F;
+  const double *mx = mn + 3;
+  bool active[3] = {dim > 0, dim > 1, dim > 2};
+  int pv = dim + 1;
+  int dropped = 0;
+  const double n = red[0];
+  int S[4];
+  double R[4][4];
+  bool have_R = false;
+  for (;;) {
+    int c = 0;
+    S[c++] = 0;
+    for (int a = 0; a < dim; ++a)
+      if (active[a]) S[c++] = a + 1;
+    if (pv <= 1) {
+      have_R = false;
+      break;
+    }
+    double Gs[4][4];
+    for (int i = 0; i < pv; ++i)
+      for (int j = 0; j < pv; ++j) Gs[i][j] = G[S[i]][S[j]];
+    double cond = INFINITY;
+    if (n >= double(pv) && small_chol(Gs, pv, R)) {
+      double M[4][4];
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) M[i][j] = 0.0;
+      for (int i = 0; i < pv; ++i) {
+        M[i][0] = R[i][0];
+        for (int j = 1; j < pv; ++j) M[i][j] = R[i][j] + R[i][0] * shift[S[j] - 1];
+      }
+      double sig[4];
+      small_svd(M, pv, sig);
+      cond = sig[0] / fmax(sig[pv - 1], kEps);
+      have_R = true;
+    } else {
+      have_R = false;
+    }
+    if (!(cond > kCondMax)) break;
+    // SerialDeactivateOneAxis (serial_ops.hpp:28-57).
+    double best = 1.7976931348623157e308;
+    int bi = 0;
+    for (int a = 0; a < dim; ++a) {
+      const double rg = active[a] ? fabs(mx[a] - mn[a]) : 1.7976931348623157e308;
+      if (rg < best) {
+        best = rg;
+        bi = a;
+      }
+    }
+    active[bi] = false;
+    --pv;
+    dropped = 1;
+  }
+  if (!have_R) {
+    double Gs[4][4];
+    for (int i = 0; i < pv; ++i)
+      for (int j = 0; j < pv; ++j) Gs[i][j] = G[S[i]][S[j]];
+    small_chol(Gs, pv, R);
+  }
+  int na = 0;
+  for (int a = 0; a < dim; ++a)
+    if (active[a]) act[na++] = a;
+  for (int a = na; a < 3; ++a) act[a] = -1;
+  for (int f = 0; f < F; ++f) {
+    const double *h = red + 10 + 4 * f;
+    double z[4], bp[4];
+    // R^T z = h_S, R bp = z.
+    for (int i = 0; i < pv; ++i) {
+      double s = h[S[i]];
+      for (int k = 0; k < i; ++k) s -= R[k][i] * z[k];
+      z[i] = s / R[i][i];
+    }
+    for (int i = pv - 1; i >= 0; --i) {
+      double s = z[i];
+      for (int k = i + 1; k < pv; ++k) s -= R[i][k] * bp[k];
+      bp[i] = s / R[i][i];
+    }
+    double b0 = bp[0];
+    for (int i = 1; i < pv; ++i) b0 -= shift[S[i] - 1] * bp[i];
+    beta[4 * f + 0] = b0;
+    for (int i = 1; i < pv; ++i) beta[4 * f + i] = bp[i];
+    for (int i = pv; i < 4; ++i) beta[4 * f + i] = 0.0;
+  }
+  return dropped;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kSolveThreads)
+    k_patch_solve(PatchArgs a, const int *__restrict__ plist, int np, int use_global) {
+  extern __shared__ double smem[];
+  __shared__ double red[kWarps][kRedVals];
+  __shared__ double redf[kRedVals];
+  __shared__ double beta_s[4 * kMaxF];
+  __shared__ int act_s[3];
+  __shared__ int flag_s;
+  const int e = blockIdx.x;
+  if (e >= np) return;
+  const int k = plist[e];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t s0 = a.soff[k];
+  const int n = int(a.soff[k + 1] - s0);
+  const int64_t t0 = a.toff[k];
+  const int m = int(a.toff[k + 1] - t0);
+  const int F = a.F;
+  const int lda = n + F;
+  double *xs = smem;
+  double *ys = xs + n;
+  double *zs = ys + n;
+  double *A = use_global ? (a.gA + a.gAoff[e]) : (zs + n);
+  if (tid == 0) flag_s = 0;
+
+  // Gather the patch (TeamFillB, team_ops.hpp:113-121) and its moments.
+  const double4 c = a.centers[k];
+  const double shift[3] = {c.x, c.y, c.z};
+  double acc[kRedVals];
+  const int nred = 10 + 4 * F;
+  for (int v = 0; v < nred; ++v) acc[v] = 0.0;
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int i = tid; i < n; i += kSolveThreads) {
+    const int id = a.sidx[s0 + i];
+    const double4 p = a.src[id];
+    xs[i] = p.x;
+    ys[i] = p.y;
+    zs[i] = p.z;
+    const double q[4] = {1.0, p.x - shift[0], p.y - shift[1], p.z - shift[2]};
+    acc[0] += 1.0;
+    acc[1] += q[1];
+    acc[2] += q[2];
+    acc[3] += q[3];
+    acc[4] += q[1] * q[1];
+    acc[5] += q[1] * q[2];
+    acc[6] += q[1] * q[3];
+    acc[7] += q[2] * q[2];
+    acc[8] += q[2] * q[3];
+    acc[9] += q[3] * q[3];
+    for (int f = 0; f < F; ++f) {
+      const double b = a.vals[int64_t(id) * F + f];
+      A[int64_t(i) * lda + n + f] = b;
+      for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
+    }
+    const double pc[3] = {p.x, p.y, p.z};
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = fmin(mn[d], pc[d]);
+      mx[d] = fmax(mx[d], pc[d]);
+    }
+  }
+  for (int v = 0; v < nred; ++v) {
+    const double s = warp_sum(acc[v]);
+    if (lane == 0) red[warp][v] = s;
+  }
+  for (int d = 0; d < 3; ++d) {
+    double lo = mn[d], hi = mx[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+      red[warp][nred + d] = lo;
+      red[warp][nred + 3 + d] = hi;
+    }
+  }
+  __syncthreads();
+  if (tid < nred + 6) {
+    double s;
+    if (tid < nred) {
+      s = 0.0;
+      for (int w = 0; w < kWarps; ++w) s += red[w][tid];
+    } else if (tid < nred + 3) {
+      s = INFINITY;
+      for (int w = 0; w < kWarps; ++w) s = fmin(s, red[w][tid]);
+    } else {
+      s = -INFINITY;
+      for (int w = 0; w < kWarps; ++w) s = fmax(s, red[w][tid]);
+    }
+    redf[tid] = s;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int act[3];
+    const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
+    for (int d = 0; d < 3; ++d) act_s[d] = act[d];
+    flag_s = dropped ? kStatusDropped : 0;
+  }
+  __syncthreads();
+
+  // Residual r = b - Q beta (serial_ops.hpp:149-185, gemv + vector sub).
+  for (int i = tid; i < n; i += kSolveThreads) {
+    const double pc[3] = {xs[i], ys[i], zs[i]};
+    for (int f = 0; f < F; ++f) {
+      double t = beta_s[4 * f];
+      for (int j = 0; j < 3; ++j)
+        if (act_s[j] >= 0) t = __fma_rn(pc[act_s[j]], beta_s[4 * f + 1 + j], t);
+      A[int64_t(i) * lda + n + f] -= t;
+    }
+  }
+  // A_ij = phi(|x_i - x_j|) (TeamFillA, team_ops.hpp:35-52): warp per row,
+  // upper triangle evaluated once and mirrored.
+  for (int i = warp; i < n; i += kWarps) {
+    const double xi = xs[i], yi = ys[i], zi = zs[i];
+    for (int j = i + lane; j < n; j += 32) {
+      const double d = __dsqrt_rn(sqdist3(xi, yi, zi, xs[j], ys[j], zs[j]));
+      const double v = wendland<double>(a.basis, d, a.rinv);
+      A[int64_t(i) * lda + j] = v;
+      A[int64_t(j) * lda + i] = v;
+    }
+  }
+  __syncthreads();
+
+  // Factorisation with the right-hand sides as extra columns (the forward
+  // substitution happens inside the elimination).
+  if (MODE == kLU) {
+    for (int p = 0; p < n; ++p) {
+      const double piv = A[int64_t(p) * lda + p];
+      for (int i = p + 1 + warp; i < n; i += kWarps) {
+        double l = 0.0;
+        if (lane == 0) {
+          l = A[int64_t(i) * lda + p] / piv;
+          A[int64_t(i) * lda + p] = l;
+        }
+        l = __shfl_sync(0xffffffffu, l, 0);
+        double *ri = A + int64_t(i) * lda;
+        const double *rp = A + int64_t(p) * lda;
+        for (int j = p + 1 + lane; j < lda; j += 32) ri[j] = __fma_rn(-l, rp[j], ri[j]);
+      }
+      __syncthreads();
+    }
+  } else {
+    double *lcol = xs;  // reuse after the assembly: xs is no longer needed here
+    __shared__ double piv_s;
+    (void)lcol;
+    for (int p = 0; p < n; ++p) {
+      if (tid == 0) {
+        const double app = A[int64_t(p) * lda + p];
+        if (!(app > 0.0)) flag_s |= kStatusBreakdown;
+        piv_s = sqrt(app);
+      }
+      __syncthreads();
+      const double d = piv_s;
+      for (int i = p + tid; i < n; i += kSolveThreads) {
+        double *ai = A + int64_t(i) * lda + p;
+        *ai = (i == p) ? d : (*ai / d);
+      }
+      if (tid < F) A[int64_t(p) * lda + n + tid] /= d;
+      __syncthreads();
+      for (int i = p + 1 + warp; i < n; i += kWarps) {
+        double *ri = A + int64_t(i) * lda;
+        const double li = ri[p];
+        for (int j = p + 1 + lane; j <= i; j += 32)
+          ri[j] = __fma_rn(-li, A[int64_t(j) * lda + p], ri[j]);
+        if (lane < F) ri[n + lane] = __fma_rn(-li, A[int64_t(p) * lda + n + lane], ri[n + lane]);
+      }
+      __syncthreads();
+    }
+  }
+  // Back substitution, one warp per field: U alpha = y (LU) or L^T alpha = y.
+  if (warp < F) {
+    const int f = warp;
+    for (int p = n - 1; p >= 0; --p) {
+      double xp = 0.0;
+      if (lane == 0) {
+        xp = A[int64_t(p) * lda + n + f] / A[int64_t(p) * lda + p];
+        A[int64_t(p) * lda + n + f] = xp;
+      }
+      xp = __shfl_sync(0xffffffffu, xp, 0);
+      for (int i = lane; i < p; i += 32) {
+        const double u = (MODE == kLU) ? A[int64_t(i) * lda + p] : A[int64_t(p) * lda + i];
+        A[int64_t(i) * lda + n + f] = __fma_rn(-u, xp, A[int64_t(i) * lda + n + f]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+
+  // local = E alpha + V beta (solver.hpp:270-273), warp per target.
+  int nonfinite = 0;
+  for (int i = warp; i < m; i += kWarps) {
+    const double4 y = a.tgt[a.tidx[t0 + i]];
+    double s[kMaxF];
+    for (int f = 0; f < F; ++f) s[f] = 0.0;
+    for (int j = lane; j < n; j += 32) {
+      const double d = __dsqrt_rn(sqdist3(y.x, y.y, y.z, xs[j], ys[j], zs[j]));
+      const double ph = wendland<double>(a.basis, d, a.rinv);
+      for (int f = 0; f < F; ++f) s[f] = __fma_rn(ph, A[int64_t(j) * lda + n + f], s[f]);
+    }
+    for (int f = 0; f < F; ++f) s[f] = warp_sum(s[f]);
+    if (lane == 0) {
+      const double yc[3] = {y.x, y.y, y.z};
+      for (int f = 0; f < F; ++f) {
+        double v = beta_s[4 * f];
+        for (int j = 0; j < 3; ++j)
+          if (act_s[j] >= 0) v = __fma_rn(yc[act_s[j]], beta_s[4 * f + 1 + j], v);
+        const double out = s[f] + v;
+        if (!isfinite(out)) nonfinite = 1;
+        a.local[(t0 + i) * F + f] = out;
+      }
+    }
+  }
+  if (nonfinite) atomicOr(&flag_s, kStatusNonFinite);
+  __syncthreads();
+  if (tid == 0) a.status[k] = flag_s;
+}
+
+// Shared memory of one patch: 3n coordinates + n x (n + F) matrix.
+static size_t smem_bytes(int n, int F, bool with_A) {
+  size_t d = size_t(3) * n;
+  if (with_A) d += size_t(n) * size_t(n + F);
+  return d * sizeof(double);
+}
+
+static void launch(int mode, const PatchArgs &a, const int *plist, int np, int use_global,
+                   size_t smem, cudaStream_t st) {
+  if (np == 0) return;
+  if (mode == kLU) {
+    PB_CUDA(cudaFuncSetAttribute(k_patch_solve<kLU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem)));
+    k_patch_solve<kLU><<<np, kSolveThreads, smem, st>>>(a, plist, np, use_global);
+    note_launch();
+  } else {
+    PB_CUDA(cudaFuncSetAttribute(k_patch_solve<kChol>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_patch_solve<kChol><<<np, kSolveThreads, smem, st>>>(a, plist, np, use_global);
+    note_launch();
+  }
+  PB_CUDA(cudaGetLastError());
+}
+
+// Runs one mode over a list of patches: buckets by size so the dynamic
+// shared memory follows the bucket's largest patch; patches too large for
+// shared memory use the global workspace.
+static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &patches,
+                     SolveReport &rep) {
+  cudaStream_t st = p.stream;
+  for (int k : patches) {
+    const double n = p.n_host[k], m = p.m_host[k];
+    rep.factor_flops += (mode == kLU ? 2.0 / 3.0 : 1.0 / 3.0) * n * n * n +
+                        2.0 * n * n * a.F + 2.0 * m * n * a.F;
+  }
+  cudaEvent_t ev0, ev1;
+  PB_CUDA(cudaEventCreate(&ev0));
+  PB_CUDA(cudaEventCreate(&ev1));
+  const int F = a.F;
+  const size_t smem_cap = 200 * 1024;
+  std::vector<int> order(patches);
+  std::sort(order.begin(), order.end(),
+            [&](int x, int y) { return p.n_host[x] < p.n_host[y]; });
+  std::vector<int> small, big;
+  for (int k : order) {
+    if (smem_bytes(p.n_host[k], F, true) <= smem_cap) small.push_back(k);
+    else big.push_back(k);
+  }
+  DevMem list;
+  list.alloc(sizeof(int) * std::max<size_t>(order.size(), 1), st);
+  std::vector<int> host_list;
+  host_list.reserve(order.size());
+  // Small: buckets of doubling size.
+  size_t pos = 0;
+  std::vector<std::pair<size_t, size_t>> ranges;
+  while (pos < small.size()) {
+    const int n0 = p.n_host[small[pos]];
+    int cap = 32;
+    while (cap < n0) cap *= 2;
+    size_t end = pos;
+    while (end < small.size() && p.n_host[small[end]] <= cap &&
+           smem_bytes(p.n_host[small[end]], F, true) <= smem_cap)
+      ++end;
+    ranges.emplace_back(pos, end);
+    pos = end;
+  }
+  for (int k : small) host_list.push_back(k);
+  for (int k : big) host_list.push_back(k);
+  if (!host_list.empty())
+    PB_CUDA(cudaMemcpyAsync(list.p, host_list.data(), sizeof(int) * host_list.size(),
+                            cudaMemcpyHostToDevice, st));
+  PB_CUDA(cudaEventRecord(ev0, st));
+  for (auto &r : ranges) {
+    int nmax = 0;
+    for (size_t i = r.first; i < r.second; ++i) nmax = std::max(nmax, p.n_host[small[i]]);
+    launch(mode, a, list.as<int>() + r.first, int(r.second - r.first), 0,
+           smem_bytes(nmax, F, true), st);
+  }
+  if (!big.empty()) {
+    std::vector<int64_t> offs(big.size());
+    int64_t tot = 0;
+    int nmax = 0;
+    for (size_t i = 0; i < big.size(); ++i) {
+      offs[i] = tot;
+      const int64_t n = p.n_host[big[i]];
+      tot += n * (n + F);
+      nmax = std::max<int>(nmax, int(n));
+    }
+    DevMem goff, gA;
+    goff.alloc(sizeof(int64_t) * big.size(), st);
+    gA.alloc(sizeof(double) * size_t(tot), st);
+    PB_CUDA(cudaMemcpyAsync(goff.p, offs.data(), sizeof(int64_t) * offs.size(),
+                            cudaMemcpyHostToDevice, st));
+    PatchArgs b = a;
+    b.gA = gA.as<double>();
+    b.gAoff = goff.as<int64_t>();
+    launch(mode, b, list.as<int>() + small.size(), int(big.size()), 1,
+           smem_bytes(nmax, F, false), st);
+  }
+  PB_CUDA(cudaEventRecord(ev1, st));
+  PB_CUDA(cudaEventSynchronize(ev1));
+  float ms = 0.f;
+  PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  rep.ms_factor += ms;
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+}
+
+void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
+                   double *local_dev, SolveReport &rep) {
+  cudaStream_t st = p.stream;
+  const int K = p.K;
+  if (K == 0) return;
+  p.status.alloc(sizeof(int) * K, st);
+  PatchArgs a{};
+  a.src = p.src4.as<double4>();
+  a.tgt = p.tgt4.as<double4>();
+  a.vals = vals_dev;
+  a.soff = p.soff.as<int64_t>();
+  a.sidx = p.sidx.as<int>();
+  a.toff = p.toff.as<int64_t>();
+  a.tidx = p.tidx.as<int>();
+  a.centers = p.centers.as<double4>();
+  a.local = local_dev;
+  a.status = p.status.as<int>();
+  a.rinv = 1.0 / p.opts.support_radius;
+  a.F = F;
+  a.dim = p.dim;
+  a.basis = basis;
+  std::vector<int> all(K);
+  for (int k = 0; k < K; ++k) all[k] = k;
+  const int mode = precision == PACMAN_B200_FP64 ? kLU : kChol;
+  run_list(p, a, mode, all, rep);
+  std::vector<int> stat(K);
+  PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
+  PB_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> redo;
+  for (int k = 0; k < K; ++k) {
+    if (stat[k] & kStatusDropped) rep.dropped++;
+    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite))) redo.push_back(k);
+  }
+  rep.patches_fp64 = K;
+  if (!redo.empty()) {
+    run_list(p, a, kLU, redo, rep);
+    rep.patches_fallback += int64_t(redo.size());
+  }
+}
+
+}  // namespace pacman_b200

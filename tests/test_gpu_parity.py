@@ -1,0 +1,223 @@
+"""CUDA path against the CPU oracle, through the C ABI (pacman_b200.rbf).
+
+Geometry (patch radius, centres, sorted membership lists) must be bit-exact;
+FP64 results within rel-L2 1e-12 of the oracle, mixed-precision results within
+1e-10 (the tolerances the transfer is specified to)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+import pacman_b200 as pacman
+from pacman_b200 import workloads as W
+from tests.conftest import ROOT, grid_cloud, rel_l2, slab_meshes
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+TOL_MIXED = 1e-10
+BASES = [0x10, 0x11, 0x12, 0x13, 0x14]
+CUDA = pacman.execspaces.CUDA
+
+
+def _cases():
+    rng = np.random.default_rng(3)
+    u = W.make("uniform_20k")
+    gb = W.make("grid_blobs_1m", scale=0.01)
+    return {
+        "uniform_20k_c2": (3, u["src"], u["tgt"], u["values"][:, 0], 0x11, 30),
+        "grid_blobs_10k_c4": (3, gb["src"], gb["tgt"], gb["values"][:, 0], 0x12, 50),
+        "uniform_2d": (2, rng.random((6000, 2)), rng.random((5000, 2)),
+                       np.sin(4 * rng.random(6000)), 0x13, 40),
+        "uniform_1d": (1, rng.random((3000, 1)), rng.random((2000, 1)),
+                       np.cos(rng.random(3000)), 0x10, 20),
+    }
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_geometry_bit_exact(name):
+    dim, S, T, v, basis, npc = CASES[name]
+    plan = pacman.rbf.Plan(dim, S, T, nodes_per_cluster=npc)
+    ref = oracle.build(dim, S, T, npc)
+    info = plan.info()
+    assert info["radius"] == ref.radius
+    assert info["num_candidates"] == ref.num_candidates
+    assert info["num_patches"] == ref.num_patches
+    assert np.array_equal(plan.centers(), ref.centers())
+    for which, csr in (("source", ref.src_csr()), ("target", ref.tgt_csr())):
+        off, idx = plan.patch_lists(which)
+        assert np.array_equal(off, csr[0]), which
+        assert np.array_equal(idx, csr[1]), which
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_transfer_matches_oracle(name, precision, tol):
+    dim, S, T, v, basis, npc = CASES[name]
+    out = pacman.rbf.interpolate(dim, CUDA, basis, S, v, T, nodes_per_cluster=npc,
+                                 precision=precision)
+    ref = oracle.interpolate(dim, basis, S, v, T, npc)
+    assert rel_l2(out, ref) <= tol
+
+
+@pytest.mark.parametrize("basis", BASES)
+def test_all_bases_fp64(basis):
+    u = W.make("uniform_20k", scale=0.25)
+    out = pacman.rbf.interpolate(3, CUDA, basis, u["src"], u["values"][:, 0], u["tgt"],
+                                 nodes_per_cluster=30)
+    ref = oracle.interpolate(3, basis, u["src"], u["values"][:, 0], u["tgt"], 30)
+    assert rel_l2(out, ref) <= TOL_FP64
+
+
+@pytest.mark.parametrize("basis", BASES)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_grid20_node_reproduction(basis, precision):
+    # The reference's C++ known-answer test (test_cpp_rbf_interface.cpp:165-198).
+    P = grid_cloud(20)
+    v = W.franke_3d(P)
+    out = pacman.rbf.interpolate(3, CUDA, basis, P, v, P, precision=precision)
+    assert rel_l2(out, v) < 1e-8
+
+
+@pytest.mark.parametrize("pair", [("0.03", "0.003"), ("0.003", "0.03"), ("0.03", "0.03")])
+def test_slab_meshes(pair):
+    # The reference's Python known-answer test (test_rbf-pum.py:58-74).
+    m = slab_meshes()
+    S, T = m[pair[0]], m[pair[1]]
+    for basis in BASES:
+        out = pacman.rbf.interpolate(3, CUDA, basis, S, W.franke_3d(S), T)
+        assert rel_l2(out, W.franke_3d(T)) < 1.5e-2
+        ref = oracle.interpolate(3, basis, S, W.franke_3d(S), T)
+        assert rel_l2(out, ref) <= TOL_FP64
+
+
+def test_local_values_match_oracle():
+    dim, S, T, v, basis, npc = CASES["uniform_20k_c2"]
+    plan = pacman.rbf.Plan(dim, S, T, nodes_per_cluster=npc)
+    out = plan.execute(basis, v)
+    ref = oracle.build(dim, S, T, npc)
+    rout, rloc, _ = ref.solve(basis, v, want_local=True)
+    assert rel_l2(plan.local_values()[:, 0], rloc[:, 0]) <= TOL_FP64
+    assert rel_l2(out, rout) <= TOL_FP64
+
+
+def test_multifield_and_plan_reuse():
+    sh = W.make("shell_4m", scale=0.004)
+    S, T, V = sh["src"], sh["tgt"], sh["values"]
+    plan = pacman.rbf.Plan(3, S, T)
+    multi = plan.execute(0x12, V)
+    ref = oracle.build(3, S, T, 50)
+    rmulti, _, _ = ref.solve(0x12, V)
+    assert multi.shape == (T.shape[0], 8)
+    assert rel_l2(multi, rmulti) <= TOL_FP64
+    single = plan.execute(0x12, V[:, 3])
+    assert rel_l2(single, rmulti[:, 3]) <= TOL_FP64
+    again = plan.execute(0x12, V)
+    assert np.array_equal(again, multi)
+
+
+def test_edge_cases():
+    rng = np.random.default_rng(11)
+    S = rng.random((800, 3))
+    v = W.franke_3d(S)
+    # No targets.
+    out = pacman.rbf.interpolate(3, CUDA, 0x11, S, v, np.zeros((0, 3)))
+    assert out.shape == (0,)
+    # Targets far outside every patch get 0 (zero-filled output).
+    far = rng.random((50, 3)) + 10.0
+    T = np.concatenate([rng.random((100, 3)), far])
+    out = pacman.rbf.interpolate(3, CUDA, 0x11, S, v, T)
+    assert np.all(out[100:] == 0.0)
+    ref = oracle.interpolate(3, 0x11, S, v, T)
+    assert rel_l2(out, ref) <= TOL_FP64
+    # Fewer sources than nodes per cluster.
+    S2 = rng.random((20, 3))
+    T2 = rng.random((30, 3))
+    out = pacman.rbf.interpolate(3, CUDA, 0x11, S2, W.franke_3d(S2), T2)
+    ref = oracle.interpolate(3, 0x11, S2, W.franke_3d(S2), T2)
+    assert rel_l2(out, ref) <= TOL_FP64
+    # Planar data in 3D: every patch drops an axis.
+    P = np.c_[rng.random((3000, 2)), np.full(3000, 0.25)]
+    Q = np.c_[rng.random((2000, 2)), np.full(2000, 0.25)]
+    f = np.cos(3 * P[:, 0]) * P[:, 1]
+    st = {}
+    out = pacman.rbf.interpolate(3, CUDA, 0x12, P, f, Q, stats=st)
+    ref = oracle.interpolate(3, 0x12, P, f, Q)
+    assert st["dropped_axis_patches"] == st["num_patches"]
+    assert rel_l2(out, ref) <= TOL_FP64
+    # Duplicate source points in the cloud.
+    D = np.concatenate([S, S[:100]])
+    dv = W.franke_3d(D)
+    Tt = rng.random((400, 3))
+    out = pacman.rbf.interpolate(3, CUDA, 0x11, D, dv, Tt, precision="mixed")
+    assert np.all(np.isfinite(out))
+
+
+def test_torch_device_tensors():
+    torch = pytest.importorskip("torch")
+    dim, S, T, v, basis, npc = CASES["uniform_20k_c2"]
+    dS = torch.tensor(S, device="cuda")
+    dT = torch.tensor(T, device="cuda")
+    dv = torch.tensor(v, device="cuda")
+    out = pacman.rbf.interpolate(dim, CUDA, basis, dS, dv, dT, nodes_per_cluster=npc)
+    assert out.is_cuda
+    ref = oracle.interpolate(dim, basis, S, v, T, npc)
+    assert rel_l2(out.cpu().numpy(), ref) <= TOL_FP64
+
+
+CPP_TEST = r"""
+#include <cmath>
+#include <cstdio>
+#include <stdexcept>
+#include <vector>
+#include "pacman_rbf.hpp"
+static double franke(double x, double y, double z) {
+  return 0.75 * std::exp(-((9*x-2)*(9*x-2) + (9*y-2)*(9*y-2) + (9*z-2)*(9*z-2)) / 4.0)
+       + 0.75 * std::exp(-((9*x+1)*(9*x+1)/49.0 + (9*y+1)/10.0 + (9*z+1)/10.0))
+       + 0.5 * std::exp(-((9*x-7)*(9*x-7) + (9*y-3)*(9*y-3) + (9*z-5)*(9*z-5)) / 4.0)
+       - 0.2 * std::exp(-((9*x-4)*(9*x-4) + (9*y-7)*(9*y-7) + (9*z-5)*(9*z-5)));
+}
+int main() {
+  const int N = 20;
+  std::vector<double> pts, vals;
+  for (int i = 0; i < N; ++i) for (int j = 0; j < N; ++j) for (int k = 0; k < N; ++k) {
+    double x = i / (N - 1.0), y = j / (N - 1.0), z = k / (N - 1.0);
+    pts.push_back(x); pts.push_back(y); pts.push_back(z); vals.push_back(franke(x, y, z));
+  }
+  int bad = 0;
+  for (unsigned char b = 0x10; b <= 0x14; ++b) {
+    auto r = PACMAN::rbf_interpolate(3, PACMAN::ExecSpaces::CUDA, b, pts.data(), N*N*N,
+                                     vals.data(), pts.data(), N*N*N);
+    double num = 0, den = 0;
+    for (int i = 0; i < N*N*N; ++i) { double d = r.targetValues[i] - vals[i]; num += d*d; den += vals[i]*vals[i]; }
+    double e = std::sqrt(num / den);
+    std::printf("basis 0x%x rel_l2 %.3e\n", b, e);
+    if (!(e < 1e-8)) bad = 1;
+  }
+  try { PACMAN::rbf_interpolate(4, 3, 0x11, pts.data(), 10, vals.data(), pts.data(), 10); bad = 1; }
+  catch (const std::runtime_error &) {}
+  try { PACMAN::rbf_interpolate(3, 3, 0x11, nullptr, 10, vals.data(), pts.data(), 10); bad = 1; }
+  catch (const std::invalid_argument &) {}
+  try { PACMAN::rbf_interpolate(3, 3, 0x77, pts.data(), 10, vals.data(), pts.data(), 10); bad = 1; }
+  catch (const std::invalid_argument &) {}
+  return bad;
+}
+"""
+
+
+def test_cpp_dropin(tmp_path):
+    # The reference's C++ known-answer test through PACMAN::rbf_interpolate.
+    src = tmp_path / "t.cpp"
+    src.write_text(CPP_TEST)
+    exe = tmp_path / "t"
+    libdir = os.path.join(ROOT, "pacman_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", str(src), "-I", os.path.join(ROOT, "include"),
+                    "-L", libdir, "-lpacman_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                   check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
