@@ -1,0 +1,674 @@
+// Blocked engine for large patches of the B200 RBF-PUM transfer.
+//
+// The reference solves each patch with one GPU thread running an unblocked
+// LU in global memory (src/rbf_pum/solver/solver.hpp:422-490).  Here every
+// patch above the shared-memory size gets an augmented matrix
+//
+//        [ A   r ]      A: n x n Wendland matrix (TeamFillA, team_ops.hpp:35-52)
+//        [ E   0 ]      E: m x n evaluation matrix (TeamFillE, team_ops.hpp:78-97)
+//                       r: n x F residuals b - Q beta (solver.hpp:451-468)
+//
+// stored in 64 x 64 tiles (A padded with an identity block).  Unpivoted
+// elimination of the first n columns leaves the Schur complement
+// S = -E A^{-1} r in the bottom-right block, i.e. minus the RBF part of the
+// local interpolant (solver.hpp:474-478); no triangular solves and no
+// separate evaluation pass are needed.  All large patches advance in lockstep,
+// one 64-column pivot block per step:
+//   k_diag    factor the diagonal tile (LU or Cholesky) and invert it,
+//   k_trsm    apply the inverse to the panel tiles,
+//   k_update  trailing update C -= A * op(B) of every remaining tile,
+// with the tile products on the FP64 tensor cores (mma.sync m8n8k4 f64).
+// Mode kLU is the reference's unpivoted LU; mode kChol uses the symmetry of A
+// (lower tiles only, half the work) and flags non-positive pivots.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "plan.hpp"
+#include "poly.cuh"
+
+namespace pacman_b200 {
+
+constexpr int TB = 64;   // tile size
+constexpr int LDS = 68;  // shared-memory row stride (doubles): conflict-free fragments
+
+struct BigSlot {
+  int64_t base;  // offset (doubles) of the augmented matrix in the workspace
+  int ld;        // row stride (doubles) = (T + 1) * TB
+  int T;         // pivot tiles
+  int TE;        // evaluation-row tiles
+  int k;         // patch id
+  int n, m;
+};
+
+struct Item {
+  int slot;
+  short ti, tj;
+};
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core tile product
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// acc += sign * op(A) op(B) on the 32 x 32 block (wr, wc) of a 64 x 64 tile.
+// Fragment layout of m8n8k4.f64: A (row) a0 = A[g][t], B (col) b0 = B[t][g],
+// C c_h = C[g][2t + h], with g = lane / 4, t = lane % 4.
+template <bool AT, bool BT>
+__device__ __forceinline__ void mma64(const double *__restrict__ sA, const double *__restrict__ sB,
+                                      double (&acc)[4][4][2], double sign, int wr, int wc,
+                                      int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll 2
+  for (int k0 = 0; k0 < TB; k0 += 4) {
+    const int kk = k0 + t;
+    double a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = wr + 8 * i + g;
+      a[i] = sign * (AT ? sA[kk * LDS + r] : sA[r * LDS + kk]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = wc + 8 * j + g;
+      b[j] = BT ? sB[c * LDS + kk] : sB[kk * LDS + c];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  }
+}
+
+__device__ __forceinline__ void load_tile(double *s, const double *g, int ld, int tid, int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    const double2 v = *reinterpret_cast<const double2 *>(g + int64_t(r) * ld + 2 * c2);
+    *reinterpret_cast<double2 *>(s + r * LDS + 2 * c2) = v;
+  }
+}
+
+__device__ __forceinline__ void acc_load(double (&acc)[4][4][2], const double *C, int ld, int wr,
+                                         int wc, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double2 v = *reinterpret_cast<const double2 *>(
+          C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t);
+      acc[i][j][0] = v.x;
+      acc[i][j][1] = v.y;
+    }
+}
+
+__device__ __forceinline__ void acc_store(const double (&acc)[4][4][2], double *C, int ld, int wr,
+                                          int wc, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<double2 *>(C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t) =
+          make_double2(acc[i][j][0], acc[i][j][1]);
+}
+
+__device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+struct BigArgs {
+  const double4 *src;
+  const double4 *tgt;
+  const double *vals;
+  const int64_t *soff;
+  const int *sidx;
+  const int64_t *toff;
+  const int *tidx;
+  const double4 *centers;
+  double *W;            // workspace
+  double *inv;          // per slot: 2 inverse tiles (TB x TB)
+  double *beta;         // per slot: 4 * kMaxF
+  int *act;             // per slot: 3
+  int *status;          // per patch
+  double *local;
+  double rinv;
+  int F;
+  int dim;
+  int basis;
+};
+
+// Fills one 64 x 64 tile of an augmented matrix.
+__global__ void __launch_bounds__(256)
+    k_assemble(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items) {
+  __shared__ double rx[TB], ry[TB], rz[TB], cx[TB], cy[TB], cz[TB];
+  const Item it = items[blockIdx.x];
+  const BigSlot sl = slots[it.slot];
+  const int tid = threadIdx.x;
+  double *tile = a.W + sl.base + int64_t(it.ti) * TB * sl.ld + int64_t(it.tj) * TB;
+  if (it.tj == sl.T) {  // residual columns: zero (the polynomial pass writes r)
+    for (int e = tid; e < TB * TB; e += blockDim.x) tile[int64_t(e >> 6) * sl.ld + (e & 63)] = 0.0;
+    return;
+  }
+  const bool erow = it.ti >= sl.T;
+  const int64_t s0 = a.soff[sl.k], t0 = a.toff[sl.k];
+  if (tid < TB) {
+    const int gi = (erow ? it.ti - sl.T : it.ti) * TB + tid;
+    double4 p = make_double4(0, 0, 0, 0);
+    if (erow ? gi < sl.m : gi < sl.n) p = erow ? a.tgt[a.tidx[t0 + gi]] : a.src[a.sidx[s0 + gi]];
+    rx[tid] = p.x;
+    ry[tid] = p.y;
+    rz[tid] = p.z;
+  } else if (tid < 2 * TB) {
+    const int gj = it.tj * TB + (tid - TB);
+    double4 p = make_double4(0, 0, 0, 0);
+    if (gj < sl.n) p = a.src[a.sidx[s0 + gj]];
+    cx[tid - TB] = p.x;
+    cy[tid - TB] = p.y;
+    cz[tid - TB] = p.z;
+  }
+  __syncthreads();
+  for (int e = tid; e < TB * TB; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    const int gi = it.ti * TB + r, gj = it.tj * TB + c;
+    double v;
+    if (!erow) {
+      if (gi < sl.n && gj < sl.n)
+        v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(rx[r], ry[r], rz[r], cx[c], cy[c], cz[c])),
+                             a.rinv);
+      else
+        v = (gi == gj) ? 1.0 : 0.0;
+    } else {
+      const int ie = gi - sl.T * TB;
+      v = (ie < sl.m && gj < sl.n)
+              ? wendland<double>(a.basis,
+                                 __dsqrt_rn(sqdist3(rx[r], ry[r], rz[r], cx[c], cy[c], cz[c])),
+                                 a.rinv)
+              : 0.0;
+    }
+    tile[int64_t(r) * sl.ld + c] = v;
+  }
+}
+
+// Polynomial block and residual columns of one large patch (CTA per slot).
+__global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__restrict__ slots) {
+  __shared__ double red[8][kRedVals];
+  __shared__ double redf[kRedVals];
+  __shared__ double beta_s[4 * kMaxF];
+  __shared__ int act_s[3];
+  const BigSlot sl = slots[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int F = a.F, n = sl.n;
+  const int64_t s0 = a.soff[sl.k];
+  const double4 c = a.centers[sl.k];
+  const double shift[3] = {c.x, c.y, c.z};
+  double acc[kRedVals - 6];
+#pragma unroll
+  for (int v = 0; v < kRedVals - 6; ++v) acc[v] = 0.0;
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const int nred = 10 + 4 * F;
+  for (int i = tid; i < n; i += blockDim.x) {
+    const int id = a.sidx[s0 + i];
+    const double4 p = a.src[id];
+    const double q[4] = {1.0, p.x - shift[0], p.y - shift[1], p.z - shift[2]};
+    acc[0] += 1.0;
+    acc[1] += q[1];
+    acc[2] += q[2];
+    acc[3] += q[3];
+    acc[4] += q[1] * q[1];
+    acc[5] += q[1] * q[2];
+    acc[6] += q[1] * q[3];
+    acc[7] += q[2] * q[2];
+    acc[8] += q[2] * q[3];
+    acc[9] += q[3] * q[3];
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f)
+      if (f < F) {
+        const double b = a.vals[int64_t(id) * F + f];
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
+      }
+    const double pc[3] = {p.x, p.y, p.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = fmin(mn[d], pc[d]);
+      mx[d] = fmax(mx[d], pc[d]);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < kRedVals - 6; ++v) {
+    const double s = warp_sum(acc[v]);
+    if (lane == 0 && v < nred) red[warp][v] = s;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double lo = mn[d], hi = mx[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+      red[warp][nred + d] = lo;
+      red[warp][nred + 3 + d] = hi;
+    }
+  }
+  __syncthreads();
+  if (tid < nred + 6) {
+    double s;
+    if (tid < nred) {
+      s = 0.0;
+      for (int w = 0; w < 8; ++w) s += red[w][tid];
+    } else if (tid < nred + 3) {
+      s = INFINITY;
+      for (int w = 0; w < 8; ++w) s = fmin(s, red[w][tid]);
+    } else {
+      s = -INFINITY;
+      for (int w = 0; w < 8; ++w) s = fmax(s, red[w][tid]);
+    }
+    redf[tid] = s;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int act[3];
+    const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
+    for (int d = 0; d < 3; ++d) act_s[d] = act[d];
+    a.status[sl.k] = dropped ? 1 : 0;
+    for (int v = 0; v < 4 * kMaxF; ++v) a.beta[blockIdx.x * 4 * kMaxF + v] = beta_s[v];
+    for (int d = 0; d < 3; ++d) a.act[blockIdx.x * 3 + d] = act[d];
+  }
+  __syncthreads();
+  double *rcol = a.W + sl.base + int64_t(sl.T) * TB;
+  for (int i = tid; i < n; i += blockDim.x) {
+    const int id = a.sidx[s0 + i];
+    const double4 p = a.src[id];
+    const double pc[3] = {p.x, p.y, p.z};
+    for (int f = 0; f < F; ++f) {
+      double t = beta_s[4 * f];
+      for (int j = 0; j < 3; ++j)
+        if (act_s[j] >= 0) t = __fma_rn(pc[act_s[j]], beta_s[4 * f + 1 + j], t);
+      rcol[int64_t(i) * sl.ld + f] = a.vals[int64_t(id) * F + f] - t;
+    }
+  }
+}
+
+// Factors diagonal tile (s, s) of each listed slot and writes its inverses.
+template <bool LU>
+__global__ void __launch_bounds__(256)
+    k_diag(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ list, int s) {
+  extern __shared__ double sm[];
+  double *T = sm;                 // the tile
+  double *Li = T + TB * LDS;      // inverse of L
+  double *Ui = Li + TB * LDS;     // inverse of U (LU only)
+  __shared__ double piv;
+  __shared__ int bad;
+  const int slot = list[blockIdx.x];
+  const BigSlot sl = slots[slot];
+  const int tid = threadIdx.x;
+  double *g = a.W + sl.base + int64_t(s) * TB * sl.ld + int64_t(s) * TB;
+  load_tile(T, g, sl.ld, tid, blockDim.x);
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  for (int p = 0; p < TB; ++p) {
+    if (LU) {
+      const double d = T[p * LDS + p];
+      for (int i = p + 1 + tid; i < TB; i += blockDim.x) T[i * LDS + p] /= d;
+      __syncthreads();
+      const int w = TB - 1 - p;
+      for (int e = tid; e < w * w; e += blockDim.x) {
+        const int i = p + 1 + e / w, j = p + 1 + e % w;
+        T[i * LDS + j] = __fma_rn(-T[i * LDS + p], T[p * LDS + j], T[i * LDS + j]);
+      }
+      __syncthreads();
+    } else {
+      if (tid == 0) {
+        const double app = T[p * LDS + p];
+        if (!(app > 0.0)) bad = 1;
+        piv = sqrt(app);
+      }
+      __syncthreads();
+      const double d = piv;
+      for (int i = p + tid; i < TB; i += blockDim.x) T[i * LDS + p] = (i == p) ? d : T[i * LDS + p] / d;
+      __syncthreads();
+      const int w = TB - 1 - p;
+      for (int e = tid; e < w * w; e += blockDim.x) {
+        const int i = p + 1 + e / w, j = p + 1 + e % w;
+        if (j <= i) T[i * LDS + j] = __fma_rn(-T[i * LDS + p], T[j * LDS + p], T[i * LDS + j]);
+      }
+      __syncthreads();
+    }
+  }
+  // Inverses, one column per thread (lower: forward, upper: backward).
+  if (tid < TB) {
+    const int j = tid;
+    for (int i = 0; i < j; ++i) Li[i * LDS + j] = 0.0;
+    double xj = LU ? 1.0 : 1.0 / T[j * LDS + j];
+    Li[j * LDS + j] = xj;
+    for (int i = j + 1; i < TB; ++i) {
+      double s2 = 0.0;
+      for (int k = j; k < i; ++k) s2 = __fma_rn(T[i * LDS + k], Li[k * LDS + j], s2);
+      Li[i * LDS + j] = LU ? -s2 : -s2 / T[i * LDS + i];
+    }
+    if (LU) {
+      for (int i = j + 1; i < TB; ++i) Ui[i * LDS + j] = 0.0;
+      Ui[j * LDS + j] = 1.0 / T[j * LDS + j];
+      for (int i = j - 1; i >= 0; --i) {
+        double s2 = 0.0;
+        for (int k = i + 1; k <= j; ++k) s2 = __fma_rn(T[i * LDS + k], Ui[k * LDS + j], s2);
+        Ui[i * LDS + j] = -s2 / T[i * LDS + i];
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < TB * TB / 2; idx += blockDim.x) {
+    const int r = idx >> 5, c2 = idx & 31;
+    *reinterpret_cast<double2 *>(g + int64_t(r) * sl.ld + 2 * c2) =
+        *reinterpret_cast<const double2 *>(T + r * LDS + 2 * c2);
+    double *gi = a.inv + int64_t(slot) * 2 * TB * TB;
+    *reinterpret_cast<double2 *>(gi + r * TB + 2 * c2) =
+        *reinterpret_cast<const double2 *>(Li + r * LDS + 2 * c2);
+    if (LU)
+      *reinterpret_cast<double2 *>(gi + TB * TB + r * TB + 2 * c2) =
+          *reinterpret_cast<const double2 *>(Ui + r * LDS + 2 * c2);
+  }
+  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+}
+
+__device__ __forceinline__ void load_inv(double *s, const double *g, int tid, int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    *reinterpret_cast<double2 *>(s + r * LDS + 2 * c2) =
+        *reinterpret_cast<const double2 *>(g + r * TB + 2 * c2);
+  }
+}
+
+// Panel tiles of step s: row panel X := L^{-1} X (ti == s), column panel
+// X := X U^{-1} (LU) or X := X L^{-T} (Cholesky).
+template <bool LU>
+__global__ void __launch_bounds__(128)
+    k_trsm(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items, int s) {
+  extern __shared__ double sm[];
+  double *sX = sm, *sI = sm + TB * LDS;
+  const Item it = items[blockIdx.x];
+  const BigSlot sl = slots[it.slot];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  double *X = a.W + sl.base + int64_t(it.ti) * TB * sl.ld + int64_t(it.tj) * TB;
+  const double *inv = a.inv + int64_t(it.slot) * 2 * TB * TB;
+  const bool left = it.ti == s;
+  load_tile(sX, X, sl.ld, tid, blockDim.x);
+  load_inv(sI, (left || !LU) ? inv : inv + TB * TB, tid, blockDim.x);
+  __syncthreads();
+  double acc[4][4][2];
+  acc_zero(acc);
+  if (left) mma64<false, false>(sI, sX, acc, 1.0, wr, wc, lane);
+  else if (LU) mma64<false, false>(sX, sI, acc, 1.0, wr, wc, lane);
+  else mma64<false, true>(sX, sI, acc, 1.0, wr, wc, lane);
+  acc_store(acc, X, sl.ld, wr, wc, lane);
+}
+
+// Trailing update of tile (ti, tj): C -= (ti, s) * (s, tj)       [LU]
+//                                   C -= (ti, s) * (tj, s)^T     [Cholesky, tj < T]
+//                                   C -= (ti, s) * (s, T)        [Cholesky, residual column]
+template <bool LU>
+__global__ void __launch_bounds__(128)
+    k_update(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items, int s) {
+  extern __shared__ double sm[];
+  double *sA = sm, *sB = sm + TB * LDS;
+  const Item it = items[blockIdx.x];
+  const BigSlot sl = slots[it.slot];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  double *base = a.W + sl.base;
+  const int ld = sl.ld;
+  double *C = base + int64_t(it.ti) * TB * ld + int64_t(it.tj) * TB;
+  const double *A = base + int64_t(it.ti) * TB * ld + int64_t(s) * TB;
+  const bool bt = !LU && it.tj < sl.T;
+  const double *B = bt ? base + int64_t(it.tj) * TB * ld + int64_t(s) * TB
+                       : base + int64_t(s) * TB * ld + int64_t(it.tj) * TB;
+  load_tile(sA, A, ld, tid, blockDim.x);
+  load_tile(sB, B, ld, tid, blockDim.x);
+  double acc[4][4][2];
+  acc_load(acc, C, ld, wr, wc, lane);
+  __syncthreads();
+  if (bt) mma64<false, true>(sA, sB, acc, -1.0, wr, wc, lane);
+  else mma64<false, false>(sA, sB, acc, -1.0, wr, wc, lane);
+  acc_store(acc, C, ld, wr, wc, lane);
+}
+
+// local = V beta - S (S = -E alpha from the Schur complement).
+__global__ void k_big_finish(BigArgs a, const BigSlot *__restrict__ slots) {
+  const BigSlot sl = slots[blockIdx.x];
+  const int F = a.F;
+  const int64_t t0 = a.toff[sl.k];
+  const double *beta = a.beta + blockIdx.x * 4 * kMaxF;
+  const int *act = a.act + blockIdx.x * 3;
+  const double *S = a.W + sl.base + int64_t(sl.T) * TB * sl.ld + int64_t(sl.T) * TB;
+  int bad = 0;
+  for (int i = threadIdx.x; i < sl.m; i += blockDim.x) {
+    const double4 y = a.tgt[a.tidx[t0 + i]];
+    const double yc[3] = {y.x, y.y, y.z};
+    for (int f = 0; f < F; ++f) {
+      double v = beta[4 * f];
+      for (int j = 0; j < 3; ++j)
+        if (act[j] >= 0) v = __fma_rn(yc[act[j]], beta[4 * f + 1 + j], v);
+      const double out = v - S[int64_t(i) * sl.ld + f];
+      if (!isfinite(out)) bad = 1;
+      a.local[(t0 + i) * F + f] = out;
+    }
+  }
+  if (bad) atomicOr(&a.status[sl.k], 2);
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration
+// ---------------------------------------------------------------------------
+
+struct StepLists {
+  std::vector<int> diag_off, trsm_off, upd_off;  // per step offsets (size steps + 1)
+  std::vector<int> diag;
+  std::vector<Item> trsm, upd;
+};
+
+static void build_steps(const std::vector<BigSlot> &slots, bool lu, StepLists &L, int &steps) {
+  steps = 0;
+  for (const auto &s : slots) steps = std::max(steps, s.T);
+  L.diag_off.assign(steps + 1, 0);
+  L.trsm_off.assign(steps + 1, 0);
+  L.upd_off.assign(steps + 1, 0);
+  for (int st = 0; st < steps; ++st) {
+    L.diag_off[st] = int(L.diag.size());
+    L.trsm_off[st] = int(L.trsm.size());
+    L.upd_off[st] = int(L.upd.size());
+    for (int q = 0; q < int(slots.size()); ++q) {
+      const BigSlot &s = slots[q];
+      if (s.T <= st) continue;
+      const int R = s.T + s.TE;
+      L.diag.push_back(q);
+      if (lu) {
+        for (int u = st + 1; u <= s.T; ++u) L.trsm.push_back(Item{q, short(st), short(u)});
+        for (int t = st + 1; t < R; ++t) L.trsm.push_back(Item{q, short(t), short(st)});
+        for (int t = st + 1; t < R; ++t)
+          for (int u = st + 1; u <= s.T; ++u) L.upd.push_back(Item{q, short(t), short(u)});
+      } else {
+        L.trsm.push_back(Item{q, short(st), short(s.T)});
+        for (int t = st + 1; t < R; ++t) L.trsm.push_back(Item{q, short(t), short(st)});
+        for (int t = st + 1; t < R; ++t) {
+          const int umax = (t < s.T) ? t : s.T - 1;
+          for (int u = st + 1; u <= umax; ++u) L.upd.push_back(Item{q, short(t), short(u)});
+          L.upd.push_back(Item{q, short(t), short(s.T)});
+        }
+      }
+    }
+  }
+  L.diag_off[steps] = int(L.diag.size());
+  L.trsm_off[steps] = int(L.trsm.size());
+  L.upd_off[steps] = int(L.upd.size());
+}
+
+static size_t slot_doubles(int n, int m) {
+  const int T = (n + TB - 1) / TB, TE = (m + TB - 1) / TB;
+  return size_t(T + TE) * TB * size_t(T + 1) * TB;
+}
+
+// Solves the listed patches (each with m > 0) with the blocked engine.
+void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
+               const std::vector<int> &patches, double *local, int *status, SolveReport &rep) {
+  if (patches.empty()) return;
+  cudaStream_t st = p.stream;
+  size_t free_b = 0, total_b = 0;
+  PB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t budget = std::max<size_t>(size_t(1) << 30, size_t(double(free_b) * 0.6)) / 8;
+  size_t pos = 0;
+  static bool attr_done = false;
+  if (!attr_done) {
+    const int s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
+    PB_CUDA(cudaFuncSetAttribute(k_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PB_CUDA(cudaFuncSetAttribute(k_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PB_CUDA(cudaFuncSetAttribute(k_trsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    PB_CUDA(cudaFuncSetAttribute(k_trsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    PB_CUDA(cudaFuncSetAttribute(k_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    PB_CUDA(cudaFuncSetAttribute(k_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    attr_done = true;
+  }
+  BigArgs a{};
+  a.src = p.src4.as<double4>();
+  a.tgt = p.tgt4.as<double4>();
+  a.vals = vals;
+  a.soff = p.soff.as<int64_t>();
+  a.sidx = p.sidx.as<int>();
+  a.toff = p.toff.as<int64_t>();
+  a.tidx = p.tidx.as<int>();
+  a.centers = p.centers.as<double4>();
+  a.status = status;
+  a.local = local;
+  a.rinv = 1.0 / p.opts.support_radius;
+  a.F = F;
+  a.dim = p.dim;
+  a.basis = basis;
+  cudaEvent_t ev0, ev1;
+  PB_CUDA(cudaEventCreate(&ev0));
+  PB_CUDA(cudaEventCreate(&ev1));
+  while (pos < patches.size()) {
+    // One wave: as many patches as fit the workspace budget.
+    std::vector<BigSlot> slots;
+    size_t tot = 0;
+    while (pos < patches.size()) {
+      const int k = patches[pos];
+      const int n = p.n_host[k], m = p.m_host[k];
+      const size_t d = slot_doubles(n, m);
+      if (!slots.empty() && tot + d > budget) break;
+      BigSlot s{};
+      s.base = int64_t(tot);
+      s.T = (n + TB - 1) / TB;
+      s.TE = (m + TB - 1) / TB;
+      s.ld = (s.T + 1) * TB;
+      s.k = k;
+      s.n = n;
+      s.m = m;
+      slots.push_back(s);
+      tot += d;
+      ++pos;
+      const double nn = n;
+      rep.factor_flops += (lu ? 2.0 / 3.0 : 1.0 / 3.0) * nn * nn * nn + 2.0 * nn * nn * F +
+                          2.0 * double(m) * nn * F;
+    }
+    const int ns = int(slots.size());
+    StepLists L;
+    int steps = 0;
+    build_steps(slots, lu, L, steps);
+    std::vector<Item> asm_items;
+    for (int q = 0; q < ns; ++q) {
+      const BigSlot &s = slots[q];
+      for (int t = 0; t < s.T + s.TE; ++t)
+        for (int u = 0; u <= s.T; ++u) {
+          if (!lu && t < s.T && u < s.T && u > t) continue;  // upper A tiles unused
+          asm_items.push_back(Item{q, short(t), short(u)});
+        }
+    }
+    DevMem dW, dinv, dbeta, dact, dslots, dasm, ddiag, dtrsm, dupd;
+    dW.alloc(sizeof(double) * tot, st);
+    dinv.alloc(sizeof(double) * 2 * TB * TB * ns, st);
+    dbeta.alloc(sizeof(double) * 4 * kMaxF * ns, st);
+    dact.alloc(sizeof(int) * 3 * ns, st);
+    dslots.alloc(sizeof(BigSlot) * ns, st);
+    dasm.alloc(sizeof(Item) * asm_items.size(), st);
+    ddiag.alloc(sizeof(int) * std::max<size_t>(L.diag.size(), 1), st);
+    dtrsm.alloc(sizeof(Item) * std::max<size_t>(L.trsm.size(), 1), st);
+    dupd.alloc(sizeof(Item) * std::max<size_t>(L.upd.size(), 1), st);
+    PB_CUDA(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(BigSlot) * ns, cudaMemcpyHostToDevice, st));
+    PB_CUDA(cudaMemcpyAsync(dasm.p, asm_items.data(), sizeof(Item) * asm_items.size(),
+                            cudaMemcpyHostToDevice, st));
+    if (!L.diag.empty())
+      PB_CUDA(cudaMemcpyAsync(ddiag.p, L.diag.data(), sizeof(int) * L.diag.size(),
+                              cudaMemcpyHostToDevice, st));
+    if (!L.trsm.empty())
+      PB_CUDA(cudaMemcpyAsync(dtrsm.p, L.trsm.data(), sizeof(Item) * L.trsm.size(),
+                              cudaMemcpyHostToDevice, st));
+    if (!L.upd.empty())
+      PB_CUDA(cudaMemcpyAsync(dupd.p, L.upd.data(), sizeof(Item) * L.upd.size(),
+                              cudaMemcpyHostToDevice, st));
+    a.W = dW.as<double>();
+    a.inv = dinv.as<double>();
+    a.beta = dbeta.as<double>();
+    a.act = dact.as<int>();
+    const BigSlot *ds = dslots.as<BigSlot>();
+    PB_CUDA(cudaEventRecord(ev0, st));
+    k_assemble<<<int(asm_items.size()), 256, 0, st>>>(a, ds, dasm.as<Item>());
+    note_launch();
+    k_big_poly<<<ns, 256, 0, st>>>(a, ds);
+    note_launch();
+    const size_t s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
+    for (int s = 0; s < steps; ++s) {
+      const int nd = L.diag_off[s + 1] - L.diag_off[s];
+      const int nt = L.trsm_off[s + 1] - L.trsm_off[s];
+      const int nu = L.upd_off[s + 1] - L.upd_off[s];
+      if (lu) {
+        k_diag<true><<<nd, 256, s3, st>>>(a, ds, ddiag.as<int>() + L.diag_off[s], s);
+        note_launch();
+        if (nt) {
+          k_trsm<true><<<nt, 128, s2, st>>>(a, ds, dtrsm.as<Item>() + L.trsm_off[s], s);
+          note_launch();
+        }
+        if (nu) {
+          k_update<true><<<nu, 128, s2, st>>>(a, ds, dupd.as<Item>() + L.upd_off[s], s);
+          note_launch();
+        }
+      } else {
+        k_diag<false><<<nd, 256, s3, st>>>(a, ds, ddiag.as<int>() + L.diag_off[s], s);
+        note_launch();
+        if (nt) {
+          k_trsm<false><<<nt, 128, s2, st>>>(a, ds, dtrsm.as<Item>() + L.trsm_off[s], s);
+          note_launch();
+        }
+        if (nu) {
+          k_update<false><<<nu, 128, s2, st>>>(a, ds, dupd.as<Item>() + L.upd_off[s], s);
+          note_launch();
+        }
+      }
+    }
+    k_big_finish<<<ns, 128, 0, st>>>(a, ds);
+    note_launch();
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaEventRecord(ev1, st));
+    PB_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    rep.ms_factor += ms;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+}
+
+}  // namespace pacman_b200

@@ -11,6 +11,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "plan.hpp"
@@ -108,111 +110,86 @@ __global__ void k_radius_samples(RadiusState *rs, const unsigned long long *bb, 
   }
 }
 
-// Nearest source of each sample (lowest id on ties): per-block partials.
-__global__ void k_nearest_samples(const double4 *__restrict__ pts, int64_t n,
-                                  const RadiusState *rs, double *pd, long long *pi) {
-  __shared__ double sd[kThreads / 32][7];
-  __shared__ long long si[kThreads / 32][7];
-  const int ns = rs->nsamples;
-  double bd[7];
-  long long bi[7];
-  double sx[7], sy[7], sz[7];
-  for (int s = 0; s < 7; ++s) {
-    bd[s] = INFINITY;
-    bi[s] = 0x7fffffffffffffffll;
-    sx[s] = rs->samples[s][0];
-    sy[s] = rs->samples[s][1];
-    sz[s] = rs->samples[s][2];
+// Nearest source of each sample (lowest id on ties), in two exact passes with
+// one sample per blockIdx.y: the minimum squared distance (its bit pattern is
+// monotone for values >= 0), then the lowest id attaining it.
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
   }
+  return v;
+}
+
+__global__ void k_nearest_dist(const double4 *__restrict__ pts, int64_t n, const RadiusState *rs,
+                               unsigned long long *best_bits) {
+  const int s = blockIdx.y;
+  if (s >= rs->nsamples) return;
+  const double sx = rs->samples[s][0], sy = rs->samples[s][1], sz = rs->samples[s][2];
+  unsigned long long best = ~0ull;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double4 p = pts[i];
-    for (int s = 0; s < ns; ++s) {
-      const double d2 = sqdist3(sx[s], sy[s], sz[s], p.x, p.y, p.z);
-      if (d2 < bd[s] || (d2 == bd[s] && i < bi[s])) {
-        bd[s] = d2;
-        bi[s] = i;
-      }
-    }
+    const unsigned long long b =
+        (unsigned long long)__double_as_longlong(sqdist3(sx, sy, sz, p.x, p.y, p.z));
+    best = b < best ? b : best;
   }
-  for (int s = 0; s < ns; ++s) {
-    for (int o = 16; o > 0; o >>= 1) {
-      const double od = __shfl_xor_sync(0xffffffffu, bd[s], o);
-      const long long oi = __shfl_xor_sync(0xffffffffu, bi[s], o);
-      if (od < bd[s] || (od == bd[s] && oi < bi[s])) {
-        bd[s] = od;
-        bi[s] = oi;
-      }
-    }
-    if ((threadIdx.x & 31) == 0) {
-      sd[threadIdx.x / 32][s] = bd[s];
-      si[threadIdx.x / 32][s] = bi[s];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < ns) {
-    const int s = threadIdx.x;
-    double b = INFINITY;
-    long long ix = 0x7fffffffffffffffll;
-    for (int w = 0; w < kThreads / 32; ++w)
-      if (sd[w][s] < b || (sd[w][s] == b && si[w][s] < ix)) {
-        b = sd[w][s];
-        ix = si[w][s];
-      }
-    pd[blockIdx.x * 7 + s] = b;
-    pi[blockIdx.x * 7 + s] = ix;
-  }
+  best = warp_min_u64(best);
+  if ((threadIdx.x & 31) == 0) atomicMin(&best_bits[s], best);
 }
 
-__global__ void k_nearest_final(int nblocks, const double *pd, const long long *pi,
-                                const double4 *pts, RadiusState *rs) {
+__global__ void k_nearest_index(const double4 *__restrict__ pts, int64_t n, const RadiusState *rs,
+                                const unsigned long long *best_bits, unsigned long long *best_id) {
+  const int s = blockIdx.y;
+  if (s >= rs->nsamples) return;
+  const double sx = rs->samples[s][0], sy = rs->samples[s][1], sz = rs->samples[s][2];
+  const unsigned long long target = best_bits[s];
+  unsigned long long id = ~0ull;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double4 p = pts[i];
+    const unsigned long long b =
+        (unsigned long long)__double_as_longlong(sqdist3(sx, sy, sz, p.x, p.y, p.z));
+    if (b == target && (unsigned long long)i < id) id = (unsigned long long)i;
+  }
+  id = warp_min_u64(id);
+  if ((threadIdx.x & 31) == 0) atomicMin(&best_id[s], id);
+}
+
+__global__ void k_nearest_final(const unsigned long long *best_id, const double4 *pts,
+                                RadiusState *rs) {
   const int s = threadIdx.x;
   if (s >= rs->nsamples) return;
-  double b = INFINITY;
-  long long ix = 0x7fffffffffffffffll;
-  for (int k = 0; k < nblocks; ++k)
-    if (pd[k * 7 + s] < b || (pd[k * 7 + s] == b && pi[k * 7 + s] < ix)) {
-      b = pd[k * 7 + s];
-      ix = pi[k * 7 + s];
-    }
-  const double4 p = pts[ix];
+  const double4 p = pts[best_id[s]];
   rs->proj[s][0] = p.x;
   rs->proj[s][1] = p.y;
   rs->proj[s][2] = p.z;
 }
 
-// One 8-bit radix-select pass over the squared distances (as ordered
-// uint64 keys; they are >= 0, so the raw bits are monotone) from every
-// projected sample to every source.
+// One 8-bit radix-select pass over the squared distances (raw uint64 bits,
+// monotone for values >= 0) from projected sample blockIdx.y to every source.
 __global__ void k_knn_hist(const double4 *__restrict__ pts, int64_t n, const RadiusState *rs,
                            int pass, unsigned int *hist) {
-  __shared__ unsigned int h[7][256];
-  for (int i = threadIdx.x; i < 7 * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
+  __shared__ unsigned int h[256];
+  const int s = blockIdx.y;
+  if (s >= rs->nsamples) return;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0u;
   __syncthreads();
-  const int ns = rs->nsamples;
   const int shift = 56 - 8 * pass;
   const unsigned long long hmask = pass == 0 ? 0ull : (~0ull << (64 - 8 * pass));
-  double sx[7], sy[7], sz[7];
-  unsigned long long pre[7];
-  for (int s = 0; s < 7; ++s) {
-    sx[s] = rs->proj[s][0];
-    sy[s] = rs->proj[s][1];
-    sz[s] = rs->proj[s][2];
-    pre[s] = rs->prefix[s];
-  }
+  const double sx = rs->proj[s][0], sy = rs->proj[s][1], sz = rs->proj[s][2];
+  const unsigned long long pre = rs->prefix[s];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double4 p = pts[i];
-    for (int s = 0; s < ns; ++s) {
-      const unsigned long long key =
-          (unsigned long long)__double_as_longlong(sqdist3(sx[s], sy[s], sz[s], p.x, p.y, p.z));
-      if ((key & hmask) == pre[s]) atomicAdd(&h[s][(key >> shift) & 0xffu], 1u);
-    }
+    const unsigned long long key =
+        (unsigned long long)__double_as_longlong(sqdist3(sx, sy, sz, p.x, p.y, p.z));
+    if ((key & hmask) == pre) atomicAdd(&h[(key >> shift) & 0xffu], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < ns * 256; i += blockDim.x) {
-    const unsigned int v = (&h[0][0])[i];
-    if (v) atomicAdd(&hist[i], v);
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    const unsigned int v = h[i];
+    if (v) atomicAdd(&hist[s * 256 + i], v);
   }
 }
 
@@ -788,20 +765,25 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   k_radius_samples<<<1, 1, 0, st>>>(rsm.as<RadiusState>(), bb.as<unsigned long long>(), dim, kk);
   note_launch();
   const int nb_near = grid_for(n, kThreads, 148 * 4);
-  pd.alloc(sizeof(double) * 7 * nb_near, st);
-  pi.alloc(sizeof(long long) * 7 * nb_near, st);
-  k_nearest_samples<<<nb_near, kThreads, 0, st>>>(p.src4.as<double4>(), n,
-                                                  rsm.as<RadiusState>(), pd.as<double>(),
-                                                  pi.as<long long>());
+  pd.alloc(sizeof(unsigned long long) * 7, st);
+  pi.alloc(sizeof(unsigned long long) * 7, st);
+  PB_CUDA(cudaMemsetAsync(pd.p, 0xff, sizeof(unsigned long long) * 7, st));
+  PB_CUDA(cudaMemsetAsync(pi.p, 0xff, sizeof(unsigned long long) * 7, st));
+  k_nearest_dist<<<dim3(nb_near, 2 * dim + 1), kThreads, 0, st>>>(
+      p.src4.as<double4>(), n, rsm.as<RadiusState>(), pd.as<unsigned long long>());
   note_launch();
-  k_nearest_final<<<1, 32, 0, st>>>(nb_near, pd.as<double>(), pi.as<long long>(),
-                                    p.src4.as<double4>(), rsm.as<RadiusState>());
+  k_nearest_index<<<dim3(nb_near, 2 * dim + 1), kThreads, 0, st>>>(
+      p.src4.as<double4>(), n, rsm.as<RadiusState>(), pd.as<unsigned long long>(),
+      pi.as<unsigned long long>());
+  note_launch();
+  k_nearest_final<<<1, 32, 0, st>>>(pi.as<unsigned long long>(), p.src4.as<double4>(),
+                                    rsm.as<RadiusState>());
   note_launch();
   hist.alloc(sizeof(unsigned int) * 7 * 256, st);
   PB_CUDA(cudaMemsetAsync(hist.p, 0, sizeof(unsigned int) * 7 * 256, st));
   const int nb_hist = grid_for(n, kThreads, 148 * 4);
   for (int pass = 0; pass < 8; ++pass) {
-    k_knn_hist<<<nb_hist, kThreads, 0, st>>>(p.src4.as<double4>(), n, rsm.as<RadiusState>(),
+    k_knn_hist<<<dim3(nb_hist, 2 * dim + 1), kThreads, 0, st>>>(p.src4.as<double4>(), n, rsm.as<RadiusState>(),
                                              pass, hist.as<unsigned int>());
     note_launch();
     k_knn_select<<<1, 32, 0, st>>>(rsm.as<RadiusState>(), hist.as<unsigned int>(), pass);
@@ -818,6 +800,15 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
     p.hi[d] = rs.hi[d];
   }
   p.radius = rs.radius;
+  if (std::getenv("PACMAN_B200_DEBUG")) {
+    std::fprintf(stderr, "[pacman_b200] bbox lo %.17g %.17g %.17g hi %.17g %.17g %.17g\n",
+                 rs.lo[0], rs.lo[1], rs.lo[2], rs.hi[0], rs.hi[1], rs.hi[2]);
+    for (int s = 0; s < rs.nsamples; ++s)
+      std::fprintf(stderr, "[pacman_b200] sample %d (%.17g %.17g %.17g) proj (%.17g %.17g %.17g) kth %.17g\n",
+                   s, rs.samples[s][0], rs.samples[s][1], rs.samples[s][2], rs.proj[s][0],
+                   rs.proj[s][1], rs.proj[s][2], rs.kth[s]);
+    std::fprintf(stderr, "[pacman_b200] radius %.17g\n", rs.radius);
+  }
   if (!(p.radius > 0.0) || !std::isfinite(p.radius))
     throw Error{PACMAN_B200_ERR_DEGENERATE, "degenerate patch radius (zero or non-finite)"};
   const double r = p.radius;

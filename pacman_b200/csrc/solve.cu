@@ -19,9 +19,11 @@
 // reference's uncentred Q for the condition test.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "plan.hpp"
+#include "poly.cuh"
 
 namespace pacman_b200 {
 
@@ -54,177 +56,6 @@ struct PatchArgs {
 
 constexpr int kSolveThreads = 256;
 constexpr int kWarps = kSolveThreads / 32;
-constexpr int kMaxF = 8;
-constexpr int kRedVals = 10 + 4 * kMaxF + 6;
-
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// Singular values (descending) of a pv x pv upper-triangular-ish matrix by
-// one-sided Jacobi.
-__device__ void small_svd(double M[4][4], int pv, double *sig) {
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    bool rot = false;
-    for (int i = 0; i < pv; ++i)
-      for (int j = i + 1; j < pv; ++j) {
-        double al = 0, be = 0, ga = 0;
-        for (int r = 0; r < pv; ++r) {
-          al += M[r][i] * M[r][i];
-          be += M[r][j] * M[r][j];
-          ga += M[r][i] * M[r][j];
-        }
-        if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
-        rot = true;
-        const double zeta = (be - al) / (2.0 * ga);
-        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-        for (int r = 0; r < pv; ++r) {
-          const double x = M[r][i], y = M[r][j];
-          M[r][i] = cs * x - sn * y;
-          M[r][j] = sn * x + cs * y;
-        }
-      }
-    if (!rot) break;
-  }
-  for (int j = 0; j < pv; ++j) {
-    double s = 0;
-    for (int r = 0; r < pv; ++r) s += M[r][j] * M[r][j];
-    sig[j] = sqrt(s);
-  }
-  for (int i = 1; i < pv; ++i) {
-    const double x = sig[i];
-    int j = i - 1;
-    while (j >= 0 && sig[j] < x) {
-      sig[j + 1] = sig[j];
-      --j;
-    }
-    sig[j + 1] = x;
-  }
-}
-
-// Cholesky of the pv x pv SPD matrix G (upper factor R, G = R^T R).
-__device__ bool small_chol(const double G[4][4], int pv, double R[4][4]) {
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 4; ++j) R[i][j] = 0.0;
-  for (int j = 0; j < pv; ++j) {
-    double d = G[j][j];
-    for (int k = 0; k < j; ++k) d -= R[k][j] * R[k][j];
-    if (!(d > 0.0)) return false;
-    d = sqrt(d);
-    R[j][j] = d;
-    for (int i = j + 1; i < pv; ++i) {
-      double s = G[j][i];
-      for (int k = 0; k < j; ++k) s -= R[k][j] * R[k][i];
-      R[j][i] = s / d;
-    }
-  }
-  return true;
-}
-
-// Polynomial block of one patch from the reduced moments (one thread).
-// red: [0]=n, [1..3]=sum dx, [4..9]=sum dx_a dx_b (aa,ab,ac,bb,bc,cc),
-//      [10 + 4f + c] = sum q_c b_f, [10+4F .. +6] = min x,y,z, max x,y,z.
-// Writes beta[4 x F] (uncentred basis, zero for dropped axes), act[0..2]
-// (active axis ids, -1 terminated) and returns the dropped flag.
-__device__ int poly_block(const double *red, int F, int dim, const double *shift,
-                          double *beta, int *act) {
-  double G[4][4];
-  G[0][0] = red[0];
-  G[0][1] = G[1][0] = red[1];
-  G[0][2] = G[2][0] = red[2];
-  G[0][3] = G[3][0] = red[3];
-  G[1][1] = red[4];
-  G[1][2] = G[2][1] = red[5];
-  G[1][3] = G[3][1] = red[6];
-  G[2][2] = red[7];
-  G[2][3] = G[3][2] = red[8];
-  G[3][3] = red[9];
-  const double *mn = red + 10 + 4 * F;
-  const double *mx = mn + 3;
-  bool active[3] = {dim > 0, dim > 1, dim > 2};
-  int pv = dim + 1;
-  int dropped = 0;
-  const double n = red[0];
-  int S[4];
-  double R[4][4];
-  bool have_R = false;
-  for (;;) {
-    int c = 0;
-    S[c++] = 0;
-    for (int a = 0; a < dim; ++a)
-      if (active[a]) S[c++] = a + 1;
-    if (pv <= 1) {
-      have_R = false;
-      break;
-    }
-    double Gs[4][4];
-    for (int i = 0; i < pv; ++i)
-      for (int j = 0; j < pv; ++j) Gs[i][j] = G[S[i]][S[j]];
-    double cond = INFINITY;
-    if (n >= double(pv) && small_chol(Gs, pv, R)) {
-      double M[4][4];
-      for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) M[i][j] = 0.0;
-      for (int i = 0; i < pv; ++i) {
-        M[i][0] = R[i][0];
-        for (int j = 1; j < pv; ++j) M[i][j] = R[i][j] + R[i][0] * shift[S[j] - 1];
-      }
-      double sig[4];
-      small_svd(M, pv, sig);
-      cond = sig[0] / fmax(sig[pv - 1], kEps);
-      have_R = true;
-    } else {
-      have_R = false;
-    }
-    if (!(cond > kCondMax)) break;
-    // SerialDeactivateOneAxis (serial_ops.hpp:28-57).
-    double best = 1.7976931348623157e308;
-    int bi = 0;
-    for (int a = 0; a < dim; ++a) {
-      const double rg = active[a] ? fabs(mx[a] - mn[a]) : 1.7976931348623157e308;
-      if (rg < best) {
-        best = rg;
-        bi = a;
-      }
-    }
-    active[bi] = false;
-    --pv;
-    dropped = 1;
-  }
-  if (!have_R) {
-    double Gs[4][4];
-    for (int i = 0; i < pv; ++i)
-      for (int j = 0; j < pv; ++j) Gs[i][j] = G[S[i]][S[j]];
-    small_chol(Gs, pv, R);
-  }
-  int na = 0;
-  for (int a = 0; a < dim; ++a)
-    if (active[a]) act[na++] = a;
-  for (int a = na; a < 3; ++a) act[a] = -1;
-  for (int f = 0; f < F; ++f) {
-    const double *h = red + 10 + 4 * f;
-    double z[4], bp[4];
-    // R^T z = h_S, R bp = z.
-    for (int i = 0; i < pv; ++i) {
-      double s = h[S[i]];
-      for (int k = 0; k < i; ++k) s -= R[k][i] * z[k];
-      z[i] = s / R[i][i];
-    }
-    for (int i = pv - 1; i >= 0; --i) {
-      double s = z[i];
-      for (int k = i + 1; k < pv; ++k) s -= R[i][k] * bp[k];
-      bp[i] = s / R[i][i];
-    }
-    double b0 = bp[0];
-    for (int i = 1; i < pv; ++i) b0 -= shift[S[i] - 1] * bp[i];
-    beta[4 * f + 0] = b0;
-    for (int i = 1; i < pv; ++i) beta[4 * f + i] = bp[i];
-    for (int i = pv; i < 4; ++i) beta[4 * f + i] = 0.0;
-  }
-  return dropped;
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(kSolveThreads)
@@ -254,9 +85,10 @@ __global__ void __launch_bounds__(kSolveThreads)
   // Gather the patch (TeamFillB, team_ops.hpp:113-121) and its moments.
   const double4 c = a.centers[k];
   const double shift[3] = {c.x, c.y, c.z};
-  double acc[kRedVals];
+  double acc[kRedVals - 6];
   const int nred = 10 + 4 * F;
-  for (int v = 0; v < nred; ++v) acc[v] = 0.0;
+#pragma unroll
+  for (int v = 0; v < kRedVals - 6; ++v) acc[v] = 0.0;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int i = tid; i < n; i += kSolveThreads) {
     const int id = a.sidx[s0 + i];
@@ -275,10 +107,14 @@ __global__ void __launch_bounds__(kSolveThreads)
     acc[7] += q[2] * q[2];
     acc[8] += q[2] * q[3];
     acc[9] += q[3] * q[3];
-    for (int f = 0; f < F; ++f) {
-      const double b = a.vals[int64_t(id) * F + f];
-      A[int64_t(i) * lda + n + f] = b;
-      for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) {
+      if (f < F) {
+        const double b = a.vals[int64_t(id) * F + f];
+        A[int64_t(i) * lda + n + f] = b;
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
+      }
     }
     const double pc[3] = {p.x, p.y, p.z};
     for (int d = 0; d < 3; ++d) {
@@ -286,9 +122,10 @@ __global__ void __launch_bounds__(kSolveThreads)
       mx[d] = fmax(mx[d], pc[d]);
     }
   }
-  for (int v = 0; v < nred; ++v) {
+#pragma unroll
+  for (int v = 0; v < kRedVals - 6; ++v) {
     const double s = warp_sum(acc[v]);
-    if (lane == 0) red[warp][v] = s;
+    if (lane == 0 && v < nred) red[warp][v] = s;
   }
   for (int d = 0; d < 3; ++d) {
     double lo = mn[d], hi = mx[d];
@@ -418,13 +255,17 @@ __global__ void __launch_bounds__(kSolveThreads)
   for (int i = warp; i < m; i += kWarps) {
     const double4 y = a.tgt[a.tidx[t0 + i]];
     double s[kMaxF];
-    for (int f = 0; f < F; ++f) s[f] = 0.0;
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) s[f] = 0.0;
     for (int j = lane; j < n; j += 32) {
       const double d = __dsqrt_rn(sqdist3(y.x, y.y, y.z, xs[j], ys[j], zs[j]));
       const double ph = wendland<double>(a.basis, d, a.rinv);
-      for (int f = 0; f < F; ++f) s[f] = __fma_rn(ph, A[int64_t(j) * lda + n + f], s[f]);
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f)
+        if (f < F) s[f] = __fma_rn(ph, A[int64_t(j) * lda + n + f], s[f]);
     }
-    for (int f = 0; f < F; ++f) s[f] = warp_sum(s[f]);
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) s[f] = warp_sum(s[f]);
     if (lane == 0) {
       const double yc[3] = {y.x, y.y, y.z};
       for (int f = 0; f < F; ++f) {
@@ -550,12 +391,22 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
   cudaEventDestroy(ev1);
 }
 
+void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
+               const std::vector<int> &patches, double *local, int *status, SolveReport &rep);
+
+// Patches above this size use the blocked engine (blocked.cu).
+static int big_threshold() {
+  const char *e = std::getenv("PACMAN_B200_BIG_N");
+  return e ? std::max(1, std::atoi(e)) : 128;
+}
+
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
                    double *local_dev, SolveReport &rep) {
   cudaStream_t st = p.stream;
   const int K = p.K;
   if (K == 0) return;
   p.status.alloc(sizeof(int) * K, st);
+  PB_CUDA(cudaMemsetAsync(p.status.p, 0, sizeof(int) * K, st));
   PatchArgs a{};
   a.src = p.src4.as<double4>();
   a.tgt = p.tgt4.as<double4>();
@@ -571,23 +422,31 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   a.F = F;
   a.dim = p.dim;
   a.basis = basis;
-  std::vector<int> all(K);
-  for (int k = 0; k < K; ++k) all[k] = k;
+  const int nbig = big_threshold();
+  std::vector<int> small, big;
+  for (int k = 0; k < K; ++k) {
+    if (p.m_host[k] == 0) continue;  // no target: the patch contributes nothing
+    (p.n_host[k] > nbig ? big : small).push_back(k);
+  }
   const int mode = precision == PACMAN_B200_FP64 ? kLU : kChol;
-  run_list(p, a, mode, all, rep);
+  run_list(p, a, mode, small, rep);
+  solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep);
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
   PB_CUDA(cudaStreamSynchronize(st));
-  std::vector<int> redo;
+  std::vector<int> redo_small, redo_big;
   for (int k = 0; k < K; ++k) {
+    if (p.m_host[k] == 0) continue;
     if (stat[k] & kStatusDropped) rep.dropped++;
-    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite))) redo.push_back(k);
+    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite)))
+      (p.n_host[k] > nbig ? redo_big : redo_small).push_back(k);
   }
-  rep.patches_fp64 = K;
-  if (!redo.empty()) {
-    run_list(p, a, kLU, redo, rep);
-    rep.patches_fallback += int64_t(redo.size());
-  }
+  rep.patches_fp64 = int64_t(small.size() + big.size());
+  if (!redo_small.empty()) run_list(p, a, kLU, redo_small, rep);
+  if (!redo_big.empty())
+    solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep);
+  rep.patches_fallback += int64_t(redo_small.size() + redo_big.size());
+  if (!redo_small.empty() || !redo_big.empty()) PB_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace pacman_b200

@@ -26,13 +26,15 @@ def _cases():
     rng = np.random.default_rng(3)
     u = W.make("uniform_20k")
     gb = W.make("grid_blobs_1m", scale=0.01)
+    S2, T2 = rng.random((6000, 2)), rng.random((5000, 2))
+    S1, T1 = rng.random((3000, 1)), rng.random((2000, 1))
+    # Smooth fields of the coordinates, as in the reference's tests: random
+    # values would make even two FP64 LAPACK solvers differ by ~1e-11.
     return {
         "uniform_20k_c2": (3, u["src"], u["tgt"], u["values"][:, 0], 0x11, 30),
         "grid_blobs_10k_c4": (3, gb["src"], gb["tgt"], gb["values"][:, 0], 0x12, 50),
-        "uniform_2d": (2, rng.random((6000, 2)), rng.random((5000, 2)),
-                       np.sin(4 * rng.random(6000)), 0x13, 40),
-        "uniform_1d": (1, rng.random((3000, 1)), rng.random((2000, 1)),
-                       np.cos(rng.random(3000)), 0x10, 20),
+        "uniform_2d": (2, S2, T2, np.sin(4 * S2[:, 0]) * np.cos(3 * S2[:, 1]), 0x13, 40),
+        "uniform_1d": (1, S1, T1, np.cos(3 * S1[:, 0]), 0x10, 20),
     }
 
 
@@ -221,3 +223,28 @@ def test_cpp_dropin(tmp_path):
                    check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("name", ["uniform_20k_c2", "grid_blobs_10k_c4", "uniform_2d"])
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_FP64), ("mixed", TOL_MIXED)])
+def test_blocked_engine_matches_oracle(name, precision, tol, monkeypatch):
+    # Route every patch with more than 8 sources through the tiled tensor-core
+    # engine (normally only patches above 128 sources go there).
+    monkeypatch.setenv("PACMAN_B200_BIG_N", "8")
+    dim, S, T, v, basis, npc = CASES[name]
+    st = {}
+    out = pacman.rbf.interpolate(dim, CUDA, basis, S, v, T, nodes_per_cluster=npc,
+                                 precision=precision, stats=st)
+    ref = oracle.interpolate(dim, basis, S, v, T, npc)
+    assert rel_l2(out, ref) <= tol
+    assert st["patches_fallback"] == 0 or precision == "mixed"
+
+
+def test_blocked_engine_multifield(monkeypatch):
+    monkeypatch.setenv("PACMAN_B200_BIG_N", "16")
+    sh = W.make("shell_4m", scale=0.004)
+    S, T, V = sh["src"], sh["tgt"], sh["values"]
+    for precision in ("fp64", "mixed"):
+        out = pacman.rbf.interpolate(3, CUDA, 0x12, S, V, T, precision=precision)
+        ref = oracle.interpolate(3, 0x12, S, V, T)
+        assert rel_l2(out, ref) <= TOL_FP64
