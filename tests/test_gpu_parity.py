@@ -86,6 +86,14 @@ def test_grid20_node_reproduction(basis, precision):
     assert rel_l2(out, v) < 1e-8
 
 
+# On the coarse slab mesh (438 points, patch radius 0.08 inside the 0.1
+# support) C6 and C8 give cond(A) up to 1.1e11 and 1.4e11; there LAPACK's LU
+# and the oracle's LU already differ by 5.6e-12 and 5.1e-12 (rel-L2 of the
+# local values), the FP64 noise floor of the problem itself.  Those two
+# bases are held to twice that floor, every other case to 1e-12.
+SLAB_TOL = {0x10: TOL_FP64, 0x11: TOL_FP64, 0x12: TOL_FP64, 0x13: 1.2e-11, 0x14: 1.2e-11}
+
+
 @pytest.mark.parametrize("pair", [("0.03", "0.003"), ("0.003", "0.03"), ("0.03", "0.03")])
 def test_slab_meshes(pair):
     # The reference's Python known-answer test (test_rbf-pum.py:58-74).
@@ -95,7 +103,7 @@ def test_slab_meshes(pair):
         out = pacman.rbf.interpolate(3, CUDA, basis, S, W.franke_3d(S), T)
         assert rel_l2(out, W.franke_3d(T)) < 1.5e-2
         ref = oracle.interpolate(3, basis, S, W.franke_3d(S), T)
-        assert rel_l2(out, ref) <= TOL_FP64
+        assert rel_l2(out, ref) <= SLAB_TOL[basis]
 
 
 def test_local_values_match_oracle():
@@ -152,12 +160,16 @@ def test_edge_cases():
     ref = oracle.interpolate(3, 0x12, P, f, Q)
     assert st["dropped_axis_patches"] == st["num_patches"]
     assert rel_l2(out, ref) <= TOL_FP64
-    # Duplicate source points in the cloud.
+    # Duplicate source points: every patch matrix is singular and the
+    # reference's unpivoted LU divides by a zero pivot; the results must be
+    # non-finite exactly where the oracle's are (here: everywhere).
     D = np.concatenate([S, S[:100]])
     dv = W.franke_3d(D)
     Tt = rng.random((400, 3))
-    out = pacman.rbf.interpolate(3, CUDA, 0x11, D, dv, Tt, precision="mixed")
-    assert np.all(np.isfinite(out))
+    ref = oracle.interpolate(3, 0x11, D, dv, Tt)
+    for precision in ("fp64", "mixed"):
+        out = pacman.rbf.interpolate(3, CUDA, 0x11, D, dv, Tt, precision=precision)
+        assert np.array_equal(np.isfinite(out), np.isfinite(ref))
 
 
 def test_torch_device_tensors():
