@@ -133,6 +133,27 @@ PACMAN_B200_API int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, i
  * order of the target membership lists, times n_fields. */
 PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local);
 
+/*
+ * Patch radius (the transfer's cluster-size heuristic: 2*dim+1 sample points
+ * projected onto their nearest source, k-th nearest source distance with
+ * k = nodes_per_cluster, median) WITHOUT ANY DEVICE ALLOCATION.  No
+ * counterpart in the reference: it exists for callers that cannot let a
+ * library allocate device memory, e.g. a coupled code that reserves the GPU
+ * for its own pool allocator at start-up.  Its working memory is one fixed
+ * 16 KiB file-scope __device__ array, present on every GPU that loads this
+ * library until the process exits; the first call on a device resolves that
+ * array's address (cudaGetSymbolAddress) with the device current, so make the
+ * first call before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.
+ * source_points: device memory of the current device, row-major [n x dim];
+ * limits: dim <= 3 (the array holds at most 7 samples), 1 <= n <= 2^31 - 1.
+ * stream: cudaStream_t (NULL = default stream); the call returns after
+ * *radius (host or device pointer) has been written.
+ */
+PACMAN_B200_API int pacman_b200_patch_radius_noalloc(int32_t dim, const double *source_points,
+                                                     int64_t n_source, int32_t nodes_per_cluster,
+                                                     void *stream, double *radius);
+
 /* Message of the last error on the calling thread ("" if none). */
 PACMAN_B200_API const char *pacman_b200_last_error(void);
 PACMAN_B200_API int32_t pacman_b200_abi_version(void);

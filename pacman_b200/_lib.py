@@ -81,6 +81,8 @@ SIGNATURES = {
     "pacman_b200_plan_centers": (ctypes.c_int, [_VP, _VP]),
     "pacman_b200_plan_patch_lists": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP]),
     "pacman_b200_plan_local_values": (ctypes.c_int, [_VP, _VP]),
+    "pacman_b200_patch_radius_noalloc": (ctypes.c_int, [
+        ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int32, _VP, _VP]),
     "pacman_b200_last_error": (ctypes.c_char_p, []),
     "pacman_b200_abi_version": (ctypes.c_int32, []),
 }

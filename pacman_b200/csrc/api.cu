@@ -26,8 +26,12 @@ int64_t &launch_counter() {
 }
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+namespace {
 
 int fail(int code, const std::string &msg) {
   g_last_error = msg;
