@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="run warmup + steps transfers and exit (for ncu launch lists)")
     return ap.parse_args()
 
 
@@ -303,6 +305,14 @@ def main():
     for _ in range(args.warmup):
         step(args.precision)
     torch.cuda.synchronize()
+    if args.kernels_only:
+        st = {}
+        for _ in range(args.steps):
+            step(args.precision, st)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"kernels_only": True, "steps": args.steps, "stats": st}), flush=True)
+        return
     stats = {}
     with ClockSampler(local) as clk:
         times = timed(lambda: step(args.precision, stats), args.steps)
