@@ -6,6 +6,7 @@
 // phase (geometry.cu), the patch solves (solve.cu, blocked.cu) and the
 // partition-of-unity gather, and copies the result back when the caller
 // passed a host pointer.  No exception crosses the ABI.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -30,6 +31,41 @@ thread_local std::string g_last_error;
 }  // namespace
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+HostArena &HostArena::get() {
+  static thread_local HostArena arena;
+  return arena;
+}
+
+void HostArena::reset() {
+  for (char *b : retired_) cudaFreeHost(b);
+  retired_.clear();
+  used_ = 0;
+}
+
+void *HostArena::alloc(size_t bytes) {
+  bytes = (bytes + 255) & ~size_t(255);
+  if (used_ + bytes > cap_) {
+    size_t cap = std::max<size_t>(cap_ * 2, std::max<size_t>(bytes, size_t(1) << 20));
+    char *nb = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&nb), cap, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{PACMAN_B200_ERR_NOMEM, "pinned host staging allocation failed"};
+    }
+    if (base_) retired_.push_back(base_);
+    base_ = nb;
+    cap_ = cap;
+    used_ = 0;
+  }
+  void *p = base_ + used_;
+  used_ += bytes;
+  return p;
+}
+
+HostArena::~HostArena() {
+  reset();
+  if (base_) cudaFreeHost(base_);
+}
 
 namespace {
 
@@ -134,6 +170,7 @@ int create_plan(int32_t dim, const double *src, int64_t n, const double *tgt, in
   try {
     DeviceScope ds(o.device);
     tune_pool(ds.dev);
+    HostArena::get().reset();
     p.device = ds.dev;
     p.dim = dim;
     p.n = n;
@@ -172,6 +209,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
   if (out == nullptr && p.m > 0) return fail(PACMAN_B200_ERR_INVALID, "target_values is null");
   try {
     DeviceScope ds(p.device);
+    HostArena::get().reset();
     cudaStream_t st = p.stream;
     cudaEvent_t e0, e1, e2;
     PB_CUDA(cudaEventCreate(&e0));

@@ -41,10 +41,87 @@ struct BigSlot {
   int n, m;
 };
 
-struct Item {
-  int slot;
-  short ti, tj;
-};
+// Work of one launch is addressed by blockIdx.x through prefix counts over
+// the active slots (slots are sorted by decreasing T, so the slots still
+// active at step s are 0..cnt-1): pre[q] <= blockIdx.x < pre[q + 1].
+__device__ __forceinline__ int find_slot(const int *__restrict__ pre, int cnt, int b) {
+  int lo = 0, hi = cnt;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Tiles filled by the assembly of one slot: LU every (row, column) tile of
+// the augmented matrix; Cholesky the lower A tiles, every E tile and the
+// residual column (row t < T: t + 2 tiles, row t >= T: T + 1 tiles).
+__device__ __forceinline__ void decode_assemble(bool lu, const BigSlot &sl, int l, int &ti,
+                                                int &tj) {
+  if (lu) {
+    ti = l / (sl.T + 1);
+    tj = l % (sl.T + 1);
+    return;
+  }
+  int t = 0;
+  for (;;) {
+    const int len = (t < sl.T) ? t + 2 : sl.T + 1;
+    if (l < len) {
+      ti = t;
+      tj = (t < sl.T) ? (l <= t ? l : sl.T) : l;
+      return;
+    }
+    l -= len;
+    ++t;
+  }
+}
+
+// Panel tiles of step s.  LU: row panel (s, s+1..T) then column panel
+// (s+1..R-1, s).  Cholesky: residual tile (s, T) then column panel.
+__device__ __forceinline__ void decode_trsm(bool lu, const BigSlot &sl, int s, int l, int &ti,
+                                            int &tj) {
+  if (lu) {
+    const int nrow = sl.T - s;
+    if (l < nrow) {
+      ti = s;
+      tj = s + 1 + l;
+    } else {
+      ti = s + 1 + (l - nrow);
+      tj = s;
+    }
+  } else if (l == 0) {
+    ti = s;
+    tj = sl.T;
+  } else {
+    ti = s + l;
+    tj = s;
+  }
+}
+
+// Trailing tiles of step s.  LU: rows s+1..R-1 x columns s+1..T.  Cholesky:
+// row t < T holds columns s+1..t then the residual column T; row t >= T
+// holds columns s+1..T-1 then T.
+__device__ __forceinline__ void decode_update(bool lu, const BigSlot &sl, int s, int l, int &ti,
+                                              int &tj) {
+  if (lu) {
+    const int w = sl.T - s;
+    ti = s + 1 + l / w;
+    tj = s + 1 + l % w;
+    return;
+  }
+  int t = s + 1;
+  for (;;) {
+    const int ncol = (t < sl.T) ? (t - s) : (sl.T - s - 1);
+    if (l <= ncol) {
+      ti = t;
+      tj = (l < ncol) ? s + 1 + l : sl.T;
+      return;
+    }
+    l -= ncol + 1;
+    ++t;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core tile product
@@ -152,10 +229,15 @@ struct BigArgs {
 
 // Fills one 64 x 64 tile of an augmented matrix.
 __global__ void __launch_bounds__(256)
-    k_assemble(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items) {
+    k_assemble(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
+               int lu) {
   __shared__ double rx[TB], ry[TB], rz[TB], cx[TB], cy[TB], cz[TB];
-  const Item it = items[blockIdx.x];
-  const BigSlot sl = slots[it.slot];
+  const int q = find_slot(pre, cnt, blockIdx.x);
+  const BigSlot sl = slots[q];
+  struct {
+    int ti, tj;
+  } it;
+  decode_assemble(lu != 0, sl, blockIdx.x - pre[q], it.ti, it.tj);
   const int tid = threadIdx.x;
   double *tile = a.W + sl.base + int64_t(it.ti) * TB * sl.ld + int64_t(it.tj) * TB;
   if (it.tj == sl.T) {  // residual columns: zero (the polynomial pass writes r)
@@ -305,15 +387,14 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
 
 // Factors diagonal tile (s, s) of each listed slot and writes its inverses.
 template <bool LU>
-__global__ void __launch_bounds__(256)
-    k_diag(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ list, int s) {
+__global__ void __launch_bounds__(256) k_diag(BigArgs a, const BigSlot *__restrict__ slots, int s) {
   extern __shared__ double sm[];
   double *T = sm;                 // the tile
   double *Li = T + TB * LDS;      // inverse of L
   double *Ui = Li + TB * LDS;     // inverse of U (LU only)
   __shared__ double piv;
   __shared__ int bad;
-  const int slot = list[blockIdx.x];
+  const int slot = blockIdx.x;
   const BigSlot sl = slots[slot];
   const int tid = threadIdx.x;
   double *g = a.W + sl.base + int64_t(s) * TB * sl.ld + int64_t(s) * TB;
@@ -397,11 +478,17 @@ __device__ __forceinline__ void load_inv(double *s, const double *g, int tid, in
 // X := X U^{-1} (LU) or X := X L^{-T} (Cholesky).
 template <bool LU>
 __global__ void __launch_bounds__(128)
-    k_trsm(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items, int s) {
+    k_trsm(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
+           int s) {
   extern __shared__ double sm[];
   double *sX = sm, *sI = sm + TB * LDS;
-  const Item it = items[blockIdx.x];
-  const BigSlot sl = slots[it.slot];
+  const int q = find_slot(pre, cnt, blockIdx.x);
+  const BigSlot sl = slots[q];
+  struct {
+    int slot, ti, tj;
+  } it;
+  it.slot = q;
+  decode_trsm(LU, sl, s, blockIdx.x - pre[q], it.ti, it.tj);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   double *X = a.W + sl.base + int64_t(it.ti) * TB * sl.ld + int64_t(it.tj) * TB;
@@ -423,11 +510,16 @@ __global__ void __launch_bounds__(128)
 //                                   C -= (ti, s) * (s, T)        [Cholesky, residual column]
 template <bool LU>
 __global__ void __launch_bounds__(128)
-    k_update(BigArgs a, const BigSlot *__restrict__ slots, const Item *__restrict__ items, int s) {
+    k_update(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
+             int s) {
   extern __shared__ double sm[];
   double *sA = sm, *sB = sm + TB * LDS;
-  const Item it = items[blockIdx.x];
-  const BigSlot sl = slots[it.slot];
+  const int q = find_slot(pre, cnt, blockIdx.x);
+  const BigSlot sl = slots[q];
+  struct {
+    int ti, tj;
+  } it;
+  decode_update(LU, sl, s, blockIdx.x - pre[q], it.ti, it.tj);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   double *base = a.W + sl.base;
@@ -475,73 +567,52 @@ __global__ void k_big_finish(BigArgs a, const BigSlot *__restrict__ slots) {
 // Host orchestration
 // ---------------------------------------------------------------------------
 
-struct StepLists {
-  std::vector<int> diag_off, trsm_off, upd_off;  // per step offsets (size steps + 1)
-  std::vector<int> diag;
-  std::vector<Item> trsm, upd;
-};
-
-static void build_steps(const std::vector<BigSlot> &slots, bool lu, StepLists &L, int &steps) {
-  steps = 0;
-  for (const auto &s : slots) steps = std::max(steps, s.T);
-  L.diag_off.assign(steps + 1, 0);
-  L.trsm_off.assign(steps + 1, 0);
-  L.upd_off.assign(steps + 1, 0);
-  for (int st = 0; st < steps; ++st) {
-    L.diag_off[st] = int(L.diag.size());
-    L.trsm_off[st] = int(L.trsm.size());
-    L.upd_off[st] = int(L.upd.size());
-    for (int q = 0; q < int(slots.size()); ++q) {
-      const BigSlot &s = slots[q];
-      if (s.T <= st) continue;
-      const int R = s.T + s.TE;
-      L.diag.push_back(q);
-      if (lu) {
-        for (int u = st + 1; u <= s.T; ++u) L.trsm.push_back(Item{q, short(st), short(u)});
-        for (int t = st + 1; t < R; ++t) L.trsm.push_back(Item{q, short(t), short(st)});
-        for (int t = st + 1; t < R; ++t)
-          for (int u = st + 1; u <= s.T; ++u) L.upd.push_back(Item{q, short(t), short(u)});
-      } else {
-        L.trsm.push_back(Item{q, short(st), short(s.T)});
-        for (int t = st + 1; t < R; ++t) L.trsm.push_back(Item{q, short(t), short(st)});
-        for (int t = st + 1; t < R; ++t) {
-          const int umax = (t < s.T) ? t : s.T - 1;
-          for (int u = st + 1; u <= umax; ++u) L.upd.push_back(Item{q, short(t), short(u)});
-          L.upd.push_back(Item{q, short(t), short(s.T)});
-        }
-      }
-    }
-  }
-  L.diag_off[steps] = int(L.diag.size());
-  L.trsm_off[steps] = int(L.trsm.size());
-  L.upd_off[steps] = int(L.upd.size());
-}
-
 static size_t slot_doubles(int n, int m) {
   const int T = (n + TB - 1) / TB, TE = (m + TB - 1) / TB;
   return size_t(T + TE) * TB * size_t(T + 1) * TB;
 }
 
-// Solves the listed patches (each with m > 0) with the blocked engine.
+static int64_t count_assemble(bool lu, const BigSlot &q) {
+  return lu ? int64_t(q.T + q.TE) * (q.T + 1) : int64_t(q.T) * (q.T + 3) / 2 + int64_t(q.TE) * (q.T + 1);
+}
+static int64_t count_trsm(bool lu, const BigSlot &q, int s) {
+  const int R = q.T + q.TE;
+  return lu ? int64_t(q.T - s) + (R - s - 1) : int64_t(R - s);
+}
+static int64_t count_update(bool lu, const BigSlot &q, int s) {
+  const int64_t R = q.T + q.TE, w = q.T - s;
+  return lu ? (R - s - 1) * w : (w - 1) * w / 2 + (w - 1) + int64_t(q.TE) * w;
+}
+
+static void set_smem_attributes() {
+  static bool done = false;
+  if (done) return;
+  const int s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
+  PB_CUDA(cudaFuncSetAttribute(k_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+  PB_CUDA(cudaFuncSetAttribute(k_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+  PB_CUDA(cudaFuncSetAttribute(k_trsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+  PB_CUDA(cudaFuncSetAttribute(k_trsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+  PB_CUDA(cudaFuncSetAttribute(k_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+  PB_CUDA(cudaFuncSetAttribute(k_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+  done = true;
+}
+
+// Solves the listed patches (each with m > 0) with the blocked engine.  The
+// launches are queued on p.stream without host synchronisation; the
+// workspace of each wave is released stream-ordered after its kernels, so the
+// next wave reuses it.
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                const std::vector<int> &patches, double *local, int *status, SolveReport &rep) {
   if (patches.empty()) return;
   cudaStream_t st = p.stream;
+  set_smem_attributes();
   size_t free_b = 0, total_b = 0;
   PB_CUDA(cudaMemGetInfo(&free_b, &total_b));
   const size_t budget = std::max<size_t>(size_t(1) << 30, size_t(double(free_b) * 0.6)) / 8;
-  size_t pos = 0;
-  static bool attr_done = false;
-  if (!attr_done) {
-    const int s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
-    PB_CUDA(cudaFuncSetAttribute(k_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
-    PB_CUDA(cudaFuncSetAttribute(k_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
-    PB_CUDA(cudaFuncSetAttribute(k_trsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-    PB_CUDA(cudaFuncSetAttribute(k_trsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-    PB_CUDA(cudaFuncSetAttribute(k_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-    PB_CUDA(cudaFuncSetAttribute(k_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-    attr_done = true;
-  }
+  // Largest patches first: the slots active at step s are then a prefix.
+  std::vector<int> order(patches);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return p.n_host[x] > p.n_host[y]; });
   BigArgs a{};
   a.src = p.src4.as<double4>();
   a.tgt = p.tgt4.as<double4>();
@@ -557,27 +628,26 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   a.F = F;
   a.dim = p.dim;
   a.basis = basis;
-  cudaEvent_t ev0, ev1;
-  PB_CUDA(cudaEventCreate(&ev0));
-  PB_CUDA(cudaEventCreate(&ev1));
-  while (pos < patches.size()) {
+  HostArena &arena = HostArena::get();
+  size_t pos = 0;
+  while (pos < order.size()) {
     // One wave: as many patches as fit the workspace budget.
     std::vector<BigSlot> slots;
     size_t tot = 0;
-    while (pos < patches.size()) {
-      const int k = patches[pos];
+    while (pos < order.size()) {
+      const int k = order[pos];
       const int n = p.n_host[k], m = p.m_host[k];
       const size_t d = slot_doubles(n, m);
       if (!slots.empty() && tot + d > budget) break;
-      BigSlot s{};
-      s.base = int64_t(tot);
-      s.T = (n + TB - 1) / TB;
-      s.TE = (m + TB - 1) / TB;
-      s.ld = (s.T + 1) * TB;
-      s.k = k;
-      s.n = n;
-      s.m = m;
-      slots.push_back(s);
+      BigSlot q{};
+      q.base = int64_t(tot);
+      q.T = (n + TB - 1) / TB;
+      q.TE = (m + TB - 1) / TB;
+      q.ld = (q.T + 1) * TB;
+      q.k = k;
+      q.n = n;
+      q.m = m;
+      slots.push_back(q);
       tot += d;
       ++pos;
       const double nn = n;
@@ -585,90 +655,83 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                           2.0 * double(m) * nn * F;
     }
     const int ns = int(slots.size());
-    StepLists L;
-    int steps = 0;
-    build_steps(slots, lu, L, steps);
-    std::vector<Item> asm_items;
+    const int steps = slots.front().T;
+    // Prefix counts: assembly over all slots, then per step the trsm and
+    // update counts over the active slots (a prefix of the sorted slots).
+    std::vector<int> pre_asm(ns + 1, 0);
     for (int q = 0; q < ns; ++q) {
-      const BigSlot &s = slots[q];
-      for (int t = 0; t < s.T + s.TE; ++t)
-        for (int u = 0; u <= s.T; ++u) {
-          if (!lu && t < s.T && u < s.T && u > t) continue;  // upper A tiles unused
-          asm_items.push_back(Item{q, short(t), short(u)});
-        }
+      const int64_t v = pre_asm[q] + count_assemble(lu, slots[q]);
+      if (v > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
+      pre_asm[q + 1] = int(v);
     }
-    DevMem dW, dinv, dbeta, dact, dslots, dasm, ddiag, dtrsm, dupd;
+    std::vector<int> cnt(steps), off(steps + 1, 0), pre;
+    pre.reserve(size_t(steps) * 2 * (ns + 1));
+    for (int s = 0; s < steps; ++s) {
+      int c = 0;
+      while (c < ns && slots[c].T > s) ++c;
+      cnt[s] = c;
+      off[s] = int(pre.size());
+      int64_t acc = 0;
+      pre.push_back(0);
+      for (int q = 0; q < c; ++q) pre.push_back(int(acc += count_trsm(lu, slots[q], s)));
+      acc = 0;
+      pre.push_back(0);
+      for (int q = 0; q < c; ++q) {
+        acc += count_update(lu, slots[q], s);
+        if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
+        pre.push_back(int(acc));
+      }
+    }
+    off[steps] = int(pre.size());
+    DevMem dW, dsmall;
     dW.alloc(sizeof(double) * tot, st);
-    dinv.alloc(sizeof(double) * 2 * TB * TB * ns, st);
-    dbeta.alloc(sizeof(double) * 4 * kMaxF * ns, st);
-    dact.alloc(sizeof(int) * 3 * ns, st);
-    dslots.alloc(sizeof(BigSlot) * ns, st);
-    dasm.alloc(sizeof(Item) * asm_items.size(), st);
-    ddiag.alloc(sizeof(int) * std::max<size_t>(L.diag.size(), 1), st);
-    dtrsm.alloc(sizeof(Item) * std::max<size_t>(L.trsm.size(), 1), st);
-    dupd.alloc(sizeof(Item) * std::max<size_t>(L.upd.size(), 1), st);
-    PB_CUDA(cudaMemcpyAsync(dslots.p, slots.data(), sizeof(BigSlot) * ns, cudaMemcpyHostToDevice, st));
-    PB_CUDA(cudaMemcpyAsync(dasm.p, asm_items.data(), sizeof(Item) * asm_items.size(),
-                            cudaMemcpyHostToDevice, st));
-    if (!L.diag.empty())
-      PB_CUDA(cudaMemcpyAsync(ddiag.p, L.diag.data(), sizeof(int) * L.diag.size(),
-                              cudaMemcpyHostToDevice, st));
-    if (!L.trsm.empty())
-      PB_CUDA(cudaMemcpyAsync(dtrsm.p, L.trsm.data(), sizeof(Item) * L.trsm.size(),
-                              cudaMemcpyHostToDevice, st));
-    if (!L.upd.empty())
-      PB_CUDA(cudaMemcpyAsync(dupd.p, L.upd.data(), sizeof(Item) * L.upd.size(),
-                              cudaMemcpyHostToDevice, st));
+    const size_t n_inv = size_t(2) * TB * TB * ns, n_beta = size_t(4) * kMaxF * ns;
+    const size_t bytes_small = sizeof(double) * (n_inv + n_beta) + sizeof(int) * 3 * ns +
+                               sizeof(BigSlot) * ns + sizeof(int) * (pre_asm.size() + pre.size()) +
+                               64;
+    dsmall.alloc(bytes_small, st);
+    char *cur = dsmall.as<char>();
+    auto take = [&](size_t bytes) {
+      char *r = cur;
+      cur += (bytes + 15) & ~size_t(15);
+      return r;
+    };
     a.W = dW.as<double>();
-    a.inv = dinv.as<double>();
-    a.beta = dbeta.as<double>();
-    a.act = dact.as<int>();
-    const BigSlot *ds = dslots.as<BigSlot>();
-    PB_CUDA(cudaEventRecord(ev0, st));
-    k_assemble<<<int(asm_items.size()), 256, 0, st>>>(a, ds, dasm.as<Item>());
+    a.inv = reinterpret_cast<double *>(take(sizeof(double) * n_inv));
+    a.beta = reinterpret_cast<double *>(take(sizeof(double) * n_beta));
+    a.act = reinterpret_cast<int *>(take(sizeof(int) * 3 * ns));
+    BigSlot *ds = reinterpret_cast<BigSlot *>(take(sizeof(BigSlot) * ns));
+    int *dpre_asm = reinterpret_cast<int *>(take(sizeof(int) * pre_asm.size()));
+    int *dpre = reinterpret_cast<int *>(take(sizeof(int) * pre.size()));
+    arena.upload(slots.data(), slots.size(), ds, st);
+    arena.upload(pre_asm.data(), pre_asm.size(), dpre_asm, st);
+    arena.upload(pre.data(), pre.size(), dpre, st);
+    k_assemble<<<pre_asm[ns], 256, 0, st>>>(a, ds, dpre_asm, ns, lu ? 1 : 0);
     note_launch();
     k_big_poly<<<ns, 256, 0, st>>>(a, ds);
     note_launch();
     const size_t s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
     for (int s = 0; s < steps; ++s) {
-      const int nd = L.diag_off[s + 1] - L.diag_off[s];
-      const int nt = L.trsm_off[s + 1] - L.trsm_off[s];
-      const int nu = L.upd_off[s + 1] - L.upd_off[s];
+      const int c = cnt[s];
+      const int *pt = dpre + off[s];
+      const int *pu = pt + c + 1;
+      const int nt = pre[off[s] + c];
+      const int nu = pre[off[s] + c + 1 + c];
       if (lu) {
-        k_diag<true><<<nd, 256, s3, st>>>(a, ds, ddiag.as<int>() + L.diag_off[s], s);
-        note_launch();
-        if (nt) {
-          k_trsm<true><<<nt, 128, s2, st>>>(a, ds, dtrsm.as<Item>() + L.trsm_off[s], s);
-          note_launch();
-        }
-        if (nu) {
-          k_update<true><<<nu, 128, s2, st>>>(a, ds, dupd.as<Item>() + L.upd_off[s], s);
-          note_launch();
-        }
+        k_diag<true><<<c, 256, s3, st>>>(a, ds, s);
+        if (nt) k_trsm<true><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
+        if (nu) k_update<true><<<nu, 128, s2, st>>>(a, ds, pu, c, s);
       } else {
-        k_diag<false><<<nd, 256, s3, st>>>(a, ds, ddiag.as<int>() + L.diag_off[s], s);
-        note_launch();
-        if (nt) {
-          k_trsm<false><<<nt, 128, s2, st>>>(a, ds, dtrsm.as<Item>() + L.trsm_off[s], s);
-          note_launch();
-        }
-        if (nu) {
-          k_update<false><<<nu, 128, s2, st>>>(a, ds, dupd.as<Item>() + L.upd_off[s], s);
-          note_launch();
-        }
+        k_diag<false><<<c, 256, s3, st>>>(a, ds, s);
+        if (nt) k_trsm<false><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
+        if (nu) k_update<false><<<nu, 128, s2, st>>>(a, ds, pu, c, s);
       }
+      note_launch(1 + (nt ? 1 : 0) + (nu ? 1 : 0));
     }
     k_big_finish<<<ns, 128, 0, st>>>(a, ds);
     note_launch();
     PB_CUDA(cudaGetLastError());
-    PB_CUDA(cudaEventRecord(ev1, st));
-    PB_CUDA(cudaEventSynchronize(ev1));
-    float ms = 0.f;
-    PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-    rep.ms_factor += ms;
   }
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
 }
 
 }  // namespace pacman_b200

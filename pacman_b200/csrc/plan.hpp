@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -87,6 +88,32 @@ struct Plan {
   int64_t dropped_axis_patches = 0;
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
+};
+
+// Pinned host staging for the small host-to-device uploads of one call.  A
+// copy from pageable memory first synchronises its stream, which would stall
+// the host behind every queued kernel; copies from this arena do not.  The
+// arena is reset at the start of each call (the previous call synchronised
+// before returning), blocks outgrown in the middle of a call are released at
+// the next reset.
+class HostArena {
+ public:
+  static HostArena &get();
+  void reset();
+  void *alloc(size_t bytes);
+  template <typename T> T *upload(const T *src, size_t count, void *dst, cudaStream_t st) {
+    if (count == 0) return static_cast<T *>(dst);
+    void *h = alloc(sizeof(T) * count);
+    std::memcpy(h, src, sizeof(T) * count);
+    PB_CUDA(cudaMemcpyAsync(dst, h, sizeof(T) * count, cudaMemcpyHostToDevice, st));
+    return static_cast<T *>(dst);
+  }
+  ~HostArena();
+
+ private:
+  char *base_ = nullptr;
+  size_t cap_ = 0, used_ = 0;
+  std::vector<char *> retired_;
 };
 
 // Launch counter of this library's own kernels on the calling thread.

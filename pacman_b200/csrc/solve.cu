@@ -312,15 +312,13 @@ static void launch(int mode, const PatchArgs &a, const int *plist, int np, int u
 // shared memory use the global workspace.
 static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &patches,
                      SolveReport &rep) {
+  if (patches.empty()) return;
   cudaStream_t st = p.stream;
   for (int k : patches) {
     const double n = p.n_host[k], m = p.m_host[k];
     rep.factor_flops += (mode == kLU ? 2.0 / 3.0 : 1.0 / 3.0) * n * n * n +
                         2.0 * n * n * a.F + 2.0 * m * n * a.F;
   }
-  cudaEvent_t ev0, ev1;
-  PB_CUDA(cudaEventCreate(&ev0));
-  PB_CUDA(cudaEventCreate(&ev1));
   const int F = a.F;
   const size_t smem_cap = 200 * 1024;
   std::vector<int> order(patches);
@@ -331,11 +329,7 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
     if (smem_bytes(p.n_host[k], F, true) <= smem_cap) small.push_back(k);
     else big.push_back(k);
   }
-  DevMem list;
-  list.alloc(sizeof(int) * std::max<size_t>(order.size(), 1), st);
-  std::vector<int> host_list;
-  host_list.reserve(order.size());
-  // Small: buckets of doubling size.
+  // Small: buckets of doubling size, each launched with its own shared memory.
   size_t pos = 0;
   std::vector<std::pair<size_t, size_t>> ranges;
   while (pos < small.size()) {
@@ -349,12 +343,11 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
     ranges.emplace_back(pos, end);
     pos = end;
   }
-  for (int k : small) host_list.push_back(k);
-  for (int k : big) host_list.push_back(k);
-  if (!host_list.empty())
-    PB_CUDA(cudaMemcpyAsync(list.p, host_list.data(), sizeof(int) * host_list.size(),
-                            cudaMemcpyHostToDevice, st));
-  PB_CUDA(cudaEventRecord(ev0, st));
+  std::vector<int> host_list(small);
+  host_list.insert(host_list.end(), big.begin(), big.end());
+  DevMem list;
+  list.alloc(sizeof(int) * host_list.size(), st);
+  HostArena::get().upload(host_list.data(), host_list.size(), list.p, st);
   for (auto &r : ranges) {
     int nmax = 0;
     for (size_t i = r.first; i < r.second; ++i) nmax = std::max(nmax, p.n_host[small[i]]);
@@ -374,21 +367,13 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
     DevMem goff, gA;
     goff.alloc(sizeof(int64_t) * big.size(), st);
     gA.alloc(sizeof(double) * size_t(tot), st);
-    PB_CUDA(cudaMemcpyAsync(goff.p, offs.data(), sizeof(int64_t) * offs.size(),
-                            cudaMemcpyHostToDevice, st));
+    HostArena::get().upload(offs.data(), offs.size(), goff.p, st);
     PatchArgs b = a;
     b.gA = gA.as<double>();
     b.gAoff = goff.as<int64_t>();
     launch(mode, b, list.as<int>() + small.size(), int(big.size()), 1,
            smem_bytes(nmax, F, false), st);
   }
-  PB_CUDA(cudaEventRecord(ev1, st));
-  PB_CUDA(cudaEventSynchronize(ev1));
-  float ms = 0.f;
-  PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-  rep.ms_factor += ms;
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
 }
 
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
@@ -429,11 +414,19 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
     (p.n_host[k] > nbig ? big : small).push_back(k);
   }
   const int mode = precision == PACMAN_B200_FP64 ? kLU : kChol;
+  cudaEvent_t ev0, ev1;
+  PB_CUDA(cudaEventCreate(&ev0));
+  PB_CUDA(cudaEventCreate(&ev1));
+  PB_CUDA(cudaEventRecord(ev0, st));
   run_list(p, a, mode, small, rep);
   solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep);
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
+  PB_CUDA(cudaEventRecord(ev1, st));
   PB_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  rep.ms_factor += ms;
   std::vector<int> redo_small, redo_big;
   for (int k = 0; k < K; ++k) {
     if (p.m_host[k] == 0) continue;
@@ -442,11 +435,18 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
       (p.n_host[k] > nbig ? redo_big : redo_small).push_back(k);
   }
   rep.patches_fp64 = int64_t(small.size() + big.size());
-  if (!redo_small.empty()) run_list(p, a, kLU, redo_small, rep);
-  if (!redo_big.empty())
+  if (!redo_small.empty() || !redo_big.empty()) {
+    PB_CUDA(cudaEventRecord(ev0, st));
+    run_list(p, a, kLU, redo_small, rep);
     solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep);
-  rep.patches_fallback += int64_t(redo_small.size() + redo_big.size());
-  if (!redo_small.empty() || !redo_big.empty()) PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(cudaEventRecord(ev1, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    rep.ms_factor += ms;
+    rep.patches_fallback += int64_t(redo_small.size() + redo_big.size());
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
 }
 
 }  // namespace pacman_b200
