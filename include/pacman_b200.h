@@ -119,6 +119,25 @@ PACMAN_B200_API int pacman_b200_plan_execute(pacman_b200_plan *plan, int32_t rbf
                              double *target_values, pacman_b200_stats *stats);
 PACMAN_B200_API void pacman_b200_plan_destroy(pacman_b200_plan *plan);
 
+/* Adjoint of the transfer (no counterpart in the reference, which only
+ * evaluates the forward map).  execute_ex with PACMAN_B200_SAVE_FOR_ADJOINT
+ * keeps the per-patch coefficients of that call; plan_adjoint then applies
+ * the transpose of the (fixed-geometry, linear in the values) transfer to an
+ * upstream gradient grad_target_values [n_target x n_fields]:
+ *   grad_source_values [n_source x n_fields] = M^T grad   (may be NULL),
+ *   grad_target_points [n_target x dim]       = d <grad, out> / d targets
+ *                                               at fixed patch membership
+ *                                               (may be NULL). */
+#define PACMAN_B200_SAVE_FOR_ADJOINT 1u
+PACMAN_B200_API int pacman_b200_plan_execute_ex(pacman_b200_plan *plan, int32_t rbf_function,
+                                                const double *source_values, int32_t n_fields,
+                                                double *target_values, uint32_t flags,
+                                                pacman_b200_stats *stats);
+PACMAN_B200_API int pacman_b200_plan_adjoint(pacman_b200_plan *plan,
+                                             const double *grad_target_values,
+                                             double *grad_source_values,
+                                             double *grad_target_points);
+
 /* Geometry of a plan, for inspection and parity tests.
  * info[0] = K, info[1] = candidates, info[2] = total source memberships,
  * info[3] = total target memberships; *radius = patch radius. */

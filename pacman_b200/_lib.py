@@ -23,6 +23,7 @@ ERR_LIMIT = -6
 
 FP64 = 0
 MIXED = 1
+SAVE_FOR_ADJOINT = 1
 
 _lock = threading.Lock()
 _lib = None
@@ -77,6 +78,9 @@ SIGNATURES = {
     "pacman_b200_plan_execute": (ctypes.c_int, [
         _VP, ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.POINTER(Stats)]),
     "pacman_b200_plan_destroy": (None, [_VP]),
+    "pacman_b200_plan_execute_ex": (ctypes.c_int, [
+        _VP, ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_uint32, ctypes.POINTER(Stats)]),
+    "pacman_b200_plan_adjoint": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
     "pacman_b200_plan_info": (ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_int64)]),
     "pacman_b200_plan_centers": (ctypes.c_int, [_VP, _VP]),
     "pacman_b200_plan_patch_lists": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP]),

@@ -199,7 +199,7 @@ int create_plan(int32_t dim, const double *src, int64_t n, const double *tgt, in
 }
 
 int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t F, double *out,
-                 pacman_b200_stats *stats) {
+                 pacman_b200_stats *stats, uint32_t flags = 0) {
   if (!h) return fail(PACMAN_B200_ERR_INVALID, "plan is null");
   if (int rc = check_basis(basis)) return rc;
   Plan &p = h->p;
@@ -217,6 +217,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
     PB_CUDA(cudaEventCreate(&e2));
     PB_CUDA(cudaEventRecord(e0, st));
     const int64_t launches0 = launch_counter();
+    p.saved_basis = -1;
     SolveReport rep;
     if (p.m > 0) {
       const bool out_dev = is_device_ptr(out, p.device);
@@ -233,7 +234,8 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
         InBuf v;
         v.stage(vals, size_t(p.n) * F, p.device, st);
         p.local.alloc(sizeof(double) * size_t(std::max<int64_t>(p.tnnz, 1)) * F, st);
-        solve_patches(p, basis, v.ptr, F, p.opts.precision, p.local.as<double>(), rep);
+        solve_patches(p, basis, v.ptr, F, p.opts.precision, p.local.as<double>(), rep,
+                      (flags & PACMAN_B200_SAVE_FOR_ADJOINT) != 0);
         PB_CUDA(cudaEventRecord(e1, st));
         pu_gather(p, p.local.as<double>(), F, o);
       }
@@ -246,6 +248,10 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
     PB_CUDA(cudaEventRecord(e2, st));
     PB_CUDA(cudaEventSynchronize(e2));
     PB_CUDA(cudaGetLastError());
+    if (flags & PACMAN_B200_SAVE_FOR_ADJOINT) {
+      p.saved_basis = basis;
+      p.saved_F = F;
+    }
     if (stats) {
       float ms_solve = 0.f, ms_total = 0.f;
       cudaEventElapsedTime(&ms_solve, e0, e1);
@@ -310,6 +316,51 @@ int pacman_b200_plan_execute(pacman_b200_plan *plan, int32_t basis, const double
                              int32_t F, double *out, pacman_b200_stats *stats) {
   g_last_error.clear();
   return execute_plan(plan, basis, vals, F, out, stats);
+}
+
+int pacman_b200_plan_execute_ex(pacman_b200_plan *plan, int32_t basis, const double *vals,
+                                int32_t F, double *out, uint32_t flags,
+                                pacman_b200_stats *stats) {
+  g_last_error.clear();
+  return execute_plan(plan, basis, vals, F, out, stats, flags);
+}
+
+int pacman_b200_plan_adjoint(pacman_b200_plan *plan, const double *grad_out, double *grad_values,
+                             double *grad_targets) {
+  g_last_error.clear();
+  if (!plan) return fail(PACMAN_B200_ERR_INVALID, "plan is null");
+  Plan &p = plan->p;
+  if (p.saved_basis < 0)
+    return fail(PACMAN_B200_ERR_INVALID,
+                "the adjoint needs a previous execute with PACMAN_B200_SAVE_FOR_ADJOINT");
+  if (!grad_out && p.m > 0) return fail(PACMAN_B200_ERR_INVALID, "grad_target_values is null");
+  try {
+    DeviceScope ds(p.device);
+    HostArena::get().reset();
+    cudaStream_t st = p.stream;
+    const int F = p.saved_F;
+    InBuf g;
+    g.stage(grad_out, size_t(p.m) * F, p.device, st);
+    DevMem gv, gt;
+    double *dv = grad_values, *dt = grad_targets;
+    const bool hv = grad_values && !is_device_ptr(grad_values, p.device);
+    const bool ht = grad_targets && !is_device_ptr(grad_targets, p.device);
+    if (hv) {
+      gv.alloc(sizeof(double) * std::max<int64_t>(p.n, 1) * F, st);
+      dv = gv.as<double>();
+    }
+    if (ht) {
+      gt.alloc(sizeof(double) * std::max<int64_t>(p.m, 1) * p.dim, st);
+      dt = gt.as<double>();
+    }
+    adjoint(p, g.ptr, dv, dt);
+    if (hv) PB_CUDA(cudaMemcpyAsync(grad_values, dv, sizeof(double) * p.n * F, cudaMemcpyDeviceToHost, st));
+    if (ht) PB_CUDA(cudaMemcpyAsync(grad_targets, dt, sizeof(double) * p.m * p.dim, cudaMemcpyDeviceToHost, st));
+    PB_CUDA(cudaStreamSynchronize(st));
+  } catch (const Error &e) {
+    return fail(e.code, e.msg);
+  }
+  return 0;
 }
 
 void pacman_b200_plan_destroy(pacman_b200_plan *plan) {

@@ -225,7 +225,16 @@ struct BigArgs {
   int F;
   int dim;
   int basis;
+  int mode;            // kBigForward, kBigForwardSave or kBigAdjoint
+  double *alpha_out;   // forward + save: RBF coefficients per (patch, source)
+  double *beta_out;    // forward + save: K x 4*kMaxF
+  int *act_out;        // forward + save: K x 3
+  const double *h;     // adjoint: weighted upstream gradient per (patch, target)
+  double *g_out;       // adjoint: result per (patch, source)
+  double *red_out;     // adjoint: per slot reduced moments (kRedVals)
 };
+
+
 
 // Fills one 64 x 64 tile of an augmented matrix.
 __global__ void __launch_bounds__(256)
@@ -300,7 +309,8 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
 #pragma unroll
   for (int v = 0; v < kRedVals - 6; ++v) acc[v] = 0.0;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  const int nred = 10 + 4 * F;
+  const int Fm = (a.mode == kBigAdjoint) ? 0 : F;
+  const int nred = 10 + 4 * Fm;
   for (int i = tid; i < n; i += blockDim.x) {
     const int id = a.sidx[s0 + i];
     const double4 p = a.src[id];
@@ -317,7 +327,7 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
     acc[9] += q[3] * q[3];
 #pragma unroll
     for (int f = 0; f < kMaxF; ++f)
-      if (f < F) {
+      if (f < Fm) {
         const double b = a.vals[int64_t(id) * F + f];
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
@@ -362,6 +372,10 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
     redf[tid] = s;
   }
   __syncthreads();
+  if (a.mode == kBigAdjoint) {
+    if (tid < nred + 6) a.red_out[int64_t(blockIdx.x) * kRedVals + tid] = redf[tid];
+    return;
+  }
   if (tid == 0) {
     int act[3];
     const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
@@ -369,6 +383,10 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
     a.status[sl.k] = dropped ? 1 : 0;
     for (int v = 0; v < 4 * kMaxF; ++v) a.beta[blockIdx.x * 4 * kMaxF + v] = beta_s[v];
     for (int d = 0; d < 3; ++d) a.act[blockIdx.x * 3 + d] = act[d];
+    if (a.mode == kBigForwardSave) {
+      for (int v = 0; v < 4 * kMaxF; ++v) a.beta_out[int64_t(sl.k) * 4 * kMaxF + v] = beta_s[v];
+      for (int d = 0; d < 3; ++d) a.act_out[int64_t(sl.k) * 3 + d] = act[d];
+    }
   }
   __syncthreads();
   double *rcol = a.W + sl.base + int64_t(sl.T) * TB;
@@ -563,6 +581,168 @@ __global__ void k_big_finish(BigArgs a, const BigSlot *__restrict__ slots) {
   if (bad) atomicOr(&a.status[sl.k], 2);
 }
 
+
+// Adjoint right-hand sides c = E^T h of one slot, in its residual column.
+__global__ void __launch_bounds__(256) k_big_adj_rhs(BigArgs a, const BigSlot *__restrict__ slots) {
+  const BigSlot sl = slots[blockIdx.x];
+  const int F = a.F;
+  const int64_t s0 = a.soff[sl.k], t0 = a.toff[sl.k];
+  double *rcol = a.W + sl.base + int64_t(sl.T) * TB;
+  for (int j = threadIdx.x; j < sl.n; j += blockDim.x) {
+    const double4 x = a.src[a.sidx[s0 + j]];
+    double cs[kMaxF];
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) cs[f] = 0.0;
+    for (int i = 0; i < sl.m; ++i) {
+      const double4 y = a.tgt[a.tidx[t0 + i]];
+      const double ph =
+          wendland<double>(a.basis, __dsqrt_rn(sqdist3(y.x, y.y, y.z, x.x, x.y, x.z)), a.rinv);
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f)
+        if (f < F) cs[f] = __fma_rn(ph, a.h[(t0 + i) * F + f], cs[f]);
+    }
+    for (int f = 0; f < F; ++f) rcol[int64_t(j) * sl.ld + f] = cs[f];
+  }
+}
+
+// Backward sweep after the elimination: the residual column holds
+// y = L^{-1} r; solves U z = y (LU) or L^T z = y (Cholesky) tile row by tile
+// row from the last, in place.  In forward-save mode z (the RBF coefficients
+// alpha) is also written per (patch, source).
+template <bool LU>
+__global__ void __launch_bounds__(256) k_back_sweep(BigArgs a, const BigSlot *__restrict__ slots) {
+  __shared__ double tile[TB][TB + 1];
+  __shared__ double zt[TB][kMaxF];
+  __shared__ double acc[TB][kMaxF];
+  const BigSlot sl = slots[blockIdx.x];
+  const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ld = sl.ld;
+  double *W = a.W + sl.base;
+  double *rcol = W + int64_t(sl.T) * TB;
+  for (int s = sl.T - 1; s >= 0; --s) {
+    for (int e = tid; e < TB * F; e += blockDim.x) {
+      const int r = e / F, f = e % F;
+      acc[r][f] = rcol[int64_t(s * TB + r) * ld + f];
+    }
+    for (int t = s + 1; t < sl.T; ++t) {
+      const double *g = LU ? W + int64_t(s) * TB * ld + int64_t(t) * TB
+                           : W + int64_t(t) * TB * ld + int64_t(s) * TB;
+      __syncthreads();
+      for (int e = tid; e < TB * TB; e += blockDim.x) tile[e >> 6][e & 63] = g[int64_t(e >> 6) * ld + (e & 63)];
+      for (int e = tid; e < TB * F; e += blockDim.x) {
+        const int r = e / F, f = e % F;
+        zt[r][f] = rcol[int64_t(t * TB + r) * ld + f];
+      }
+      __syncthreads();
+      const int o = tid & 63;
+      for (int f = tid >> 6; f < F; f += 4) {
+        double sum = 0.0;
+        for (int c = 0; c < TB; ++c) sum = __fma_rn(LU ? tile[o][c] : tile[c][o], zt[c][f], sum);
+        acc[o][f] -= sum;
+      }
+    }
+    __syncthreads();
+    const double *gd = W + int64_t(s) * TB * ld + int64_t(s) * TB;
+    for (int e = tid; e < TB * TB; e += blockDim.x) tile[e >> 6][e & 63] = gd[int64_t(e >> 6) * ld + (e & 63)];
+    __syncthreads();
+    if (warp < F) {
+      const int f = warp;
+      for (int i = TB - 1; i >= 0; --i) {
+        double sum = 0.0;
+        for (int j = i + 1 + lane; j < TB; j += 32) sum = __fma_rn(LU ? tile[i][j] : tile[j][i], acc[j][f], sum);
+        sum = warp_sum(sum);
+        if (lane == 0) acc[i][f] = (acc[i][f] - sum) / tile[i][i];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < TB * F; e += blockDim.x) {
+      const int r = e / F, f = e % F;
+      rcol[int64_t(s * TB + r) * ld + f] = acc[r][f];
+      const int j = s * TB + r;
+      if (a.mode == kBigForwardSave && j < sl.n) a.alpha_out[(a.soff[sl.k] + j) * F + f] = acc[r][f];
+    }
+    __syncthreads();
+  }
+}
+
+// Adjoint result of one slot: g = z - Q' G'^{-1} (Q'^T z - V'^T h).
+__global__ void __launch_bounds__(256) k_big_adj_finish(BigArgs a, const BigSlot *__restrict__ slots) {
+  __shared__ double red[8][8];
+  __shared__ double corr[4 * kMaxF];
+  const BigSlot sl = slots[blockIdx.x];
+  const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t s0 = a.soff[sl.k], t0 = a.toff[sl.k];
+  const double4 c = a.centers[sl.k];
+  const double shift[3] = {c.x, c.y, c.z};
+  const double *rcol = a.W + sl.base + int64_t(sl.T) * TB;
+  __shared__ int S_s[4], pv_s;
+  __shared__ double R_s[4][4];
+  if (tid == 0) {
+    const double *redf = a.red_out + int64_t(blockIdx.x) * kRedVals;
+    int S[4], pv;
+    double R[4][4];
+    poly_axes(redf, a.dim, shift, redf + 10, redf + 13, S, pv, R);
+    for (int i = 0; i < 4; ++i) {
+      S_s[i] = S[i];
+      for (int j = 0; j < 4; ++j) R_s[i][j] = R[i][j];
+    }
+    pv_s = pv;
+  }
+  __syncthreads();
+  for (int f = 0; f < F; ++f) {
+    double u[4] = {0, 0, 0, 0}, v[4] = {0, 0, 0, 0};
+    for (int j = tid; j < sl.n; j += blockDim.x) {
+      const double4 x = a.src[a.sidx[s0 + j]];
+      const double z = rcol[int64_t(j) * sl.ld + f];
+      const double q[4] = {1.0, x.x - shift[0], x.y - shift[1], x.z - shift[2]};
+      for (int c2 = 0; c2 < 4; ++c2) u[c2] += q[c2] * z;
+    }
+    for (int i = tid; i < sl.m; i += blockDim.x) {
+      const double4 y = a.tgt[a.tidx[t0 + i]];
+      const double hv = a.h[(t0 + i) * F + f];
+      const double q[4] = {1.0, y.x - shift[0], y.y - shift[1], y.z - shift[2]};
+      for (int c2 = 0; c2 < 4; ++c2) v[c2] += q[c2] * hv;
+    }
+    for (int c2 = 0; c2 < 4; ++c2) {
+      const double su = warp_sum(u[c2]), sv = warp_sum(v[c2]);
+      if (lane == 0) {
+        red[warp][c2] = su;
+        red[warp][4 + c2] = sv;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const int pv = pv_s;
+      double rhs[4], x[4];
+      for (int i = 0; i < pv; ++i) {
+        double su = 0.0, sv = 0.0;
+        for (int w = 0; w < 8; ++w) {
+          su += red[w][S_s[i]];
+          sv += red[w][4 + S_s[i]];
+        }
+        rhs[i] = su - sv;
+      }
+      gram_solve(R_s, pv, rhs, x);
+      for (int c2 = 0; c2 < 4; ++c2) corr[4 * f + c2] = 0.0;
+      for (int i = 0; i < pv; ++i) corr[4 * f + S_s[i]] = x[i];
+    }
+    __syncthreads();
+  }
+  int bad = 0;
+  for (int j = tid; j < sl.n; j += blockDim.x) {
+    const double4 x = a.src[a.sidx[s0 + j]];
+    const double q[4] = {1.0, x.x - shift[0], x.y - shift[1], x.z - shift[2]};
+    for (int f = 0; f < F; ++f) {
+      double g = rcol[int64_t(j) * sl.ld + f];
+      for (int c2 = 0; c2 < 4; ++c2) g -= q[c2] * corr[4 * f + c2];
+      if (!isfinite(g)) bad = 1;
+      a.g_out[(s0 + j) * F + f] = g;
+    }
+  }
+  if (bad) atomicOr(&a.status[sl.k], 2);
+}
+
 // ---------------------------------------------------------------------------
 // Host orchestration
 // ---------------------------------------------------------------------------
@@ -602,7 +782,8 @@ static void set_smem_attributes() {
 // workspace of each wave is released stream-ordered after its kernels, so the
 // next wave reuses it.
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
-               const std::vector<int> &patches, double *local, int *status, SolveReport &rep) {
+               const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
+               const BigExtra &extra) {
   if (patches.empty()) return;
   cudaStream_t st = p.stream;
   set_smem_attributes();
@@ -628,6 +809,14 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   a.F = F;
   a.dim = p.dim;
   a.basis = basis;
+  a.mode = extra.mode;
+  a.alpha_out = extra.alpha_out;
+  a.beta_out = extra.beta_out;
+  a.act_out = extra.act_out;
+  a.h = extra.h;
+  a.g_out = extra.g_out;
+  const bool adjoint = extra.mode == kBigAdjoint;
+  if (adjoint) lu = false;
   HostArena &arena = HostArena::get();
   size_t pos = 0;
   while (pos < order.size()) {
@@ -637,12 +826,12 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     while (pos < order.size()) {
       const int k = order[pos];
       const int n = p.n_host[k], m = p.m_host[k];
-      const size_t d = slot_doubles(n, m);
+      const size_t d = slot_doubles(n, adjoint ? 0 : m);
       if (!slots.empty() && tot + d > budget) break;
       BigSlot q{};
       q.base = int64_t(tot);
       q.T = (n + TB - 1) / TB;
-      q.TE = (m + TB - 1) / TB;
+      q.TE = adjoint ? 0 : (m + TB - 1) / TB;
       q.ld = (q.T + 1) * TB;
       q.k = k;
       q.n = n;
@@ -686,7 +875,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     DevMem dW, dsmall;
     dW.alloc(sizeof(double) * tot, st);
     const size_t n_inv = size_t(2) * TB * TB * ns, n_beta = size_t(4) * kMaxF * ns;
-    const size_t bytes_small = sizeof(double) * (n_inv + n_beta) + sizeof(int) * 3 * ns +
+    const size_t n_red = size_t(kRedVals) * ns;
+    const size_t bytes_small = sizeof(double) * (n_inv + n_beta + n_red) + sizeof(int) * 3 * ns +
                                sizeof(BigSlot) * ns + sizeof(int) * (pre_asm.size() + pre.size()) +
                                64;
     dsmall.alloc(bytes_small, st);
@@ -700,6 +890,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     a.inv = reinterpret_cast<double *>(take(sizeof(double) * n_inv));
     a.beta = reinterpret_cast<double *>(take(sizeof(double) * n_beta));
     a.act = reinterpret_cast<int *>(take(sizeof(int) * 3 * ns));
+    a.red_out = reinterpret_cast<double *>(take(sizeof(double) * n_red));
     BigSlot *ds = reinterpret_cast<BigSlot *>(take(sizeof(BigSlot) * ns));
     int *dpre_asm = reinterpret_cast<int *>(take(sizeof(int) * pre_asm.size()));
     int *dpre = reinterpret_cast<int *>(take(sizeof(int) * pre.size()));
@@ -710,6 +901,10 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     note_launch();
     k_big_poly<<<ns, 256, 0, st>>>(a, ds);
     note_launch();
+    if (adjoint) {
+      k_big_adj_rhs<<<ns, 256, 0, st>>>(a, ds);
+      note_launch();
+    }
     const size_t s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
     for (int s = 0; s < steps; ++s) {
       const int c = cnt[s];
@@ -728,8 +923,19 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       }
       note_launch(1 + (nt ? 1 : 0) + (nu ? 1 : 0));
     }
-    k_big_finish<<<ns, 128, 0, st>>>(a, ds);
-    note_launch();
+    if (!adjoint) {
+      k_big_finish<<<ns, 128, 0, st>>>(a, ds);
+      note_launch();
+    }
+    if (adjoint || extra.mode == kBigForwardSave) {
+      if (lu) k_back_sweep<true><<<ns, 256, 0, st>>>(a, ds);
+      else k_back_sweep<false><<<ns, 256, 0, st>>>(a, ds);
+      note_launch();
+    }
+    if (adjoint) {
+      k_big_adj_finish<<<ns, 256, 0, st>>>(a, ds);
+      note_launch();
+    }
     PB_CUDA(cudaGetLastError());
   }
 }

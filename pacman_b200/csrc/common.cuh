@@ -79,6 +79,27 @@ __device__ __forceinline__ T wendland(int basis, T r, T rinv) {
   return mask * v;
 }
 
+// d phi / d p of the Wendland bases (p = r / rho), zero outside the support.
+// C0: -2(1-p); C2: -20p(1-p)^3; C4: -56p(1-p)^5(5p+1);
+// C6: -22p(1-p)^7(16p^2+7p+1); C8: -78p(1-p)^9(231p^3+159p^2+45p+5).
+__device__ __forceinline__ double wendland_dp(int basis, double p) {
+  if (!(p >= 0.0 && p < 1.0)) return 0.0;
+  const double q = 1.0 - p;
+  const double q2 = q * q;
+  switch (basis) {
+  case kWendlandC0:
+    return -2.0 * q;
+  case kWendlandC2:
+    return -20.0 * p * q2 * q;
+  case kWendlandC4:
+    return -56.0 * p * (q2 * q2 * q) * fma(5.0, p, 1.0);
+  case kWendlandC6:
+    return -22.0 * p * (q2 * q2 * q2 * q) * fma(fma(16.0, p, 7.0), p, 1.0);
+  default:
+    return -78.0 * p * (q2 * q2 * q2 * q2 * q) * fma(fma(fma(231.0, p, 159.0), p, 45.0), p, 5.0);
+  }
+}
+
 // Monotone uint64 image of a double (total order on non-NaN values), used for
 // exact, order-independent atomic min/max reductions.
 __device__ __forceinline__ unsigned long long dbl_to_ordered(double x) {

@@ -86,6 +86,12 @@ struct Plan {
   DevMem status;                    // per patch status words
   double ms_geometry = 0.0;
   int64_t dropped_axis_patches = 0;
+  // State saved by an execute for the adjoint (pacman_b200_plan_adjoint).
+  int saved_basis = -1, saved_F = 0;
+  DevMem alpha;              // RBF coefficients, source-membership order x F
+  DevMem beta;               // K x 4*8 polynomial coefficients
+  DevMem act;                // K x 3 active axes
+  DevMem src_t_off, src_t_pos;  // sources -> (patch, slot) transpose of the membership lists
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
 };
@@ -131,6 +137,21 @@ struct SolveReport {
   double factor_flops = 0.0;  // their algorithmic FLOPs
 };
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
-                   double *local_dev, SolveReport &rep);
+                   double *local_dev, SolveReport &rep, bool save_state = false);
+
+// Extra inputs / outputs of the blocked engine beyond the forward transfer.
+enum { kBigForward = 0, kBigForwardSave = 1, kBigAdjoint = 2 };
+struct BigExtra {
+  int mode = kBigForward;
+  double *alpha_out = nullptr;  // forward + save
+  double *beta_out = nullptr;
+  int *act_out = nullptr;
+  const double *h = nullptr;    // adjoint
+  double *g_out = nullptr;
+};
+
+// adjoint.cu
+void adjoint(Plan &p, const double *grad_out_dev, double *grad_values_dev,
+             double *grad_targets_dev);
 
 }  // namespace pacman_b200

@@ -84,14 +84,9 @@ __device__ inline bool small_chol(const double G[4][4], int pv, double R[4][4]) 
   return true;
 }
 
-// Polynomial block of one patch from the reduced moments (one thread).
-// red: [0]=n, [1..3]=sum dx, [4..9]=sum dx_a dx_b (aa,ab,ac,bb,bc,cc),
-//      [10 + 4f + c] = sum q_c b_f, [10+4F .. +6] = min x,y,z, max x,y,z.
-// Writes beta[4 x F] (uncentred basis, zero for dropped axes), act[0..2]
-// (active axis ids, -1 terminated) and returns the dropped flag.
-__device__ inline int poly_block(const double *red, int F, int dim, const double *shift,
-                          double *beta, int *act) {
-  double G[4][4];
+// Gram matrix of the centred monomials from the reduced moments.
+// red: [0]=n, [1..3]=sum dx, [4..9]=sum dx_a dx_b (aa,ab,ac,bb,bc,cc).
+__device__ inline void gram_from_moments(const double *red, double G[4][4]) {
   G[0][0] = red[0];
   G[0][1] = G[1][0] = red[1];
   G[0][2] = G[2][0] = red[2];
@@ -102,14 +97,22 @@ __device__ inline int poly_block(const double *red, int F, int dim, const double
   G[2][2] = red[7];
   G[2][3] = G[3][2] = red[8];
   G[3][3] = red[9];
-  const double *mn = red + 10 + 4 * F;
-  const double *mx = mn + 3;
+}
+
+// Active polynomial terms of a patch (SerialFillQ's condition loop,
+// serial_ops.hpp:108-139): S[0..pv) are monomial ids (0 = constant, a + 1 =
+// axis a), R is the Cholesky factor of the centred Gram matrix restricted to
+// S.  mn / mx are the coordinate ranges used to pick the axis to drop.
+// Returns 1 if an axis was dropped.
+__device__ inline int poly_axes(const double *red, int dim, const double *shift,
+                                const double *mn, const double *mx, int S[4], int &pv_out,
+                                double R[4][4]) {
+  double G[4][4];
+  gram_from_moments(red, G);
   bool active[3] = {dim > 0, dim > 1, dim > 2};
   int pv = dim + 1;
   int dropped = 0;
   const double n = red[0];
-  int S[4];
-  double R[4][4];
   bool have_R = false;
   for (;;) {
     int c = 0;
@@ -160,24 +163,45 @@ __device__ inline int poly_block(const double *red, int F, int dim, const double
       for (int j = 0; j < pv; ++j) Gs[i][j] = G[S[i]][S[j]];
     small_chol(Gs, pv, R);
   }
+  pv_out = pv;
+  return dropped;
+}
+
+// Solves (R^T R) x = rhs for the pv active terms.
+__device__ inline void gram_solve(const double R[4][4], int pv, const double *rhs, double *x) {
+  double z[4];
+  for (int i = 0; i < pv; ++i) {
+    double s = rhs[i];
+    for (int k = 0; k < i; ++k) s -= R[k][i] * z[k];
+    z[i] = s / R[i][i];
+  }
+  for (int i = pv - 1; i >= 0; --i) {
+    double s = z[i];
+    for (int k = i + 1; k < pv; ++k) s -= R[i][k] * x[k];
+    x[i] = s / R[i][i];
+  }
+}
+
+// Polynomial block of one patch from the reduced moments (one thread).
+// red: moments as above, [10 + 4f + c] = sum q_c b_f, [10+4F .. +6] = min
+// x,y,z, max x,y,z.  Writes beta[4 x F] (uncentred basis, zero for dropped
+// axes), act[0..2] (active axis ids, -1 terminated) and returns the dropped
+// flag.
+__device__ inline int poly_block(const double *red, int F, int dim, const double *shift,
+                                 double *beta, int *act) {
+  const double *mn = red + 10 + 4 * F;
+  const double *mx = mn + 3;
+  int S[4], pv;
+  double R[4][4];
+  const int dropped = poly_axes(red, dim, shift, mn, mx, S, pv, R);
   int na = 0;
-  for (int a = 0; a < dim; ++a)
-    if (active[a]) act[na++] = a;
+  for (int i = 1; i < pv; ++i) act[na++] = S[i] - 1;
   for (int a = na; a < 3; ++a) act[a] = -1;
   for (int f = 0; f < F; ++f) {
     const double *h = red + 10 + 4 * f;
-    double z[4], bp[4];
-    // R^T z = h_S, R bp = z.
-    for (int i = 0; i < pv; ++i) {
-      double s = h[S[i]];
-      for (int k = 0; k < i; ++k) s -= R[k][i] * z[k];
-      z[i] = s / R[i][i];
-    }
-    for (int i = pv - 1; i >= 0; --i) {
-      double s = z[i];
-      for (int k = i + 1; k < pv; ++k) s -= R[i][k] * bp[k];
-      bp[i] = s / R[i][i];
-    }
+    double hs[4], bp[4];
+    for (int i = 0; i < pv; ++i) hs[i] = h[S[i]];
+    gram_solve(R, pv, hs, bp);
     double b0 = bp[0];
     for (int i = 1; i < pv; ++i) b0 -= shift[S[i] - 1] * bp[i];
     beta[4 * f + 0] = b0;
@@ -186,5 +210,4 @@ __device__ inline int poly_block(const double *red, int F, int dim, const double
   }
   return dropped;
 }
-
 }  // namespace pacman_b200

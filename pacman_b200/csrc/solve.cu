@@ -27,7 +27,11 @@
 
 namespace pacman_b200 {
 
-enum SolveMode { kLU = 0, kChol = 1 };
+enum SolveMode {
+  kLU = 0,   // forward, unpivoted LU (the reference algorithm)
+  kChol = 1, // forward, Cholesky
+  kAdj = 2,  // transpose (adjoint) solve with Cholesky: g = z - Q'G'^{-1}(Q'^T z - V'^T h)
+};
 
 enum PatchStatus : int {
   kStatusDropped = 1,     // the polynomial block lost at least one axis
@@ -52,6 +56,11 @@ struct PatchArgs {
   int F;
   int dim;
   int basis;
+  double *alpha_out;      // forward: RBF coefficients per (patch, source), or null
+  double *beta_out;       // forward: polynomial coefficients, K x 4*kMaxF, or null
+  int *act_out;           // forward: active axes, K x 3, or null
+  const double *h;        // adjoint: weighted upstream gradient per (patch, target)
+  double *g_out;          // adjoint: result per (patch, source)
 };
 
 constexpr int kSolveThreads = 256;
@@ -86,7 +95,8 @@ __global__ void __launch_bounds__(kSolveThreads)
   const double4 c = a.centers[k];
   const double shift[3] = {c.x, c.y, c.z};
   double acc[kRedVals - 6];
-  const int nred = 10 + 4 * F;
+  const int Fm = (MODE == kAdj) ? 0 : F;  // value moments only for the forward fit
+  const int nred = 10 + 4 * Fm;
 #pragma unroll
   for (int v = 0; v < kRedVals - 6; ++v) acc[v] = 0.0;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -109,7 +119,7 @@ __global__ void __launch_bounds__(kSolveThreads)
     acc[9] += q[3] * q[3];
 #pragma unroll
     for (int f = 0; f < kMaxF; ++f) {
-      if (f < F) {
+      if (f < Fm) {
         const double b = a.vals[int64_t(id) * F + f];
         A[int64_t(i) * lda + n + f] = b;
 #pragma unroll
@@ -154,22 +164,54 @@ __global__ void __launch_bounds__(kSolveThreads)
     redf[tid] = s;
   }
   __syncthreads();
+  __shared__ int S_s[4], pv_s;
+  __shared__ double R_s[4][4];
   if (tid == 0) {
-    int act[3];
-    const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
-    for (int d = 0; d < 3; ++d) act_s[d] = act[d];
-    flag_s = dropped ? kStatusDropped : 0;
+    if (MODE == kAdj) {
+      int S[4], pv;
+      double R[4][4];
+      const int dropped = poly_axes(redf, a.dim, shift, redf + nred, redf + nred + 3, S, pv, R);
+      for (int i = 0; i < 4; ++i) {
+        S_s[i] = S[i];
+        for (int j = 0; j < 4; ++j) R_s[i][j] = R[i][j];
+      }
+      pv_s = pv;
+      flag_s = dropped ? kStatusDropped : 0;
+    } else {
+      int act[3];
+      const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
+      for (int d = 0; d < 3; ++d) act_s[d] = act[d];
+      flag_s = dropped ? kStatusDropped : 0;
+    }
   }
   __syncthreads();
 
-  // Residual r = b - Q beta (serial_ops.hpp:149-185, gemv + vector sub).
-  for (int i = tid; i < n; i += kSolveThreads) {
-    const double pc[3] = {xs[i], ys[i], zs[i]};
-    for (int f = 0; f < F; ++f) {
-      double t = beta_s[4 * f];
-      for (int j = 0; j < 3; ++j)
-        if (act_s[j] >= 0) t = __fma_rn(pc[act_s[j]], beta_s[4 * f + 1 + j], t);
-      A[int64_t(i) * lda + n + f] -= t;
+  if (MODE == kAdj) {
+    // Right-hand sides c = E^T h, E_ij = phi(|y_i - x_j|).
+    for (int j = tid; j < n; j += kSolveThreads) {
+      double cs[kMaxF];
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f) cs[f] = 0.0;
+      for (int i = 0; i < m; ++i) {
+        const double4 y = a.tgt[a.tidx[t0 + i]];
+        const double ph =
+            wendland<double>(a.basis, __dsqrt_rn(sqdist3(y.x, y.y, y.z, xs[j], ys[j], zs[j])), a.rinv);
+#pragma unroll
+        for (int f = 0; f < kMaxF; ++f)
+          if (f < F) cs[f] = __fma_rn(ph, a.h[(t0 + i) * F + f], cs[f]);
+      }
+      for (int f = 0; f < F; ++f) A[int64_t(j) * lda + n + f] = cs[f];
+    }
+  } else {
+    // Residual r = b - Q beta (serial_ops.hpp:149-185, gemv + vector sub).
+    for (int i = tid; i < n; i += kSolveThreads) {
+      const double pc[3] = {xs[i], ys[i], zs[i]};
+      for (int f = 0; f < F; ++f) {
+        double t = beta_s[4 * f];
+        for (int j = 0; j < 3; ++j)
+          if (act_s[j] >= 0) t = __fma_rn(pc[act_s[j]], beta_s[4 * f + 1 + j], t);
+        A[int64_t(i) * lda + n + f] -= t;
+      }
     }
   }
   // A_ij = phi(|x_i - x_j|) (TeamFillA, team_ops.hpp:35-52): warp per row,
@@ -250,6 +292,69 @@ __global__ void __launch_bounds__(kSolveThreads)
   }
   __syncthreads();
 
+  if (MODE == kAdj) {
+    // g = z - Q' G'^{-1} (Q'^T z - V'^T h), centred monomials q' = [1, x - c].
+    __shared__ double corr[4 * kMaxF];
+    for (int f = 0; f < F; ++f) {
+      double u[4] = {0, 0, 0, 0}, v[4] = {0, 0, 0, 0};
+      for (int j = tid; j < n; j += kSolveThreads) {
+        const double z = A[int64_t(j) * lda + n + f];
+        const double q[4] = {1.0, xs[j] - shift[0], ys[j] - shift[1], zs[j] - shift[2]};
+        for (int c2 = 0; c2 < 4; ++c2) u[c2] += q[c2] * z;
+      }
+      for (int i = tid; i < m; i += kSolveThreads) {
+        const double4 y = a.tgt[a.tidx[t0 + i]];
+        const double hv = a.h[(t0 + i) * F + f];
+        const double q[4] = {1.0, y.x - shift[0], y.y - shift[1], y.z - shift[2]};
+        for (int c2 = 0; c2 < 4; ++c2) v[c2] += q[c2] * hv;
+      }
+      for (int c2 = 0; c2 < 4; ++c2) {
+        const double su = warp_sum(u[c2]), sv = warp_sum(v[c2]);
+        if (lane == 0) {
+          red[warp][c2] = su;
+          red[warp][4 + c2] = sv;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        const int pv = pv_s;
+        double rhs[4], x[4];
+        for (int i = 0; i < pv; ++i) {
+          double su = 0.0, sv = 0.0;
+          for (int w = 0; w < kWarps; ++w) {
+            su += red[w][S_s[i]];
+            sv += red[w][4 + S_s[i]];
+          }
+          rhs[i] = su - sv;
+        }
+        gram_solve(R_s, pv, rhs, x);
+        for (int c2 = 0; c2 < 4; ++c2) corr[4 * f + c2] = 0.0;
+        for (int i = 0; i < pv; ++i) corr[4 * f + S_s[i]] = x[i];
+      }
+      __syncthreads();
+    }
+    int nonfinite = 0;
+    for (int j = tid; j < n; j += kSolveThreads) {
+      const double q[4] = {1.0, xs[j] - shift[0], ys[j] - shift[1], zs[j] - shift[2]};
+      for (int f = 0; f < F; ++f) {
+        double g = A[int64_t(j) * lda + n + f];
+        for (int c2 = 0; c2 < 4; ++c2) g -= q[c2] * corr[4 * f + c2];
+        if (!isfinite(g)) nonfinite = 1;
+        a.g_out[(s0 + j) * F + f] = g;
+      }
+    }
+    if (nonfinite) atomicOr(&flag_s, kStatusNonFinite);
+    __syncthreads();
+    if (tid == 0) a.status[k] = flag_s;
+    return;
+  }
+  if (a.alpha_out) {
+    for (int j = tid; j < n; j += kSolveThreads)
+      for (int f = 0; f < F; ++f) a.alpha_out[(s0 + j) * F + f] = A[int64_t(j) * lda + n + f];
+    if (tid < 4 * kMaxF) a.beta_out[int64_t(k) * 4 * kMaxF + tid] = beta_s[tid];
+    if (tid < 3) a.act_out[int64_t(k) * 3 + tid] = act_s[tid];
+  }
+
   // local = E alpha + V beta (solver.hpp:270-273), warp per target.
   int nonfinite = 0;
   for (int i = warp; i < m; i += kWarps) {
@@ -297,6 +402,11 @@ static void launch(int mode, const PatchArgs &a, const int *plist, int np, int u
     PB_CUDA(cudaFuncSetAttribute(k_patch_solve<kLU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)));
     k_patch_solve<kLU><<<np, kSolveThreads, smem, st>>>(a, plist, np, use_global);
+    note_launch();
+  } else if (mode == kAdj) {
+    PB_CUDA(cudaFuncSetAttribute(k_patch_solve<kAdj>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_patch_solve<kAdj><<<np, kSolveThreads, smem, st>>>(a, plist, np, use_global);
     note_launch();
   } else {
     PB_CUDA(cudaFuncSetAttribute(k_patch_solve<kChol>,
@@ -377,7 +487,8 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
 }
 
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
-               const std::vector<int> &patches, double *local, int *status, SolveReport &rep);
+               const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
+               const BigExtra &extra);
 
 // Patches above this size use the blocked engine (blocked.cu).
 static int big_threshold() {
@@ -386,13 +497,29 @@ static int big_threshold() {
 }
 
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
-                   double *local_dev, SolveReport &rep) {
+                   double *local_dev, SolveReport &rep, bool save) {
   cudaStream_t st = p.stream;
   const int K = p.K;
   if (K == 0) return;
   p.status.alloc(sizeof(int) * K, st);
   PB_CUDA(cudaMemsetAsync(p.status.p, 0, sizeof(int) * K, st));
+  BigExtra ex;
+  if (save) {
+    p.alpha.alloc(sizeof(double) * std::max<int64_t>(p.snnz, 1) * F, st);
+    p.beta.alloc(sizeof(double) * K * 4 * kMaxF, st);
+    p.act.alloc(sizeof(int) * K * 3, st);
+    PB_CUDA(cudaMemsetAsync(p.alpha.p, 0, sizeof(double) * std::max<int64_t>(p.snnz, 1) * F, st));
+    PB_CUDA(cudaMemsetAsync(p.beta.p, 0, sizeof(double) * K * 4 * kMaxF, st));
+    PB_CUDA(cudaMemsetAsync(p.act.p, 0xff, sizeof(int) * K * 3, st));
+    ex.mode = kBigForwardSave;
+    ex.alpha_out = p.alpha.as<double>();
+    ex.beta_out = p.beta.as<double>();
+    ex.act_out = p.act.as<int>();
+  }
   PatchArgs a{};
+  a.alpha_out = ex.alpha_out;
+  a.beta_out = ex.beta_out;
+  a.act_out = ex.act_out;
   a.src = p.src4.as<double4>();
   a.tgt = p.tgt4.as<double4>();
   a.vals = vals_dev;
@@ -419,7 +546,7 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   PB_CUDA(cudaEventCreate(&ev1));
   PB_CUDA(cudaEventRecord(ev0, st));
   run_list(p, a, mode, small, rep);
-  solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep);
+  solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep, ex);
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
   PB_CUDA(cudaEventRecord(ev1, st));
@@ -438,7 +565,7 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   if (!redo_small.empty() || !redo_big.empty()) {
     PB_CUDA(cudaEventRecord(ev0, st));
     run_list(p, a, kLU, redo_small, rep);
-    solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep);
+    solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep, ex);
     PB_CUDA(cudaEventRecord(ev1, st));
     PB_CUDA(cudaStreamSynchronize(st));
     PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
@@ -447,6 +574,42 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
+}
+
+// Per-patch adjoint solves: g (per patch, source) from h (per patch, target).
+void solve_adjoint(Plan &p, int basis, int F, const double *h, double *g_out, SolveReport &rep) {
+  cudaStream_t st = p.stream;
+  const int K = p.K;
+  if (K == 0) return;
+  p.status.alloc(sizeof(int) * K, st);
+  PB_CUDA(cudaMemsetAsync(p.status.p, 0, sizeof(int) * K, st));
+  PatchArgs a{};
+  a.src = p.src4.as<double4>();
+  a.tgt = p.tgt4.as<double4>();
+  a.soff = p.soff.as<int64_t>();
+  a.sidx = p.sidx.as<int>();
+  a.toff = p.toff.as<int64_t>();
+  a.tidx = p.tidx.as<int>();
+  a.centers = p.centers.as<double4>();
+  a.status = p.status.as<int>();
+  a.rinv = 1.0 / p.opts.support_radius;
+  a.F = F;
+  a.dim = p.dim;
+  a.basis = basis;
+  a.h = h;
+  a.g_out = g_out;
+  const int nbig = big_threshold();
+  std::vector<int> small, big;
+  for (int k = 0; k < K; ++k) {
+    if (p.m_host[k] == 0) continue;  // h = 0 there: g = 0 (the caller zeroes g)
+    (p.n_host[k] > nbig ? big : small).push_back(k);
+  }
+  run_list(p, a, kAdj, small, rep);
+  BigExtra ex;
+  ex.mode = kBigAdjoint;
+  ex.h = h;
+  ex.g_out = g_out;
+  solve_big(p, basis, nullptr, F, false, big, nullptr, p.status.as<int>(), rep, ex);
 }
 
 }  // namespace pacman_b200

@@ -125,27 +125,50 @@ def interpolate(space_dimension, execspace, rbf_function, source_points, source_
     return out
 
 
+def _as_array(x):
+    """(pointer, shape, kind, keep-alive) of a float64 C-contiguous view of x:
+    CUDA torch tensors stay on the device, everything else becomes numpy."""
+    if _is_cuda_tensor(x):
+        import torch
+        t = x.detach().to(torch.float64).contiguous()
+        return t.data_ptr(), tuple(t.shape), "cuda", t
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    return a.ctypes.data, a.shape, "host", a
+
+
+def _empty_like_kind(kind, shape, ref):
+    if kind == "cuda":
+        import torch
+        t = torch.zeros(shape, dtype=torch.float64, device=ref.device)
+        return t.data_ptr(), t
+    a = np.zeros(shape, dtype=np.float64)
+    return a.ctypes.data, a
+
+
 class Plan:
     """Reusable transfer plan: geometry built once, ``execute`` per field set.
 
     The geometry (patch radius, centre cover, membership lists) depends only
     on the points, so coupling loops that move new values over fixed meshes
-    skip it after the first call."""
+    skip it after the first call.  Points, values and gradients may be numpy
+    arrays or CUDA torch tensors."""
 
     def __init__(self, space_dimension, source_points, target_points, *, nodes_per_cluster=50,
                  relative_overlap=0.15, support_radius=0.1, precision="fp64", device=None):
         self._lib = _lib.load()
         self._h = None
-        sp = np.ascontiguousarray(source_points, dtype=np.float64)
-        tp = np.ascontiguousarray(target_points, dtype=np.float64)
-        _check_shapes(int(space_dimension), sp.shape, (sp.shape[0],), tp.shape)
+        sp_ptr, sp_shape, kind, self._sp = _as_array(source_points)
+        tp_ptr, tp_shape, _, self._tp = _as_array(target_points)
+        _check_shapes(int(space_dimension), sp_shape, (sp_shape[0],), tp_shape)
         self.dim = int(space_dimension)
-        self.n, self.m = sp.shape[0], tp.shape[0]
+        self.n, self.m = sp_shape[0], tp_shape[0]
+        if kind == "cuda" and device is None:
+            device = self._sp.device.index
         opts = _options(nodes_per_cluster, relative_overlap, support_radius, precision, device,
                         None)
         h = ctypes.c_void_p()
-        rc = self._lib.pacman_b200_plan_create(self.dim, sp.ctypes.data, self.n, tp.ctypes.data,
-                                               self.m, ctypes.byref(opts), ctypes.byref(h))
+        rc = self._lib.pacman_b200_plan_create(self.dim, sp_ptr, self.n, tp_ptr, self.m,
+                                               ctypes.byref(opts), ctypes.byref(h))
         _lib.raise_for(rc, "pacman.rbf.Plan")
         self._h = h
         self.F = None
@@ -192,17 +215,34 @@ class Plan:
         _lib.raise_for(self._lib.pacman_b200_plan_local_values(self._h, out.ctypes.data))
         return out[: inf["tgt_nnz"]]
 
-    def execute(self, rbf_function, source_values, stats=None):
-        sv = np.ascontiguousarray(source_values, dtype=np.float64)
-        if sv.shape[0] != self.n:
+    def execute(self, rbf_function, source_values, stats=None, save_for_adjoint=False):
+        """Transfer of source_values ((N,) or (N, F)); with save_for_adjoint the
+        per-patch coefficients are kept for ``adjoint``."""
+        ptr, shape, kind, keep = _as_array(source_values)
+        if shape[0] != self.n:
             raise ValueError("source values must have one row per source point")
-        F = 1 if sv.ndim == 1 else sv.shape[1]
-        out = np.zeros((self.m,) if sv.ndim == 1 else (self.m, F), dtype=np.float64)
+        F = 1 if len(shape) == 1 else shape[1]
+        out_ptr, out = _empty_like_kind(kind, (self.m,) if len(shape) == 1 else (self.m, F), keep)
         st = _lib.Stats()
-        rc = self._lib.pacman_b200_plan_execute(self._h, int(rbf_function), sv.ctypes.data, F,
-                                                out.ctypes.data, ctypes.byref(st))
+        flags = _lib.SAVE_FOR_ADJOINT if save_for_adjoint else 0
+        rc = self._lib.pacman_b200_plan_execute_ex(self._h, int(rbf_function), ptr, F, out_ptr,
+                                                   flags, ctypes.byref(st))
         _lib.raise_for(rc, "pacman.rbf.Plan.execute")
         self.F = F
+        self._vector = len(shape) == 1
         if stats is not None:
             stats.update(st.as_dict())
         return out
+
+    def adjoint(self, grad_target_values, values=True, targets=True):
+        """Transpose of the last execute(save_for_adjoint=True): returns
+        (d<G, out>/d source_values, d<G, out>/d target_points) for the upstream
+        gradient G (same shape as that execute's output); either may be None."""
+        ptr, shape, kind, keep = _as_array(grad_target_values)
+        F = self.F
+        vshape = (self.n,) if self._vector else (self.n, F)
+        gv_ptr, gv = _empty_like_kind(kind, vshape, keep) if values else (None, None)
+        gt_ptr, gt = _empty_like_kind(kind, (self.m, self.dim), keep) if targets else (None, None)
+        rc = self._lib.pacman_b200_plan_adjoint(self._h, ptr, gv_ptr, gt_ptr)
+        _lib.raise_for(rc, "pacman.rbf.Plan.adjoint")
+        return gv, gt
