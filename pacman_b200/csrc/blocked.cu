@@ -202,6 +202,52 @@ __device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 }
 
+// Asynchronous 16-byte global -> shared copies (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void async_tile(double *s, const double *g, int ld, int tid, int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    cp_async16(s + r * LDS + 2 * c2, g + int64_t(r) * ld + 2 * c2);
+  }
+}
+
+// Trailing update in row strips: one CTA owns up to kStrip consecutive tiles
+// of one tile row of step s, keeps the row's A tile in shared memory and
+// prefetches the next B tile while the current product runs.
+constexpr int kStrip = 4;
+
+// Strip l of a slot at step s -> (row t, first list index j0, count).  The
+// column list of row t is LU: s+1..T; Cholesky: s+1..min(t, T-1), then T.
+__device__ __forceinline__ void decode_strip(bool lu, const BigSlot &sl, int s, int l, int &t,
+                                             int &j0, int &count) {
+  if (lu) {
+    const int W = sl.T - s, cpr = (W + kStrip - 1) / kStrip;
+    t = s + 1 + l / cpr;
+    j0 = (l % cpr) * kStrip;
+    count = min(kStrip, W - j0);
+    return;
+  }
+  t = s + 1;
+  for (;;) {
+    const int len = (t < sl.T) ? (t - s + 1) : (sl.T - s);
+    const int ch = (len + kStrip - 1) / kStrip;
+    if (l < ch) {
+      j0 = l * kStrip;
+      count = min(kStrip, len - j0);
+      return;
+    }
+    l -= ch;
+    ++t;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
@@ -448,28 +494,39 @@ __global__ void __launch_bounds__(256) k_diag(BigArgs a, const BigSlot *__restri
       __syncthreads();
     }
   }
-  // Inverses, one column per thread (lower: forward, upper: backward).
-  if (tid < TB) {
-    const int j = tid;
-    for (int i = 0; i < j; ++i) Li[i * LDS + j] = 0.0;
-    double xj = LU ? 1.0 : 1.0 / T[j * LDS + j];
-    Li[j * LDS + j] = xj;
-    for (int i = j + 1; i < TB; ++i) {
-      double s2 = 0.0;
-      for (int k = j; k < i; ++k) s2 = __fma_rn(T[i * LDS + k], Li[k * LDS + j], s2);
-      Li[i * LDS + j] = LU ? -s2 : -s2 / T[i * LDS + i];
+  // Inverses row by row, all threads: X = L^{-1} from the top,
+  // X[p][c] = (delta_pc - sum_{c<=k<p} L[p][k] X[k][c]) / L[p][p], and for LU
+  // Y = U^{-1} from the bottom,
+  // Y[p][c] = (delta_pc - sum_{p<k<=c} U[p][k] Y[k][c]) / U[p][p];
+  // each column's dot product is split over 4 threads.
+  __shared__ double part[2][4][TB];
+  const int col = tid & 63, quarter = tid >> 6;
+  for (int i = 0; i < TB; ++i) {
+    const int pl = i, pu = TB - 1 - i;
+    double sl_ = 0.0, su_ = 0.0;
+    if (col < pl)
+      for (int k = col + quarter; k < pl; k += 4) sl_ = __fma_rn(T[pl * LDS + k], Li[k * LDS + col], sl_);
+    if (LU && col > pu)
+      for (int k = pu + 1 + quarter; k <= col; k += 4) su_ = __fma_rn(T[pu * LDS + k], Ui[k * LDS + col], su_);
+    part[0][quarter][col] = sl_;
+    part[1][quarter][col] = su_;
+    __syncthreads();
+    if (tid < TB) {
+      const double sumL = part[0][0][col] + part[0][1][col] + part[0][2][col] + part[0][3][col];
+      double x = 0.0;
+      if (col == pl) x = LU ? 1.0 : 1.0 / T[pl * LDS + pl];
+      else if (col < pl) x = LU ? -sumL : -sumL / T[pl * LDS + pl];
+      Li[pl * LDS + col] = x;
+    } else if (LU && tid < 2 * TB) {
+      const int c = tid - TB;
+      const double sumU = part[1][0][c] + part[1][1][c] + part[1][2][c] + part[1][3][c];
+      double y = 0.0;
+      if (c == pu) y = 1.0 / T[pu * LDS + pu];
+      else if (c > pu) y = -sumU / T[pu * LDS + pu];
+      Ui[pu * LDS + c] = y;
     }
-    if (LU) {
-      for (int i = j + 1; i < TB; ++i) Ui[i * LDS + j] = 0.0;
-      Ui[j * LDS + j] = 1.0 / T[j * LDS + j];
-      for (int i = j - 1; i >= 0; --i) {
-        double s2 = 0.0;
-        for (int k = i + 1; k <= j; ++k) s2 = __fma_rn(T[i * LDS + k], Ui[k * LDS + j], s2);
-        Ui[i * LDS + j] = -s2 / T[i * LDS + i];
-      }
-    }
+    __syncthreads();
   }
-  __syncthreads();
   for (int idx = tid; idx < TB * TB / 2; idx += blockDim.x) {
     const int r = idx >> 5, c2 = idx & 31;
     *reinterpret_cast<double2 *>(g + int64_t(r) * sl.ld + 2 * c2) =
@@ -555,6 +612,50 @@ __global__ void __launch_bounds__(128)
   if (bt) mma64<false, true>(sA, sB, acc, -1.0, wr, wc, lane);
   else mma64<false, false>(sA, sB, acc, -1.0, wr, wc, lane);
   acc_store(acc, C, ld, wr, wc, lane);
+}
+
+template <bool LU>
+__global__ void __launch_bounds__(128, 2)
+    k_update_strip(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre,
+                   int cnt, int s) {
+  extern __shared__ double sm[];
+  double *sA = sm;
+  double *sB[2] = {sm + TB * LDS, sm + 2 * TB * LDS};
+  const int q = find_slot(pre, cnt, blockIdx.x);
+  const BigSlot sl = slots[q];
+  int t, j0, count;
+  decode_strip(LU, sl, s, blockIdx.x - pre[q], t, j0, count);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  double *base = a.W + sl.base;
+  const int ld = sl.ld;
+  const int ncol = LU ? sl.T - s : ((t < sl.T) ? (t - s) : (sl.T - s - 1));
+  auto column = [&](int j) { return LU ? s + 1 + j : (j < ncol ? s + 1 + j : sl.T); };
+  auto bsrc = [&](int u) -> const double * {
+    const bool bt = !LU && u < sl.T;
+    return bt ? base + int64_t(u) * TB * ld + int64_t(s) * TB
+              : base + int64_t(s) * TB * ld + int64_t(u) * TB;
+  };
+  async_tile(sA, base + int64_t(t) * TB * ld + int64_t(s) * TB, ld, tid, blockDim.x);
+  async_tile(sB[0], bsrc(column(j0)), ld, tid, blockDim.x);
+  cp_async_commit();
+  for (int jj = 0; jj < count; ++jj) {
+    const int u = column(j0 + jj);
+    if (jj + 1 < count) {
+      async_tile(sB[(jj + 1) & 1], bsrc(column(j0 + jj + 1)), ld, tid, blockDim.x);
+      cp_async_commit();
+    }
+    double *C = base + int64_t(t) * TB * ld + int64_t(u) * TB;
+    double acc[4][4][2];
+    acc_load(acc, C, ld, wr, wc, lane);
+    if (jj + 1 < count) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();
+    if (!LU && u < sl.T) mma64<false, true>(sA, sB[jj & 1], acc, -1.0, wr, wc, lane);
+    else mma64<false, false>(sA, sB[jj & 1], acc, -1.0, wr, wc, lane);
+    acc_store(acc, C, ld, wr, wc, lane);
+    __syncthreads();
+  }
 }
 
 // local = V beta - S (S = -E alpha from the Schur complement).
@@ -759,6 +860,16 @@ static int64_t count_trsm(bool lu, const BigSlot &q, int s) {
   const int R = q.T + q.TE;
   return lu ? int64_t(q.T - s) + (R - s - 1) : int64_t(R - s);
 }
+static int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+// sum_{L=1}^{W} ceil(L / kStrip)
+static int64_t strip_sum(int64_t W) {
+  const int64_t qq = W / kStrip, r = W % kStrip;
+  return kStrip * qq * (qq + 1) / 2 + r * (qq + 1);
+}
+static int64_t count_strips(bool lu, const BigSlot &q, int s) {
+  const int64_t R = q.T + q.TE, W = q.T - s;
+  return lu ? (R - s - 1) * ceil_div(W, kStrip) : (strip_sum(W) - 1) + int64_t(q.TE) * ceil_div(W, kStrip);
+}
 static int64_t count_update(bool lu, const BigSlot &q, int s) {
   const int64_t R = q.T + q.TE, w = q.T - s;
   return lu ? (R - s - 1) * w : (w - 1) * w / 2 + (w - 1) + int64_t(q.TE) * w;
@@ -774,6 +885,10 @@ static void set_smem_attributes() {
   PB_CUDA(cudaFuncSetAttribute(k_trsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
   PB_CUDA(cudaFuncSetAttribute(k_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
   PB_CUDA(cudaFuncSetAttribute(k_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+  PB_CUDA(cudaFuncSetAttribute(k_update_strip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               3 * TB * LDS * int(sizeof(double))));
+  PB_CUDA(cudaFuncSetAttribute(k_update_strip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               3 * TB * LDS * int(sizeof(double))));
   done = true;
 }
 
@@ -866,7 +981,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       acc = 0;
       pre.push_back(0);
       for (int q = 0; q < c; ++q) {
-        acc += count_update(lu, slots[q], s);
+        acc += count_strips(lu, slots[q], s);
         if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
         pre.push_back(int(acc));
       }
@@ -915,11 +1030,11 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       if (lu) {
         k_diag<true><<<c, 256, s3, st>>>(a, ds, s);
         if (nt) k_trsm<true><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
-        if (nu) k_update<true><<<nu, 128, s2, st>>>(a, ds, pu, c, s);
+        if (nu) k_update_strip<true><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
       } else {
         k_diag<false><<<c, 256, s3, st>>>(a, ds, s);
         if (nt) k_trsm<false><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
-        if (nu) k_update<false><<<nu, 128, s2, st>>>(a, ds, pu, c, s);
+        if (nu) k_update_strip<false><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
       }
       note_launch(1 + (nt ? 1 : 0) + (nu ? 1 : 0));
     }
