@@ -91,77 +91,50 @@ __global__ void __launch_bounds__(kSolveThreads)
   double *A = use_global ? (a.gA + a.gAoff[e]) : (zs + n);
   if (tid == 0) flag_s = 0;
 
-  // Gather the patch (TeamFillB, team_ops.hpp:113-121) and its moments.
+  // Gather the patch (TeamFillB, team_ops.hpp:113-121).
   const double4 c = a.centers[k];
   const double shift[3] = {c.x, c.y, c.z};
-  double acc[kRedVals - 6];
   const int Fm = (MODE == kAdj) ? 0 : F;  // value moments only for the forward fit
   const int nred = 10 + 4 * Fm;
-#pragma unroll
-  for (int v = 0; v < kRedVals - 6; ++v) acc[v] = 0.0;
-  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int i = tid; i < n; i += kSolveThreads) {
     const int id = a.sidx[s0 + i];
     const double4 p = a.src[id];
     xs[i] = p.x;
     ys[i] = p.y;
     zs[i] = p.z;
-    const double q[4] = {1.0, p.x - shift[0], p.y - shift[1], p.z - shift[2]};
-    acc[0] += 1.0;
-    acc[1] += q[1];
-    acc[2] += q[2];
-    acc[3] += q[3];
-    acc[4] += q[1] * q[1];
-    acc[5] += q[1] * q[2];
-    acc[6] += q[1] * q[3];
-    acc[7] += q[2] * q[2];
-    acc[8] += q[2] * q[3];
-    acc[9] += q[3] * q[3];
-#pragma unroll
-    for (int f = 0; f < kMaxF; ++f) {
-      if (f < Fm) {
-        const double b = a.vals[int64_t(id) * F + f];
-        A[int64_t(i) * lda + n + f] = b;
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) acc[10 + 4 * f + cc] += q[cc] * b;
-      }
-    }
-    const double pc[3] = {p.x, p.y, p.z};
-    for (int d = 0; d < 3; ++d) {
-      mn[d] = fmin(mn[d], pc[d]);
-      mx[d] = fmax(mx[d], pc[d]);
-    }
-  }
-#pragma unroll
-  for (int v = 0; v < kRedVals - 6; ++v) {
-    const double s = warp_sum(acc[v]);
-    if (lane == 0 && v < nred) red[warp][v] = s;
-  }
-  for (int d = 0; d < 3; ++d) {
-    double lo = mn[d], hi = mx[d];
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    if (lane == 0) {
-      red[warp][nred + d] = lo;
-      red[warp][nred + 3 + d] = hi;
-    }
+    for (int f = 0; f < Fm; ++f) A[int64_t(i) * lda + n + f] = a.vals[int64_t(id) * F + f];
   }
   __syncthreads();
+  // Moments of the centred monomials q = [1, x - c] (and q * b per field),
+  // then the coordinate ranges: one thread per value, points in order.
   if (tid < nred + 6) {
-    double s;
+    double v;
     if (tid < nred) {
-      s = 0.0;
-      for (int w = 0; w < kWarps; ++w) s += red[w][tid];
-    } else if (tid < nred + 3) {
-      s = INFINITY;
-      for (int w = 0; w < kWarps; ++w) s = fmin(s, red[w][tid]);
+      int i0, i1 = 0, f = -1;
+      if (tid < 4) {
+        i0 = tid;
+      } else if (tid < 10) {
+        const int pr[6][2] = {{1, 1}, {1, 2}, {1, 3}, {2, 2}, {2, 3}, {3, 3}};
+        i0 = pr[tid - 4][0];
+        i1 = pr[tid - 4][1];
+      } else {
+        f = (tid - 10) >> 2;
+        i0 = (tid - 10) & 3;
+      }
+      v = 0.0;
+      for (int i = 0; i < n; ++i) {
+        const double q[4] = {1.0, xs[i] - shift[0], ys[i] - shift[1], zs[i] - shift[2]};
+        const double w = (f >= 0) ? A[int64_t(i) * lda + n + f] : (tid < 4 ? 1.0 : q[i1]);
+        v += q[i0] * w;
+      }
     } else {
-      s = -INFINITY;
-      for (int w = 0; w < kWarps; ++w) s = fmax(s, red[w][tid]);
+      const int d = (tid - nred) % 3;
+      const bool is_max = tid - nred >= 3;
+      const double *x = d == 0 ? xs : (d == 1 ? ys : zs);
+      v = x[0];
+      for (int i = 1; i < n; ++i) v = is_max ? fmax(v, x[i]) : fmin(v, x[i]);
     }
-    redf[tid] = s;
+    redf[tid] = v;
   }
   __syncthreads();
   __shared__ int S_s[4], pv_s;
