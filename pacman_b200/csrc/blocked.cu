@@ -24,35 +24,9 @@
 #include <cmath>
 #include <vector>
 
-#include "plan.hpp"
-#include "poly.cuh"
+#include "blocked.cuh"
 
 namespace pacman_b200 {
-
-constexpr int TB = 64;   // tile size
-constexpr int LDS = 68;  // shared-memory row stride (doubles): conflict-free fragments
-
-struct BigSlot {
-  int64_t base;  // offset (doubles) of the augmented matrix in the workspace
-  int ld;        // row stride (doubles) = (T + 1) * TB
-  int T;         // pivot tiles
-  int TE;        // evaluation-row tiles
-  int k;         // patch id
-  int n, m;
-};
-
-// Work of one launch is addressed by blockIdx.x through prefix counts over
-// the active slots (slots are sorted by decreasing T, so the slots still
-// active at step s are 0..cnt-1): pre[q] <= blockIdx.x < pre[q + 1].
-__device__ __forceinline__ int find_slot(const int *__restrict__ pre, int cnt, int b) {
-  int lo = 0, hi = cnt;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (pre[mid] <= b) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
 
 // Tiles filled by the assembly of one slot: LU every (row, column) tile of
 // the augmented matrix; Cholesky the lower A tiles, every E tile and the
@@ -99,125 +73,6 @@ __device__ __forceinline__ void decode_trsm(bool lu, const BigSlot &sl, int s, i
   }
 }
 
-// Trailing tiles of step s.  LU: rows s+1..R-1 x columns s+1..T.  Cholesky:
-// row t < T holds columns s+1..t then the residual column T; row t >= T
-// holds columns s+1..T-1 then T.
-__device__ __forceinline__ void decode_update(bool lu, const BigSlot &sl, int s, int l, int &ti,
-                                              int &tj) {
-  if (lu) {
-    const int w = sl.T - s;
-    ti = s + 1 + l / w;
-    tj = s + 1 + l % w;
-    return;
-  }
-  int t = s + 1;
-  for (;;) {
-    const int ncol = (t < sl.T) ? (t - s) : (sl.T - s - 1);
-    if (l <= ncol) {
-      ti = t;
-      tj = (l < ncol) ? s + 1 + l : sl.T;
-      return;
-    }
-    l -= ncol + 1;
-    ++t;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// FP64 tensor-core tile product
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-// acc += sign * op(A) op(B) on the 32 x 32 block (wr, wc) of a 64 x 64 tile.
-// Fragment layout of m8n8k4.f64: A (row) a0 = A[g][t], B (col) b0 = B[t][g],
-// C c_h = C[g][2t + h], with g = lane / 4, t = lane % 4.
-template <bool AT, bool BT>
-__device__ __forceinline__ void mma64(const double *__restrict__ sA, const double *__restrict__ sB,
-                                      double (&acc)[4][4][2], double sign, int wr, int wc,
-                                      int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll 2
-  for (int k0 = 0; k0 < TB; k0 += 4) {
-    const int kk = k0 + t;
-    double a[4], b[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int r = wr + 8 * i + g;
-      a[i] = sign * (AT ? sA[kk * LDS + r] : sA[r * LDS + kk]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = wc + 8 * j + g;
-      b[j] = BT ? sB[c * LDS + kk] : sB[kk * LDS + c];
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-  }
-}
-
-__device__ __forceinline__ void load_tile(double *s, const double *g, int ld, int tid, int nt) {
-  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
-    const int r = idx >> 5, c2 = idx & 31;
-    const double2 v = *reinterpret_cast<const double2 *>(g + int64_t(r) * ld + 2 * c2);
-    *reinterpret_cast<double2 *>(s + r * LDS + 2 * c2) = v;
-  }
-}
-
-__device__ __forceinline__ void acc_load(double (&acc)[4][4][2], const double *C, int ld, int wr,
-                                         int wc, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double2 v = *reinterpret_cast<const double2 *>(
-          C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t);
-      acc[i][j][0] = v.x;
-      acc[i][j][1] = v.y;
-    }
-}
-
-__device__ __forceinline__ void acc_store(const double (&acc)[4][4][2], double *C, int ld, int wr,
-                                          int wc, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      *reinterpret_cast<double2 *>(C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t) =
-          make_double2(acc[i][j][0], acc[i][j][1]);
-}
-
-__device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-}
-
-// Asynchronous 16-byte global -> shared copies (cp.async, sm_80+).
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-__device__ __forceinline__ void async_tile(double *s, const double *g, int ld, int tid, int nt) {
-  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
-    const int r = idx >> 5, c2 = idx & 31;
-    cp_async16(s + r * LDS + 2 * c2, g + int64_t(r) * ld + 2 * c2);
-  }
-}
-
 // Trailing update in row strips: one CTA owns up to kStrip consecutive tiles
 // of one tile row of step s, keeps the row's A tile in shared memory and
 // prefetches the next B tile while the current product runs.
@@ -252,33 +107,6 @@ __device__ __forceinline__ void decode_strip(bool lu, const BigSlot &sl, int s, 
 // Kernels
 // ---------------------------------------------------------------------------
 
-struct BigArgs {
-  const double4 *src;
-  const double4 *tgt;
-  const double *vals;
-  const int64_t *soff;
-  const int *sidx;
-  const int64_t *toff;
-  const int *tidx;
-  const double4 *centers;
-  double *W;            // workspace
-  double *inv;          // per slot: 2 inverse tiles (TB x TB)
-  double *beta;         // per slot: 4 * kMaxF
-  int *act;             // per slot: 3
-  int *status;          // per patch
-  double *local;
-  double rinv;
-  int F;
-  int dim;
-  int basis;
-  int mode;            // kBigForward, kBigForwardSave or kBigAdjoint
-  double *alpha_out;   // forward + save: RBF coefficients per (patch, source)
-  double *beta_out;    // forward + save: K x 4*kMaxF
-  int *act_out;        // forward + save: K x 3
-  const double *h;     // adjoint: weighted upstream gradient per (patch, target)
-  double *g_out;       // adjoint: result per (patch, source)
-  double *red_out;     // adjoint: per slot reduced moments (kRedVals)
-};
 
 
 
@@ -580,40 +408,6 @@ __global__ void __launch_bounds__(128)
   acc_store(acc, X, sl.ld, wr, wc, lane);
 }
 
-// Trailing update of tile (ti, tj): C -= (ti, s) * (s, tj)       [LU]
-//                                   C -= (ti, s) * (tj, s)^T     [Cholesky, tj < T]
-//                                   C -= (ti, s) * (s, T)        [Cholesky, residual column]
-template <bool LU>
-__global__ void __launch_bounds__(128)
-    k_update(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
-             int s) {
-  extern __shared__ double sm[];
-  double *sA = sm, *sB = sm + TB * LDS;
-  const int q = find_slot(pre, cnt, blockIdx.x);
-  const BigSlot sl = slots[q];
-  struct {
-    int ti, tj;
-  } it;
-  decode_update(LU, sl, s, blockIdx.x - pre[q], it.ti, it.tj);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  double *base = a.W + sl.base;
-  const int ld = sl.ld;
-  double *C = base + int64_t(it.ti) * TB * ld + int64_t(it.tj) * TB;
-  const double *A = base + int64_t(it.ti) * TB * ld + int64_t(s) * TB;
-  const bool bt = !LU && it.tj < sl.T;
-  const double *B = bt ? base + int64_t(it.tj) * TB * ld + int64_t(s) * TB
-                       : base + int64_t(s) * TB * ld + int64_t(it.tj) * TB;
-  load_tile(sA, A, ld, tid, blockDim.x);
-  load_tile(sB, B, ld, tid, blockDim.x);
-  double acc[4][4][2];
-  acc_load(acc, C, ld, wr, wc, lane);
-  __syncthreads();
-  if (bt) mma64<false, true>(sA, sB, acc, -1.0, wr, wc, lane);
-  else mma64<false, false>(sA, sB, acc, -1.0, wr, wc, lane);
-  acc_store(acc, C, ld, wr, wc, lane);
-}
-
 template <bool LU>
 __global__ void __launch_bounds__(128, 2)
     k_update_strip(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre,
@@ -870,24 +664,14 @@ static int64_t count_strips(bool lu, const BigSlot &q, int s) {
   const int64_t R = q.T + q.TE, W = q.T - s;
   return lu ? (R - s - 1) * ceil_div(W, kStrip) : (strip_sum(W) - 1) + int64_t(q.TE) * ceil_div(W, kStrip);
 }
-static int64_t count_update(bool lu, const BigSlot &q, int s) {
-  const int64_t R = q.T + q.TE, w = q.T - s;
-  return lu ? (R - s - 1) * w : (w - 1) * w / 2 + (w - 1) + int64_t(q.TE) * w;
-}
 
 static void set_smem_attributes() {
   static bool done = false;
   if (done) return;
   const int s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
   PB_CUDA(cudaFuncSetAttribute(k_diag<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
-  PB_CUDA(cudaFuncSetAttribute(k_diag<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
   PB_CUDA(cudaFuncSetAttribute(k_trsm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-  PB_CUDA(cudaFuncSetAttribute(k_trsm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-  PB_CUDA(cudaFuncSetAttribute(k_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-  PB_CUDA(cudaFuncSetAttribute(k_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
   PB_CUDA(cudaFuncSetAttribute(k_update_strip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               3 * TB * LDS * int(sizeof(double))));
-  PB_CUDA(cudaFuncSetAttribute(k_update_strip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                3 * TB * LDS * int(sizeof(double))));
   done = true;
 }
@@ -932,21 +716,36 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   a.g_out = extra.g_out;
   const bool adjoint = extra.mode == kBigAdjoint;
   if (adjoint) lu = false;
+  if (!lu) chol_set_smem_attributes();
+  // The Cholesky forward path evaluates local = E alpha + V beta from alpha
+  // per (patch, source): alpha_out when saving, else a scratch array.
+  DevMem dalpha;
+  if (!lu && !adjoint) {
+    if (extra.alpha_out != nullptr) {
+      a.alpha_c = extra.alpha_out;
+    } else {
+      dalpha.alloc(sizeof(double) * size_t(p.snnz) * size_t(F), st);
+      a.alpha_c = dalpha.as<double>();
+    }
+  }
   HostArena &arena = HostArena::get();
   size_t pos = 0;
   while (pos < order.size()) {
     // One wave: as many patches as fit the workspace budget.
     std::vector<BigSlot> slots;
     size_t tot = 0;
+    int64_t tot_inv = 0;
     while (pos < order.size()) {
       const int k = order[pos];
       const int n = p.n_host[k], m = p.m_host[k];
-      const size_t d = slot_doubles(n, adjoint ? 0 : m);
+      const size_t d = slot_doubles(n, lu ? m : 0);
       if (!slots.empty() && tot + d > budget) break;
       BigSlot q{};
       q.base = int64_t(tot);
       q.T = (n + TB - 1) / TB;
-      q.TE = adjoint ? 0 : (m + TB - 1) / TB;
+      q.TE = lu ? (m + TB - 1) / TB : 0;
+      q.inv = lu ? int64_t(slots.size()) * 2 * TB * TB : tot_inv;
+      tot_inv += int64_t(q.T) * TB * TB;
       q.ld = (q.T + 1) * TB;
       q.k = k;
       q.n = n;
@@ -968,28 +767,37 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       if (v > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
       pre_asm[q + 1] = int(v);
     }
+    // LU: per step the trsm and update-strip prefix counts over the active
+    // slots (a prefix of the sorted slots); Cholesky: chol_prefix.
     std::vector<int> cnt(steps), off(steps + 1, 0), pre;
-    pre.reserve(size_t(steps) * 2 * (ns + 1));
-    for (int s = 0; s < steps; ++s) {
-      int c = 0;
-      while (c < ns && slots[c].T > s) ++c;
-      cnt[s] = c;
-      off[s] = int(pre.size());
-      int64_t acc = 0;
-      pre.push_back(0);
-      for (int q = 0; q < c; ++q) pre.push_back(int(acc += count_trsm(lu, slots[q], s)));
-      acc = 0;
-      pre.push_back(0);
-      for (int q = 0; q < c; ++q) {
-        acc += count_strips(lu, slots[q], s);
-        if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
-        pre.push_back(int(acc));
+    CholPlan cp;
+    if (lu) {
+      pre.reserve(size_t(steps) * 2 * (ns + 1));
+      for (int s = 0; s < steps; ++s) {
+        int c = 0;
+        while (c < ns && slots[c].T > s) ++c;
+        cnt[s] = c;
+        off[s] = int(pre.size());
+        int64_t acc = 0;
+        pre.push_back(0);
+        for (int q = 0; q < c; ++q) pre.push_back(int(acc += count_trsm(lu, slots[q], s)));
+        acc = 0;
+        pre.push_back(0);
+        for (int q = 0; q < c; ++q) {
+          acc += count_strips(lu, slots[q], s);
+          if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
+          pre.push_back(int(acc));
+        }
       }
+      off[steps] = int(pre.size());
+    } else {
+      cp = chol_prefix(slots);
+      pre = cp.pre;
     }
-    off[steps] = int(pre.size());
     DevMem dW, dsmall;
     dW.alloc(sizeof(double) * tot, st);
-    const size_t n_inv = size_t(2) * TB * TB * ns, n_beta = size_t(4) * kMaxF * ns;
+    const size_t n_inv = lu ? size_t(2) * TB * TB * ns : size_t(tot_inv);
+    const size_t n_beta = size_t(4) * kMaxF * ns;
     const size_t n_red = size_t(kRedVals) * ns;
     const size_t bytes_small = sizeof(double) * (n_inv + n_beta + n_red) + sizeof(int) * 3 * ns +
                                sizeof(BigSlot) * ns + sizeof(int) * (pre_asm.size() + pre.size()) +
@@ -1020,6 +828,16 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       k_big_adj_rhs<<<ns, 256, 0, st>>>(a, ds);
       note_launch();
     }
+    if (!lu) {
+      chol_launch_steps(a, ds, cp, dpre, st);
+      chol_launch_finish(a, ds, ns, adjoint, st);
+      if (adjoint) {
+        k_big_adj_finish<<<ns, 256, 0, st>>>(a, ds);
+        note_launch();
+      }
+      PB_CUDA(cudaGetLastError());
+      continue;
+    }
     const size_t s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
     for (int s = 0; s < steps; ++s) {
       const int c = cnt[s];
@@ -1027,28 +845,15 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       const int *pu = pt + c + 1;
       const int nt = pre[off[s] + c];
       const int nu = pre[off[s] + c + 1 + c];
-      if (lu) {
-        k_diag<true><<<c, 256, s3, st>>>(a, ds, s);
-        if (nt) k_trsm<true><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
-        if (nu) k_update_strip<true><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
-      } else {
-        k_diag<false><<<c, 256, s3, st>>>(a, ds, s);
-        if (nt) k_trsm<false><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
-        if (nu) k_update_strip<false><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
-      }
+      k_diag<true><<<c, 256, s3, st>>>(a, ds, s);
+      if (nt) k_trsm<true><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
+      if (nu) k_update_strip<true><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
       note_launch(1 + (nt ? 1 : 0) + (nu ? 1 : 0));
     }
-    if (!adjoint) {
-      k_big_finish<<<ns, 128, 0, st>>>(a, ds);
-      note_launch();
-    }
-    if (adjoint || extra.mode == kBigForwardSave) {
-      if (lu) k_back_sweep<true><<<ns, 256, 0, st>>>(a, ds);
-      else k_back_sweep<false><<<ns, 256, 0, st>>>(a, ds);
-      note_launch();
-    }
-    if (adjoint) {
-      k_big_adj_finish<<<ns, 256, 0, st>>>(a, ds);
+    k_big_finish<<<ns, 128, 0, st>>>(a, ds);
+    note_launch();
+    if (extra.mode == kBigForwardSave) {
+      k_back_sweep<true><<<ns, 256, 0, st>>>(a, ds);
       note_launch();
     }
     PB_CUDA(cudaGetLastError());

@@ -1,0 +1,180 @@
+// Shared pieces of the blocked engine for large patches (blocked.cu: LU and
+// the shared assembly/polynomial kernels; cholesky.cu: the left-looking
+// Cholesky factorisation): tile geometry, slot records, launch arguments and
+// the FP64 tensor-core tile product.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "plan.hpp"
+#include "poly.cuh"
+
+namespace pacman_b200 {
+
+constexpr int TB = 64;   // tile size
+constexpr int LDS = 68;  // shared-memory row stride (doubles): conflict-free fragments
+
+struct BigSlot {
+  int64_t base;  // offset (doubles) of the augmented matrix in the workspace
+  int ld;        // row stride (doubles) = (T + 1) * TB
+  int T;         // pivot tiles
+  int TE;        // evaluation-row tiles
+  int k;         // patch id
+  int n, m;
+  int64_t inv;   // offset (doubles) of the slot's inverse tiles
+};
+
+// Work of one launch is addressed by blockIdx.x through prefix counts over
+// the active slots (slots are sorted by decreasing T, so the slots still
+// active at step s are 0..cnt-1): pre[q] <= blockIdx.x < pre[q + 1].
+__device__ __forceinline__ int find_slot(const int *__restrict__ pre, int cnt, int b) {
+  int lo = 0, hi = cnt;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core tile product
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// acc += sign * op(A) op(B) on the 32 x 32 block (wr, wc) of a 64 x 64 tile.
+// Fragment layout of m8n8k4.f64: A (row) a0 = A[g][t], B (col) b0 = B[t][g],
+// C c_h = C[g][2t + h], with g = lane / 4, t = lane % 4.
+template <bool AT, bool BT>
+__device__ __forceinline__ void mma64(const double *__restrict__ sA, const double *__restrict__ sB,
+                                      double (&acc)[4][4][2], double sign, int wr, int wc,
+                                      int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll 2
+  for (int k0 = 0; k0 < TB; k0 += 4) {
+    const int kk = k0 + t;
+    double a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = wr + 8 * i + g;
+      a[i] = sign * (AT ? sA[kk * LDS + r] : sA[r * LDS + kk]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = wc + 8 * j + g;
+      b[j] = BT ? sB[c * LDS + kk] : sB[kk * LDS + c];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  }
+}
+
+__device__ __forceinline__ void load_tile(double *s, const double *g, int ld, int tid, int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    const double2 v = *reinterpret_cast<const double2 *>(g + int64_t(r) * ld + 2 * c2);
+    *reinterpret_cast<double2 *>(s + r * LDS + 2 * c2) = v;
+  }
+}
+
+__device__ __forceinline__ void acc_load(double (&acc)[4][4][2], const double *C, int ld, int wr,
+                                         int wc, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double2 v = *reinterpret_cast<const double2 *>(
+          C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t);
+      acc[i][j][0] = v.x;
+      acc[i][j][1] = v.y;
+    }
+}
+
+__device__ __forceinline__ void acc_store(const double (&acc)[4][4][2], double *C, int ld, int wr,
+                                          int wc, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<double2 *>(C + int64_t(wr + 8 * i + g) * ld + wc + 8 * j + 2 * t) =
+          make_double2(acc[i][j][0], acc[i][j][1]);
+}
+
+__device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+}
+
+// Asynchronous 16-byte global -> shared copies (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void async_tile(double *s, const double *g, int ld, int tid, int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    cp_async16(s + r * LDS + 2 * c2, g + int64_t(r) * ld + 2 * c2);
+  }
+}
+
+struct BigArgs {
+  const double4 *src;
+  const double4 *tgt;
+  const double *vals;
+  const int64_t *soff;
+  const int *sidx;
+  const int64_t *toff;
+  const int *tidx;
+  const double4 *centers;
+  double *W;            // workspace
+  double *inv;          // inverse tiles (TB x TB): LU 2 per slot, Cholesky T per slot
+  double *beta;         // per slot: 4 * kMaxF
+  int *act;             // per slot: 3
+  int *status;          // per patch
+  double *local;
+  double rinv;
+  int F;
+  int dim;
+  int basis;
+  int mode;            // kBigForward, kBigForwardSave or kBigAdjoint
+  double *alpha_out;   // forward + save: RBF coefficients per (patch, source)
+  double *beta_out;    // forward + save: K x 4*kMaxF
+  int *act_out;        // forward + save: K x 3
+  const double *h;     // adjoint: weighted upstream gradient per (patch, target)
+  double *g_out;       // adjoint: result per (patch, source)
+  double *red_out;     // adjoint: per slot reduced moments (kRedVals)
+  double *alpha_c;     // Cholesky forward: RBF coefficients per (patch, source)
+};
+
+// Left-looking Cholesky steps, backward sweep and local evaluation of one
+// wave of slots (cholesky.cu).  `pre` holds, per step, the prefix counts of
+// the column-update and triangular-solve launches (see chol_prefix).
+struct CholPlan {
+  std::vector<int> cnt;      // active slots per step
+  std::vector<int> off;      // per step: offset of its prefix arrays in pre
+  std::vector<int> pre;      // per step: update prefix (cnt+1), trsm prefix (cnt+1)
+};
+CholPlan chol_prefix(const std::vector<BigSlot> &slots);
+void chol_set_smem_attributes();
+void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, const int *dpre,
+                       cudaStream_t st);
+void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
+                        cudaStream_t st);
+
+}  // namespace pacman_b200
