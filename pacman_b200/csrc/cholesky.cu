@@ -8,8 +8,8 @@
 // column j per step:
 //   k_col_update  C[i, j] -= sum_{p<j} L[i, p] L[j, p]^T for every i >= j: the
 //                 accumulator stays in registers for the whole K loop, the
-//                 L panels stream through a 3-stage cp.async pipeline;
-//   k_diag_chol   L[j, j] = chol(C[j, j]), its inverse, y_j = L[j, j]^{-1} r_j;
+//                 L panels stream through a cp.async pipeline;
+//   k_diag_chol   X = L[j, j]^{-1} of C[j, j] = L[j, j] L[j, j]^T, y_j = X r_j;
 //   k_col_trsm    L[i, j] = C[i, j] L[j, j]^{-T} for i > j, and the forward
 //                 substitution update r_i -= L[i, j] y_j.
 // Afterwards k_chol_back solves L^T alpha = y (tile inverses kept per step)
@@ -25,18 +25,18 @@ namespace pacman_b200 {
 
 constexpr int kKC = 32;                 // K chunk of the column update (doubles)
 constexpr int kKLD = kKC + 4;           // shared row stride of a chunk: conflict-free fragments
-constexpr int kStages = 3;              // cp.async pipeline depth
+constexpr int kStages = 2;              // cp.async pipeline depth (2 CTAs per SM)
 constexpr int kColRows = 2 * TB;        // rows of one column-update CTA (two tiles)
 constexpr int kColThreads = 256;
 constexpr int kColStage = (kColRows + TB) * kKLD;  // doubles per pipeline stage
 constexpr size_t kColSmem = size_t(kStages) * kColStage * sizeof(double);
 constexpr int kTrsmStrip = 4;           // row tiles per triangular-solve CTA
 constexpr size_t kTrsmSmem = (size_t(3) * TB * LDS + TB * kMaxF) * sizeof(double);
-constexpr size_t kDiagSmem = size_t(2) * TB * LDS * sizeof(double);
+constexpr size_t kDiagSmem = size_t(TB) * LDS * sizeof(double);
 constexpr int kBackStages = 3;
 constexpr size_t kBackSmem = size_t(kBackStages) * TB * LDS * sizeof(double);
 
-// acc -= A B^T over one K chunk: A rows wr.., B rows wc.. (both K-contiguous).
+// acc += A B^T over one K chunk: A rows wr.., B rows wc.. (both K-contiguous).
 __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
                                              const double *__restrict__ sB,
                                              double (&acc)[4][4][2], int wr, int wc, int lane) {
@@ -45,7 +45,7 @@ __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
   for (int k0 = 0; k0 < kKC; k0 += 4) {
     double a[4], b[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a[i] = -sA[(wr + 8 * i + g) * kKLD + k0 + t];
+    for (int i = 0; i < 4; ++i) a[i] = sA[(wr + 8 * i + g) * kKLD + k0 + t];
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) b[jj] = sB[(wc + 8 * jj + g) * kKLD + k0 + t];
 #pragma unroll
@@ -56,8 +56,9 @@ __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
 }
 
 // Column update of step j >= 1.  One CTA owns row tiles i0, i0 + 1 (i0 = j +
-// 2l) of tile column j; eight warps each hold a 32 x 32 accumulator.
-__global__ void __launch_bounds__(kColThreads, 1)
+// 2l) of tile column j; eight warps each hold a 32 x 32 accumulator, which
+// starts at -C and accumulates the products (no negation in the K loop).
+__global__ void __launch_bounds__(kColThreads, 2)
     k_col_update(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre,
                  int cnt, int j) {
   extern __shared__ double sm[];
@@ -94,7 +95,13 @@ __global__ void __launch_bounds__(kColThreads, 1)
   const bool active = two || wr < TB;
   double *C = a.W + sl.base + int64_t(i0) * TB * ld + int64_t(j) * TB;
   double acc[4][4][2];
-  if (active) acc_load(acc, C, ld, wr, wc, lane);
+  if (active) {
+    acc_load(acc, C, ld, wr, wc, lane);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
+  }
   for (int c = 0; c < nch; ++c) {
     cp_async_wait<kStages - 2>();
     __syncthreads();
@@ -106,127 +113,123 @@ __global__ void __launch_bounds__(kColThreads, 1)
     }
   }
   cp_async_wait<0>();
-  if (active) acc_store(acc, C, ld, wr, wc, lane);
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
+    acc_store(acc, C, ld, wr, wc, lane);
+  }
 }
 
-// Cholesky of diagonal tile (j, j) of every active slot, blocked by 16: warp 0
-// factors and inverts each 16 x 16 diagonal block, the CTA applies it to the
-// panel below and updates the trailing block.  Then the full inverse X of the
-// tile from its block rows, X[b][c] = -D_b^{-1} sum_{c<=k<b} L[b][k] X[k][c],
-// and y_j = X r_j.  Non-positive pivots set status bit 4.
-__global__ void __launch_bounds__(256) k_diag_chol(BigArgs a, const BigSlot *__restrict__ slots,
-                                                   int j) {
+// Inverse Cholesky factor of diagonal tile (j, j) of every active slot and
+// y_j = X r_j.  The tile is eliminated as L D L^T with the identity carried
+// along (Gauss-Jordan on [A | I]): at pivot p every row i > p gets
+// R_i -= (a_ip / a_pp) R_p, which leaves U = D L^T on the left and L^{-1} on
+// the right.  Each thread owns a 4 x 4 block of registers; slot (i, s) holds
+// A[i][s] until pivot s and L^{-1}[i][s] afterwards.  Per pivot the owners
+// publish one vector (row p of L^{-1} left of the pivot, the pivot, column p
+// of A below it) and all threads update their slots: one barrier per pivot.
+// Only X = L_c^{-1} = D^{-1/2} L^{-1} is kept (the trsm, the forward and the
+// backward substitution use nothing else).  Non-positive pivots set status 4.
+__global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *__restrict__ slots,
+                                                      int j) {
   extern __shared__ double sm[];
-  double *L = sm;
-  double *X = sm + TB * LDS;
+  double *Xs = sm;  // TB x LDS, the inverse factor at the end
+  __shared__ double cv[2][TB];
   __shared__ double ys[TB][kMaxF];
-  __shared__ double zs[16][48];
-  __shared__ int bad;
   const BigSlot sl = slots[blockIdx.x];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
+  const int bi = tid >> 4, bs = tid & 15;
+  bool bad = false;
   const int ld = sl.ld, F = a.F;
-  double *g = a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB;
+  const double *g = a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB;
   double *rg = a.W + sl.base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
-  load_tile(L, g, ld, tid, 256);
-  for (int e = tid; e < TB * LDS; e += 256) X[e] = 0.0;
+  double v[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const double2 lo = *reinterpret_cast<const double2 *>(g + int64_t(4 * bi + r) * ld + 4 * bs);
+    const double2 hi = *reinterpret_cast<const double2 *>(g + int64_t(4 * bi + r) * ld + 4 * bs + 2);
+    v[r][0] = lo.x;
+    v[r][1] = lo.y;
+    v[r][2] = hi.x;
+    v[r][3] = hi.y;
+  }
   for (int e = tid; e < TB * kMaxF; e += 256) {
     const int r = e / kMaxF, f = e % kMaxF;
     ys[r][f] = f < F ? rg[int64_t(r) * ld + f] : 0.0;
   }
-  if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int b = 0; b < 4; ++b) {
-    const int B0 = 16 * b;
-    if (warp == 0) {
-      for (int p = 0; p < 16; ++p) {
-        const int P = B0 + p;
-        const double app = L[P * LDS + P];
-        __syncwarp();
-        const double d = sqrt(app);
-        if (lane == 0 && !(app > 0.0)) bad = 1;
-        const double dinv = 1.0 / d;
-        if (lane < 16 - p) {
-          const int r = P + lane;
-          L[r * LDS + P] = (lane == 0) ? d : L[r * LDS + P] * dinv;
-        }
-        __syncwarp();
-        const int w = 15 - p;
-        for (int e = lane; e < w * w; e += 32) {
-          const int r = P + 1 + e / w, c = P + 1 + e % w;
-          if (c <= r) L[r * LDS + c] = __fma_rn(-L[r * LDS + P], L[c * LDS + P], L[r * LDS + c]);
-        }
-        __syncwarp();
-      }
-      if (lane < 16) {  // column lane of D^{-1}
-        const int c = B0 + lane;
-        X[c * LDS + c] = 1.0 / L[c * LDS + c];
-        for (int r = c + 1; r < B0 + 16; ++r) {
-          double s = 0.0;
-          for (int k = c; k < r; ++k) s = __fma_rn(L[r * LDS + k], X[k * LDS + c], s);
-          X[r * LDS + c] = -s / L[r * LDS + r];
-        }
-      }
-    }
-    __syncthreads();
-    if (b == 3) break;
-    // Panel rows below: P := P D^{-T}, out[r][c] = sum_{k<=c} P[r][k] Dinv[c][k].
-    const int nr = TB - B0 - 16;
-    double out[3];
-    int no = 0;
-    for (int e = tid; e < nr * 16; e += 256) {
-      const int r = B0 + 16 + e / 16, c = e % 16;
-      double s = 0.0;
-      for (int k = 0; k <= c; ++k) s = __fma_rn(L[r * LDS + B0 + k], X[(B0 + c) * LDS + B0 + k], s);
-      out[no++] = s;
-    }
-    __syncthreads();
-    no = 0;
-    for (int e = tid; e < nr * 16; e += 256) L[(B0 + 16 + e / 16) * LDS + B0 + e % 16] = out[no++];
-    __syncthreads();
-    // Trailing block: L[r][c] -= sum_k P[r][k] P[c][k], c <= r.
-    for (int e = tid; e < nr * nr; e += 256) {
-      const int r = B0 + 16 + e / nr, c = B0 + 16 + e % nr;
-      if (c <= r) {
-        double s = L[r * LDS + c];
+  for (int p = 0; p < TB; ++p) {
+    double *c = cv[p & 1];
+    const int pb = p >> 2, pr = p & 3;
+    if (bi == pb) {  // row p: L^{-1}[p][s] for s < p, the pivot at s = p
 #pragma unroll
-        for (int k = 0; k < 16; ++k) s = __fma_rn(-L[r * LDS + B0 + k], L[c * LDS + B0 + k], s);
-        L[r * LDS + c] = s;
+      for (int b = 0; b < 4; ++b)
+        if (4 * bs + b <= p) {
+          double x = v[0][b];
+          if (pr == 1) x = v[1][b];
+          if (pr == 2) x = v[2][b];
+          if (pr == 3) x = v[3][b];
+          c[4 * bs + b] = x;
+        }
+    }
+    if (bs == pb) {  // column p below the pivot: A[i][p], i > p
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (4 * bi + r > p) {
+          double x = v[r][0];
+          if (pr == 1) x = v[r][1];
+          if (pr == 2) x = v[r][2];
+          if (pr == 3) x = v[r][3];
+          c[4 * bi + r] = x;
+        }
+    }
+    __syncthreads();
+    const double piv = c[p];
+    bad |= !(piv > 0.0);
+    const double inv = 1.0 / piv;
+    double cs[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) cs[b] = c[4 * bs + b];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = 4 * bi + r;
+      if (i > p) {
+        const double m = c[i] * inv;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int sc = 4 * bs + b;
+          if (sc == p) v[r][b] = -m;
+          else if (sc <= i) v[r][b] = __fma_rn(-m, cs[b], v[r][b]);
+        }
       }
     }
-    __syncthreads();
   }
-  // Off-diagonal blocks of X, block row by block row.
-  for (int b = 1; b < 4; ++b) {
-    const int B0 = 16 * b;
-    // Z[r][c] = sum_{c <= k < B0} L[B0 + r][k] X[k][c] for c < B0 (16 x B0).
-    double z[3];
-    int nz = 0;
-    for (int e = tid; e < 16 * B0; e += 256) {
-      const int r = e / B0, c = e % B0;
-      double s = 0.0;
-      for (int k = c; k < B0; ++k) s = __fma_rn(L[(B0 + r) * LDS + k], X[k * LDS + c], s);
-      z[nz++] = s;
-    }
-    // X[B0 + r][c] = -sum_{k<=r} Dinv[r][k] Z[k][c].
-    __syncthreads();
-    nz = 0;
-    for (int e = tid; e < 16 * B0; e += 256) zs[e / B0][e % B0] = z[nz++];
-    __syncthreads();
-    for (int e = tid; e < 16 * B0; e += 256) {
-      const int r = e / B0, c = e % B0;
-      double s = 0.0;
-      for (int k = 0; k <= r; ++k) s = __fma_rn(X[(B0 + r) * LDS + B0 + k], zs[k][c], s);
-      X[(B0 + r) * LDS + c] = -s;
-    }
-    __syncthreads();
+  // X[i][s] = L^{-1}[i][s] / sqrt(d_i); d_i is the final diagonal slot.
+  __shared__ double dis[TB];
+  if (bi == bs) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) dis[4 * bi + r] = 1.0 / sqrt(v[r][r]);
   }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int i = 4 * bi + r;
+    const double di = dis[i];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int sc = 4 * bs + b;
+      Xs[i * LDS + sc] = sc < i ? v[r][b] * di : (sc == i ? di : 0.0);
+    }
+  }
+  __syncthreads();
   // y_j = X r_j (first F columns of the residual tile).
   double yv[2];
   int ny = 0;
   for (int e = tid; e < TB * F; e += 256) {
     const int r = e / F, f = e % F;
     double s = 0.0;
-    for (int k = 0; k <= r; ++k) s = __fma_rn(X[r * LDS + k], ys[k][f], s);
+    for (int k = 0; k <= r; ++k) s = __fma_rn(Xs[r * LDS + k], ys[k][f], s);
     yv[ny++] = s;
   }
   ny = 0;
@@ -234,10 +237,8 @@ __global__ void __launch_bounds__(256) k_diag_chol(BigArgs a, const BigSlot *__r
   double *gi = a.inv + sl.inv + int64_t(j) * TB * TB;
   for (int idx = tid; idx < TB * TB / 2; idx += 256) {
     const int r = idx >> 5, c2 = idx & 31;
-    *reinterpret_cast<double2 *>(g + int64_t(r) * ld + 2 * c2) =
-        *reinterpret_cast<const double2 *>(L + r * LDS + 2 * c2);
     *reinterpret_cast<double2 *>(gi + r * TB + 2 * c2) =
-        *reinterpret_cast<const double2 *>(X + r * LDS + 2 * c2);
+        *reinterpret_cast<const double2 *>(Xs + r * LDS + 2 * c2);
   }
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
