@@ -22,46 +22,9 @@
 #include <cstdlib>
 #include <vector>
 
-#include "plan.hpp"
-#include "poly.cuh"
+#include "patch.cuh"
 
 namespace pacman_b200 {
-
-enum SolveMode {
-  kLU = 0,   // forward, unpivoted LU (the reference algorithm)
-  kChol = 1, // forward, Cholesky
-  kAdj = 2,  // transpose (adjoint) solve with Cholesky: g = z - Q'G'^{-1}(Q'^T z - V'^T h)
-};
-
-enum PatchStatus : int {
-  kStatusDropped = 1,     // the polynomial block lost at least one axis
-  kStatusNonFinite = 2,   // a non-finite local value
-  kStatusBreakdown = 4,   // non-positive Cholesky pivot
-};
-
-struct PatchArgs {
-  const double4 *src;
-  const double4 *tgt;
-  const double *vals;
-  const int64_t *soff;
-  const int *sidx;
-  const int64_t *toff;
-  const int *tidx;
-  const double4 *centers;
-  double *local;
-  int *status;
-  double *gA;             // global workspace (patches whose A does not fit in smem)
-  const int64_t *gAoff;   // per list entry offset into gA, or nullptr
-  double rinv;            // 1 / support radius
-  int F;
-  int dim;
-  int basis;
-  double *alpha_out;      // forward: RBF coefficients per (patch, source), or null
-  double *beta_out;       // forward: polynomial coefficients, K x 4*kMaxF, or null
-  int *act_out;           // forward: active axes, K x 3, or null
-  const double *h;        // adjoint: weighted upstream gradient per (patch, target)
-  double *g_out;          // adjoint: result per (patch, source)
-};
 
 constexpr int kSolveThreads = 256;
 constexpr int kWarps = kSolveThreads / 32;
@@ -434,8 +397,11 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
   for (auto &r : ranges) {
     int nmax = 0;
     for (size_t i = r.first; i < r.second; ++i) nmax = std::max(nmax, p.n_host[small[i]]);
-    launch(mode, a, list.as<int>() + r.first, int(r.second - r.first), 0,
-           smem_bytes(nmax, F, true), st);
+    if (mode == kChol && nmax <= 64)
+      launch_small_chol(a, list.as<int>() + r.first, int(r.second - r.first), nmax, st);
+    else
+      launch(mode, a, list.as<int>() + r.first, int(r.second - r.first), 0,
+             smem_bytes(nmax, F, true), st);
   }
   if (!big.empty()) {
     std::vector<int64_t> offs(big.size());
@@ -463,10 +429,12 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
                const BigExtra &extra);
 
-// Patches above this size use the blocked engine (blocked.cu).
-static int big_threshold() {
+// Patches above this size use the blocked engine (blocked.cu): 64 for the
+// Cholesky path (the register kernels of small.cu take n <= 64), 128 for the
+// LU and adjoint paths.  PACMAN_B200_BIG_N overrides both.
+static int big_threshold(int mode) {
   const char *e = std::getenv("PACMAN_B200_BIG_N");
-  return e ? std::max(1, std::atoi(e)) : 128;
+  return e ? std::max(1, std::atoi(e)) : (mode == kChol ? 64 : 128);
 }
 
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
@@ -507,13 +475,13 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   a.F = F;
   a.dim = p.dim;
   a.basis = basis;
-  const int nbig = big_threshold();
+  const int mode = precision == PACMAN_B200_FP64 ? kLU : kChol;
+  const int nbig = big_threshold(mode);
   std::vector<int> small, big;
   for (int k = 0; k < K; ++k) {
     if (p.m_host[k] == 0) continue;  // no target: the patch contributes nothing
     (p.n_host[k] > nbig ? big : small).push_back(k);
   }
-  const int mode = precision == PACMAN_B200_FP64 ? kLU : kChol;
   cudaEvent_t ev0, ev1;
   PB_CUDA(cudaEventCreate(&ev0));
   PB_CUDA(cudaEventCreate(&ev1));
@@ -571,7 +539,7 @@ void solve_adjoint(Plan &p, int basis, int F, const double *h, double *g_out, So
   a.basis = basis;
   a.h = h;
   a.g_out = g_out;
-  const int nbig = big_threshold();
+  const int nbig = big_threshold(kAdj);
   std::vector<int> small, big;
   for (int k = 0; k < K; ++k) {
     if (p.m_host[k] == 0) continue;  // h = 0 there: g = 0 (the caller zeroes g)
