@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
   }
   __syncthreads();
   if (a.mode == kBigAdjoint) {
-    if (tid < nred + 6) a.red_out[int64_t(blockIdx.x) * kRedVals + tid] = redf[tid];
+    if (tid < nred + 6) a.red_out[int64_t(sl.q) * kRedVals + tid] = redf[tid];
     return;
   }
   if (tid == 0) {
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
     const int dropped = poly_block(redf, F, a.dim, shift, beta_s, act);
     for (int d = 0; d < 3; ++d) act_s[d] = act[d];
     a.status[sl.k] = dropped ? 1 : 0;
-    for (int v = 0; v < 4 * kMaxF; ++v) a.beta[blockIdx.x * 4 * kMaxF + v] = beta_s[v];
-    for (int d = 0; d < 3; ++d) a.act[blockIdx.x * 3 + d] = act[d];
+    for (int v = 0; v < 4 * kMaxF; ++v) a.beta[sl.q * 4 * kMaxF + v] = beta_s[v];
+    for (int d = 0; d < 3; ++d) a.act[sl.q * 3 + d] = act[d];
     if (a.mode == kBigForwardSave) {
       for (int v = 0; v < 4 * kMaxF; ++v) a.beta_out[int64_t(sl.k) * 4 * kMaxF + v] = beta_s[v];
       for (int d = 0; d < 3; ++d) a.act_out[int64_t(sl.k) * 3 + d] = act[d];
@@ -457,8 +457,8 @@ __global__ void k_big_finish(BigArgs a, const BigSlot *__restrict__ slots) {
   const BigSlot sl = slots[blockIdx.x];
   const int F = a.F;
   const int64_t t0 = a.toff[sl.k];
-  const double *beta = a.beta + blockIdx.x * 4 * kMaxF;
-  const int *act = a.act + blockIdx.x * 3;
+  const double *beta = a.beta + sl.q * 4 * kMaxF;
+  const int *act = a.act + sl.q * 3;
   const double *S = a.W + sl.base + int64_t(sl.T) * TB * sl.ld + int64_t(sl.T) * TB;
   int bad = 0;
   for (int i = threadIdx.x; i < sl.m; i += blockDim.x) {
@@ -570,11 +570,10 @@ __global__ void __launch_bounds__(256) k_big_adj_finish(BigArgs a, const BigSlot
   const int64_t s0 = a.soff[sl.k], t0 = a.toff[sl.k];
   const double4 c = a.centers[sl.k];
   const double shift[3] = {c.x, c.y, c.z};
-  const double *rcol = a.W + sl.base + int64_t(sl.T) * TB;
   __shared__ int S_s[4], pv_s;
   __shared__ double R_s[4][4];
   if (tid == 0) {
-    const double *redf = a.red_out + int64_t(blockIdx.x) * kRedVals;
+    const double *redf = a.red_out + int64_t(sl.q) * kRedVals;
     int S[4], pv;
     double R[4][4];
     poly_axes(redf, a.dim, shift, redf + 10, redf + 13, S, pv, R);
@@ -589,7 +588,7 @@ __global__ void __launch_bounds__(256) k_big_adj_finish(BigArgs a, const BigSlot
     double u[4] = {0, 0, 0, 0}, v[4] = {0, 0, 0, 0};
     for (int j = tid; j < sl.n; j += blockDim.x) {
       const double4 x = a.src[a.sidx[s0 + j]];
-      const double z = rcol[int64_t(j) * sl.ld + f];
+      const double z = a.zc[sl.zoff + int64_t(j) * F + f];
       const double q[4] = {1.0, x.x - shift[0], x.y - shift[1], x.z - shift[2]};
       for (int c2 = 0; c2 < 4; ++c2) u[c2] += q[c2] * z;
     }
@@ -629,7 +628,7 @@ __global__ void __launch_bounds__(256) k_big_adj_finish(BigArgs a, const BigSlot
     const double4 x = a.src[a.sidx[s0 + j]];
     const double q[4] = {1.0, x.x - shift[0], x.y - shift[1], x.z - shift[2]};
     for (int f = 0; f < F; ++f) {
-      double g = rcol[int64_t(j) * sl.ld + f];
+      double g = a.zc[sl.zoff + int64_t(j) * F + f];
       for (int c2 = 0; c2 < 4; ++c2) g -= q[c2] * corr[4 * f + c2];
       if (!isfinite(g)) bad = 1;
       a.g_out[(s0 + j) * F + f] = g;
@@ -734,7 +733,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     // One wave: as many patches as fit the workspace budget.
     std::vector<BigSlot> slots;
     size_t tot = 0;
-    int64_t tot_inv = 0;
+    int64_t tot_inv = 0, tot_z = 0;
     while (pos < order.size()) {
       const int k = order[pos];
       const int n = p.n_host[k], m = p.m_host[k];
@@ -745,6 +744,9 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       q.T = (n + TB - 1) / TB;
       q.TE = lu ? (m + TB - 1) / TB : 0;
       q.inv = lu ? int64_t(slots.size()) * 2 * TB * TB : tot_inv;
+      q.q = int(slots.size());
+      q.zoff = tot_z;
+      tot_z += int64_t(q.T) * TB * F;
       tot_inv += int64_t(q.T) * TB * TB;
       q.ld = (q.T + 1) * TB;
       q.k = k;
@@ -768,9 +770,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       pre_asm[q + 1] = int(v);
     }
     // LU: per step the trsm and update-strip prefix counts over the active
-    // slots (a prefix of the sorted slots); Cholesky: chol_prefix.
+    // slots (a prefix of the sorted slots); Cholesky: per slot group below.
     std::vector<int> cnt(steps), off(steps + 1, 0), pre;
-    CholPlan cp;
     if (lu) {
       pre.reserve(size_t(steps) * 2 * (ns + 1));
       for (int s = 0; s < steps; ++s) {
@@ -790,12 +791,14 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
         }
       }
       off[steps] = int(pre.size());
-    } else {
-      cp = chol_prefix(slots);
-      pre = cp.pre;
     }
     DevMem dW, dsmall;
     dW.alloc(sizeof(double) * tot, st);
+    DevMem dzc;
+    if (!lu) {
+      dzc.alloc(sizeof(double) * size_t(tot_z), st);
+      a.zc = dzc.as<double>();
+    }
     const size_t n_inv = lu ? size_t(2) * TB * TB * ns : size_t(tot_inv);
     const size_t n_beta = size_t(4) * kMaxF * ns;
     const size_t n_red = size_t(kRedVals) * ns;
@@ -829,11 +832,38 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       note_launch();
     }
     if (!lu) {
-      chol_launch_steps(a, ds, cp, dpre, st);
-      chol_launch_finish(a, ds, ns, adjoint, st);
-      if (adjoint) {
-        k_big_adj_finish<<<ns, 256, 0, st>>>(a, ds);
-        note_launch();
+      // Interleaved groups of slots, each stepping in lockstep on its own
+      // stream: the short diagonal and trsm launches and the tails of one
+      // group's column updates overlap the other groups' work.
+      const int G = std::min<int>(AuxStreams::kN, std::max(1, ns / 8));
+      std::vector<std::vector<BigSlot>> gs(G);
+      for (int q = 0; q < ns; ++q) gs[q % G].push_back(slots[q]);
+      std::vector<CholPlan> gp(G);
+      std::vector<DevMem> gmem(G);
+      std::vector<BigSlot *> gds(G);
+      std::vector<int *> gpre(G);
+      for (int g = 0; g < G; ++g) {
+        gp[g] = chol_prefix(gs[g]);
+        gmem[g].alloc(sizeof(BigSlot) * gs[g].size() + sizeof(int) * gp[g].pre.size() + 64, st);
+        gds[g] = gmem[g].as<BigSlot>();
+        gpre[g] = reinterpret_cast<int *>(gmem[g].as<char>() +
+                                          ((sizeof(BigSlot) * gs[g].size() + 15) & ~size_t(15)));
+        arena.upload(gs[g].data(), gs[g].size(), gds[g], st);
+        arena.upload(gp[g].pre.data(), gp[g].pre.size(), gpre[g], st);
+      }
+      p.aux.make();
+      PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN], st));
+      for (int g = 0; g < G; ++g) {
+        cudaStream_t sg = p.aux.s[g];
+        PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
+        chol_launch_steps(a, gds[g], gp[g], gpre[g], sg);
+        chol_launch_finish(a, gds[g], int(gs[g].size()), adjoint, sg);
+        if (adjoint) {
+          k_big_adj_finish<<<int(gs[g].size()), 256, 0, sg>>>(a, gds[g]);
+          note_launch();
+        }
+        PB_CUDA(cudaEventRecord(p.aux.ev[g], sg));
+        PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[g], 0));
       }
       PB_CUDA(cudaGetLastError());
       continue;

@@ -23,6 +23,8 @@ struct BigSlot {
   int k;         // patch id
   int n, m;
   int64_t inv;   // offset (doubles) of the slot's inverse tiles
+  int q;         // index of the slot in its wave (per-slot arrays beta, act, red)
+  int64_t zoff;  // offset (doubles) of the slot's backward-sweep solution in zc
 };
 
 // Work of one launch is addressed by blockIdx.x through prefix counts over
@@ -160,6 +162,7 @@ struct BigArgs {
   double *g_out;       // adjoint: result per (patch, source)
   double *red_out;     // adjoint: per slot reduced moments (kRedVals)
   double *alpha_c;     // Cholesky forward: RBF coefficients per (patch, source)
+  double *zc;          // Cholesky: backward-sweep solution per slot (T*TB x F)
 };
 
 // Left-looking Cholesky steps, backward sweep and local evaluation of one

@@ -33,8 +33,6 @@ constexpr size_t kColSmem = size_t(kStages) * kColStage * sizeof(double);
 constexpr int kTrsmStrip = 4;           // row tiles per triangular-solve CTA
 constexpr size_t kTrsmSmem = (size_t(3) * TB * LDS + TB * kMaxF) * sizeof(double);
 constexpr size_t kDiagSmem = size_t(TB) * LDS * sizeof(double);
-constexpr int kBackStages = 3;
-constexpr size_t kBackSmem = size_t(kBackStages) * TB * LDS * sizeof(double);
 
 // acc += A B^T over one K chunk: A rows wr.., B rows wc.. (both K-contiguous).
 __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
@@ -320,73 +318,76 @@ __global__ void __launch_bounds__(128, 2)
 
 // Backward sweep L^T z = y of one slot (CTA per slot), tile row by tile row
 // from the last: z_s = X_s^T (y_s - sum_{t>s} L[t, s]^T z_t), with the tile
-// inverses X_s of the factorisation.  The column tiles L[t, s] stream through
-// a cp.async ring.  z overwrites y in the residual column and goes to alpha_c
-// (forward) per (patch, source).
-__global__ void __launch_bounds__(256) k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
-  extern __shared__ double sm[];
-  __shared__ double part[4][TB][kMaxF];
+// inverses X_s of the factorisation.  Warp w takes the tiles t = s + 1 + w,
+// s + 9 + w, ... of column s and streams them from global memory (lane: two
+// columns, every row coalesced); the warps' partial sums meet in shared
+// memory.  z goes to zc (per slot) and, in the forward, to alpha_c per
+// (patch, source).
+__global__ void __launch_bounds__(256, 3) k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
+  __shared__ double part[8][TB][kMaxF];
   __shared__ double accs[TB][kMaxF];
-  __shared__ double zt[TB][kMaxF];
   const BigSlot sl = slots[blockIdx.x];
-  const int F = a.F, tid = threadIdx.x;
+  const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ld = sl.ld;
-  double *W = a.W + sl.base;
-  double *rcol = W + int64_t(sl.T) * TB;
-  const int r = tid & 63, quarter = tid >> 6;
+  const double *W = a.W + sl.base;
+  const double *rcol = W + int64_t(sl.T) * TB;
+  double *zc = a.zc + sl.zoff;
+  const int rr = tid & 63, quarter = tid >> 6;
   for (int s = sl.T - 1; s >= 0; --s) {
-    const int nt = sl.T - 1 - s;  // tiles t = s + 1 .. T - 1
-    double pacc[kMaxF];
+    double acc0[kMaxF], acc1[kMaxF];
 #pragma unroll
-    for (int f = 0; f < kMaxF; ++f) pacc[f] = 0.0;
-#pragma unroll
-    for (int u = 0; u < kBackStages - 1; ++u) {
-      if (u < nt)
-        async_tile(sm + u * TB * LDS, W + int64_t(s + 1 + u) * TB * ld + int64_t(s) * TB, ld, tid,
-                   256);
-      cp_async_commit();
-    }
-    for (int u = 0; u < nt; ++u) {
-      const int t = s + 1 + u;
-      cp_async_wait<kBackStages - 2>();
-      __syncthreads();
-      if (u + kBackStages - 1 < nt)
-        async_tile(sm + ((u + kBackStages - 1) % kBackStages) * TB * LDS,
-                   W + int64_t(t + kBackStages - 1) * TB * ld + int64_t(s) * TB, ld, tid, 256);
-      cp_async_commit();
-      for (int e = tid; e < TB * kMaxF; e += 256) {
-        const int c = e / kMaxF, f = e % kMaxF;
-        zt[c][f] = f < F ? rcol[int64_t(t * TB + c) * ld + f] : 0.0;
-      }
-      __syncthreads();
-      const double *tile = sm + (u % kBackStages) * TB * LDS;
-#pragma unroll 4
-      for (int c = quarter; c < TB; c += 4) {
-        const double l = tile[c * LDS + r];
+    for (int f = 0; f < kMaxF; ++f) acc0[f] = acc1[f] = 0.0;
+    for (int t = s + 1 + warp; t < sl.T; t += 8) {
+      const double *tile = W + int64_t(t) * TB * ld + int64_t(s) * TB;
+      const double *zt = zc + int64_t(t) * TB * F;
+#pragma unroll 8
+      for (int c = 0; c < TB; ++c) {
+        const double l0 = tile[int64_t(c) * ld + lane], l1 = tile[int64_t(c) * ld + lane + 32];
 #pragma unroll
         for (int f = 0; f < kMaxF; ++f)
-          if (f < F) pacc[f] = __fma_rn(l, zt[c][f], pacc[f]);
+          if (f < F) {
+            const double z = zt[c * F + f];
+            acc0[f] = __fma_rn(l0, z, acc0[f]);
+            acc1[f] = __fma_rn(l1, z, acc1[f]);
+          }
       }
     }
-    cp_async_wait<0>();
 #pragma unroll
-    for (int f = 0; f < kMaxF; ++f) part[quarter][r][f] = pacc[f];
-    __syncthreads();
-    for (int e = tid; e < TB * F; e += 256) {
-      const int rr = e / F, f = e % F;
-      accs[rr][f] = rcol[int64_t(s * TB + rr) * ld + f] -
-                    (part[0][rr][f] + part[1][rr][f] + part[2][rr][f] + part[3][rr][f]);
+    for (int f = 0; f < kMaxF; ++f) {
+      part[warp][lane][f] = acc0[f];
+      part[warp][lane + 32][f] = acc1[f];
     }
     __syncthreads();
-    // z_s[rr] = sum_{c >= rr} X[c][rr] acc[c]  (X lower triangular).
-    const double *xs = a.inv + sl.inv + int64_t(s) * TB * TB;
     for (int e = tid; e < TB * F; e += 256) {
-      const int rr = e % TB, f = e / TB;
-      double z = 0.0;
-      for (int c = rr; c < TB; ++c) z = __fma_rn(xs[c * TB + rr], accs[c][f], z);
-      rcol[int64_t(s * TB + rr) * ld + f] = z;
-      const int jj = s * TB + rr;
-      if (a.alpha_c != nullptr && jj < sl.n) a.alpha_c[(a.soff[sl.k] + jj) * F + f] = z;
+      const int r = e / F, f = e % F;
+      double sum = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) sum += part[w][r][f];
+      accs[r][f] = rcol[int64_t(s * TB + r) * ld + f] - sum;
+    }
+    __syncthreads();
+    // z_s[rr][f] = sum_{c >= rr} X_s[c][rr] acc_s[c][f]; quarters of c, then summed.
+    const double *xs = a.inv + sl.inv + int64_t(s) * TB * TB;
+    double zp[kMaxF];
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) zp[f] = 0.0;
+#pragma unroll 4
+    for (int c = quarter; c < TB; c += 4) {
+      if (c < rr) continue;
+      const double x = xs[c * TB + rr];
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f)
+        if (f < F) zp[f] = __fma_rn(x, accs[c][f], zp[f]);
+    }
+#pragma unroll
+    for (int f = 0; f < kMaxF; ++f) part[quarter][rr][f] = zp[f];
+    __syncthreads();
+    for (int e = tid; e < TB * F; e += 256) {
+      const int r = e / F, f = e % F;
+      const double z = part[0][r][f] + part[1][r][f] + part[2][r][f] + part[3][r][f];
+      const int j = s * TB + r;
+      zc[int64_t(j) * F + f] = z;
+      if (a.alpha_c != nullptr && j < sl.n) a.alpha_c[(a.soff[sl.k] + j) * F + f] = z;
     }
     __syncthreads();
   }
@@ -397,8 +398,8 @@ __global__ void __launch_bounds__(256) k_chol_eval(BigArgs a, const BigSlot *__r
   const BigSlot sl = slots[blockIdx.x];
   const int F = a.F, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t s0 = a.soff[sl.k], t0 = a.toff[sl.k];
-  const double *beta = a.beta + blockIdx.x * 4 * kMaxF;
-  const int *act = a.act + blockIdx.x * 3;
+  const double *beta = a.beta + sl.q * 4 * kMaxF;
+  const int *act = a.act + sl.q * 3;
   const double *alpha = a.alpha_c + s0 * F;
   int bad = 0;
   for (int i = warp; i < sl.m; i += 8) {
@@ -473,8 +474,6 @@ void chol_set_smem_attributes() {
                                int(kDiagSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_col_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kTrsmSmem)));
-  PB_CUDA(cudaFuncSetAttribute(k_chol_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(kBackSmem)));
   done = true;
 }
 
@@ -502,7 +501,7 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, 
 
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st) {
-  k_chol_back<<<ns, 256, kBackSmem, st>>>(a, ds);
+  k_chol_back<<<ns, 256, 0, st>>>(a, ds);
   note_launch();
   if (!adjoint) {
     k_chol_eval<<<ns, 256, 0, st>>>(a, ds);

@@ -63,6 +63,37 @@ struct DevGrid {
   DevMem start, items;
 };
 
+// Extra streams of a plan for independent groups of large patches, created
+// on first use on the plan's device; every use joins them back into the
+// plan's stream with events before the call returns.
+struct AuxStreams {
+  static constexpr int kN = 4;
+  cudaStream_t s[kN] = {};
+  cudaEvent_t ev[kN + 1] = {};
+  bool made = false;
+  void make() {
+    if (made) return;
+    for (int i = 0; i < kN; ++i) {
+      if (cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking) != cudaSuccess)
+        throw Error{PACMAN_B200_ERR_CUDA, "cudaStreamCreateWithFlags failed"};
+    }
+    for (int i = 0; i <= kN; ++i) {
+      if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
+        throw Error{PACMAN_B200_ERR_CUDA, "cudaEventCreateWithFlags failed"};
+    }
+    made = true;
+  }
+  AuxStreams() = default;
+  AuxStreams(const AuxStreams &) = delete;
+  AuxStreams &operator=(const AuxStreams &) = delete;
+  ~AuxStreams() {
+    for (int i = 0; i < kN; ++i)
+      if (s[i]) cudaStreamDestroy(s[i]);
+    for (int i = 0; i <= kN; ++i)
+      if (ev[i]) cudaEventDestroy(ev[i]);
+  }
+};
+
 struct Plan {
   int dim = 3;
   int64_t n = 0, m = 0;
@@ -94,6 +125,7 @@ struct Plan {
   DevMem src_t_off, src_t_pos;  // sources -> (patch, slot) transpose of the membership lists
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
+  AuxStreams aux;
 };
 
 // Pinned host staging for the small host-to-device uploads of one call.  A
