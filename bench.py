@@ -358,18 +358,29 @@ def main():
         extra["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(out_mixed - out64) / np.linalg.norm(out64))
         extra["fp64_ms_factor"] = f64_stats.get("ms_factor")
 
-    # Roofline of the dominant kernel (the dense patch factorisations).
+    # Roofline of the dominant kernel, the column update of the large-patch
+    # Cholesky (k_col_update): one extra transfer after the timed region with
+    # CUDA events around each of its launches, on the stream it runs on.
     peak = fp64_gemm_peak(torch, dev)
-    ms_factor = stats.get("ms_factor", 0.0)
-    achieved = stats.get("factor_flops", 0.0) / (ms_factor * 1e-3) / 1e12 if ms_factor else 0.0
-    roofline = {"bound": "fp64", "kernel": "patch factorisation (k_patch_solve + blocked engine)",
+    kst = {}
+    plan = pacman.rbf.Plan(3, S, T, precision=args.precision, **kw)
+    plan.execute(w["basis"], V, stats=kst, time_kernels=True)
+    plan.close()
+    ms_upd = kst.get("ms_update", 0.0)
+    achieved = kst.get("update_flops", 0.0) / (ms_upd * 1e-3) / 1e12 if ms_upd else 0.0
+    nl = max(1, int(kst.get("update_launches", 0)))
+    roofline = {"bound": "fp64", "kernel": "k_col_update (left-looking Cholesky column update, "
+                                           "FP64 tensor cores)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
-                "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64 has no faster "
-                               "tensor path on B200)",
+                "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 has no "
+                               "faster path on B200; MEASURED_PEAKS.json holds no FP64 figure)",
                 "traffic": read_traffic(args.workload),
-                "ms_factor_per_step": ms_factor,
-                "share_of_step": ms_factor / ms_per_step if ms_per_step else None}
+                "flops_per_launch": kst.get("update_flops", 0.0) / nl,
+                "ms_per_launch": ms_upd / nl,
+                "launches_per_step": nl,
+                "ms_update_per_step": ms_upd,
+                "share_of_step": ms_upd / ms_per_step if ms_per_step else None}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

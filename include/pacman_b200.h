@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PACMAN_B200_ABI_VERSION 1
+#define PACMAN_B200_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PACMAN_B200_API __attribute__((visibility("default")))
@@ -86,6 +86,12 @@ typedef struct pacman_b200_stats {
   int64_t kernel_launches;  /* this library's kernel launches in the call */
   double ms_factor;         /* device time of the dense factorisations */
   double factor_flops;      /* algorithmic FLOPs of those factorisations */
+  /* With PACMAN_B200_TIME_KERNELS: summed CUDA-event duration, algorithmic
+   * FLOPs (2 * 64^3 per tile product) and launch count of the trailing
+   * column update of the large-patch Cholesky (the dominant kernel). */
+  double ms_update;
+  double update_flops;
+  int64_t update_launches;
 } pacman_b200_stats;
 
 /* Fills the reference's defaults (50, 0.15, 0.1, FP64, current device). */
@@ -129,6 +135,9 @@ PACMAN_B200_API void pacman_b200_plan_destroy(pacman_b200_plan *plan);
  *                                               at fixed patch membership
  *                                               (may be NULL). */
 #define PACMAN_B200_SAVE_FOR_ADJOINT 1u
+/* Times every launch of the dominant kernel with CUDA events on its stream
+ * (one slot group, no concurrent groups) and reports it in the stats. */
+#define PACMAN_B200_TIME_KERNELS 2u
 PACMAN_B200_API int pacman_b200_plan_execute_ex(pacman_b200_plan *plan, int32_t rbf_function,
                                                 const double *source_values, int32_t n_fields,
                                                 double *target_values, uint32_t flags,

@@ -24,6 +24,7 @@ ERR_LIMIT = -6
 FP64 = 0
 MIXED = 1
 SAVE_FOR_ADJOINT = 1
+TIME_KERNELS = 2
 
 _lock = threading.Lock()
 _lib = None
@@ -58,6 +59,9 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_int64),
         ("ms_factor", ctypes.c_double),
         ("factor_flops", ctypes.c_double),
+        ("ms_update", ctypes.c_double),
+        ("update_flops", ctypes.c_double),
+        ("update_launches", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:

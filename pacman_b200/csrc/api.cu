@@ -234,6 +234,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
         InBuf v;
         v.stage(vals, size_t(p.n) * F, p.device, st);
         p.local.alloc(sizeof(double) * size_t(std::max<int64_t>(p.tnnz, 1)) * F, st);
+        rep.time_kernels = (flags & PACMAN_B200_TIME_KERNELS) != 0;
         solve_patches(p, basis, v.ptr, F, p.opts.precision, p.local.as<double>(), rep,
                       (flags & PACMAN_B200_SAVE_FOR_ADJOINT) != 0);
         PB_CUDA(cudaEventRecord(e1, st));
@@ -275,6 +276,9 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       stats->kernel_launches = launch_counter() - launches0 + p.launches_geometry;
       stats->ms_factor = rep.ms_factor;
       stats->factor_flops = rep.factor_flops;
+      stats->ms_update = rep.ms_update;
+      stats->update_flops = rep.update_flops;
+      stats->update_launches = rep.update_launches;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -175,8 +175,8 @@ struct CholPlan {
 };
 CholPlan chol_prefix(const std::vector<BigSlot> &slots);
 void chol_set_smem_attributes();
-void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, const int *dpre,
-                       cudaStream_t st);
+void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,
+                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep);
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st);
 

@@ -477,9 +477,14 @@ void chol_set_smem_attributes() {
   done = true;
 }
 
-void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, const int *dpre,
-                       cudaStream_t st) {
+void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,
+                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep) {
   const int steps = int(cp.cnt.size());
+  std::vector<cudaEvent_t> ev;
+  if (rep.time_kernels) {
+    ev.resize(2 * size_t(steps));
+    for (auto &e : ev) PB_CUDA(cudaEventCreate(&e));
+  }
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
     const int *pu = dpre + cp.off[j];
@@ -487,8 +492,15 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, 
     const int nu = cp.pre[cp.off[j] + c];
     const int nt = cp.pre[cp.off[j] + c + 1 + c];
     if (nu) {
+      if (rep.time_kernels) PB_CUDA(cudaEventRecord(ev[2 * j], st));
       k_col_update<<<nu, kColThreads, kColSmem, st>>>(a, ds, pu, c, j);
       note_launch();
+      if (rep.time_kernels) {
+        PB_CUDA(cudaEventRecord(ev[2 * j + 1], st));
+        for (int q = 0; q < c; ++q)
+          rep.update_flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j);
+        ++rep.update_launches;
+      }
     }
     k_diag_chol<<<c, 256, kDiagSmem, st>>>(a, ds, j);
     note_launch();
@@ -496,6 +508,16 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const CholPlan &cp, 
       k_col_trsm<<<nt, 128, kTrsmSmem, st>>>(a, ds, pt, c, j);
       note_launch();
     }
+  }
+  if (rep.time_kernels) {
+    PB_CUDA(cudaStreamSynchronize(st));
+    for (int j = 0; j < steps; ++j) {
+      if (cp.pre[cp.off[j] + cp.cnt[j]] == 0) continue;
+      float ms = 0.f;
+      PB_CUDA(cudaEventElapsedTime(&ms, ev[2 * j], ev[2 * j + 1]));
+      rep.ms_update += ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
   }
 }
 

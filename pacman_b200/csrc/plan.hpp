@@ -167,6 +167,9 @@ struct SolveReport {
   int64_t patches_fp32 = 0, patches_fp64 = 0, patches_fallback = 0, dropped = 0;
   double ms_factor = 0.0;     // device time of the factorisation launches
   double factor_flops = 0.0;  // their algorithmic FLOPs
+  bool time_kernels = false;  // input: event-time the column-update launches
+  double ms_update = 0.0, update_flops = 0.0;
+  int64_t update_launches = 0;
 };
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
                    double *local_dev, SolveReport &rep, bool save_state = false);
