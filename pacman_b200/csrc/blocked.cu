@@ -22,6 +22,7 @@
 // (lower tiles only, half the work) and flags non-positive pivots.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "blocked.cuh"
@@ -835,7 +836,11 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       // Interleaved groups of slots, each stepping in lockstep on its own
       // stream: the short diagonal and trsm launches and the tails of one
       // group's column updates overlap the other groups' work.
-      const int G = rep.time_kernels ? 1 : std::min<int>(AuxStreams::kN, std::max(1, ns / 8));
+      // PACMAN_B200_GROUPS (1..4) overrides the number of slot groups.
+      const char *genv = std::getenv("PACMAN_B200_GROUPS");
+      int G = std::min<int>(AuxStreams::kN, std::max(1, ns / 8));
+      if (genv) G = std::min<int>(AuxStreams::kN, std::max(1, std::atoi(genv)));
+      if (rep.time_kernels) G = 1;
       std::vector<std::vector<BigSlot>> gs(G);
       for (int q = 0; q < ns; ++q) gs[q % G].push_back(slots[q]);
       std::vector<CholPlan> gp(G);
@@ -856,7 +861,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       for (int g = 0; g < G; ++g) {
         cudaStream_t sg = p.aux.s[g];
         PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
-        chol_launch_steps(a, gds[g], gs[g], gp[g], gpre[g], sg, rep);
+        chol_launch_steps(a, gds[g], gs[g], gp[g], gpre[g], sg, rep,
+                          g == 0 ? rep.tail_event : nullptr);
         chol_launch_finish(a, gds[g], int(gs[g].size()), adjoint, sg);
         if (adjoint) {
           k_big_adj_finish<<<int(gs[g].size()), 256, 0, sg>>>(a, gds[g]);

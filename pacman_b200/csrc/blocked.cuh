@@ -169,14 +169,18 @@ struct BigArgs {
 // wave of slots (cholesky.cu).  `pre` holds, per step, the prefix counts of
 // the column-update and triangular-solve launches (see chol_prefix).
 struct CholPlan {
+  int ns = 0;                // slots
   std::vector<int> cnt;      // active slots per step
   std::vector<int> off;      // per step: offset of its prefix arrays in pre
-  std::vector<int> pre;      // per step: update prefix (cnt+1), trsm prefix (cnt+1)
+  std::vector<int> pre;      // per step: prefix of the CTA counts (cnt+1)
 };
 CholPlan chol_prefix(const std::vector<BigSlot> &slots);
 void chol_set_smem_attributes();
+// tail_event (or null) is recorded on st at the first step that leaves SMs
+// idle (fewer than two CTAs per SM), else after the last step.
 void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,
-                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep);
+                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep,
+                       cudaEvent_t tail_event);
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st);
 

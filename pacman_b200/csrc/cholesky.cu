@@ -5,16 +5,17 @@
 // thread (src/rbf_pum/solver/solver.hpp:422-490, KokkosBatched
 // SerialLU<Unblocked>).  A is symmetric positive definite, so here it is
 // factored as L L^T in 64 x 64 tiles, all large patches in lockstep, one tile
-// column j per step:
-//   k_col_update  C[i, j] -= sum_{p<j} L[i, p] L[j, p]^T for every i >= j: the
-//                 accumulator stays in registers for the whole K loop, the
-//                 L panels stream through a cp.async pipeline;
-//   k_diag_chol   X = L[j, j]^{-1} of C[j, j] = L[j, j] L[j, j]^T, y_j = X r_j;
-//   k_col_trsm    L[i, j] = C[i, j] L[j, j]^{-T} for i > j, and the forward
-//                 substitution update r_i -= L[i, j] y_j.
-// Afterwards k_chol_back solves L^T alpha = y (tile inverses kept per step)
-// and k_chol_eval evaluates local = E alpha + V beta (solver.hpp:270-273).
-// The tile products run on the FP64 tensor cores (mma.sync m8n8k4 f64).
+// column j per step and one launch per step (k_col_step):
+//   C[i, j] = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T for every i > j, with the
+//   accumulator in registers for the whole K loop and the L panels streaming
+//   through a cp.async pipeline; then L[i, j] = C X_j^T (X_j = L[j, j]^{-1},
+//   formed one step earlier) and the forward substitution r_i -= L[i, j] y_j;
+//   the CTA of row tile j + 1 also forms, factors and inverts the next
+//   diagonal tile (X_{j+1}, y_{j+1} = X_{j+1} r_{j+1}).
+// k_diag_chol does the diagonal tile of step 0.  Afterwards k_chol_back solves
+// L^T alpha = y (with the kept tile inverses) and k_chol_eval evaluates
+// local = E alpha + V beta (solver.hpp:270-273).  The tile products run on
+// the FP64 tensor cores (mma.sync m8n8k4 f64).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -30,8 +31,6 @@ constexpr int kColRows = 2 * TB;        // rows of one column-update CTA (two ti
 constexpr int kColThreads = 256;
 constexpr int kColStage = (kColRows + TB) * kKLD;  // doubles per pipeline stage
 constexpr size_t kColSmem = size_t(kStages) * kColStage * sizeof(double);
-constexpr int kTrsmStrip = 4;           // row tiles per triangular-solve CTA
-constexpr size_t kTrsmSmem = (size_t(3) * TB * LDS + TB * kMaxF) * sizeof(double);
 constexpr size_t kDiagSmem = size_t(TB) * LDS * sizeof(double);
 
 // acc += A B^T over one K chunk: A rows wr.., B rows wc.. (both K-contiguous).
@@ -53,75 +52,14 @@ __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
   }
 }
 
-// Column update of step j >= 1.  One CTA owns row tiles i0, i0 + 1 (i0 = j +
-// 2l) of tile column j; eight warps each hold a 32 x 32 accumulator, which
-// starts at -C and accumulates the products (no negation in the K loop).
-__global__ void __launch_bounds__(kColThreads, 2)
-    k_col_update(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre,
-                 int cnt, int j) {
-  extern __shared__ double sm[];
-  const int q = find_slot(pre, cnt, blockIdx.x);
-  const BigSlot sl = slots[q];
-  const int i0 = j + 2 * (blockIdx.x - pre[q]);
-  const bool two = i0 + 1 < sl.T;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  const int ld = sl.ld;
-  const double *gA = a.W + sl.base + int64_t(i0) * TB * ld;
-  const double *gB = a.W + sl.base + int64_t(j) * TB * ld;
-  const int arows = two ? kColRows : TB;
-  const int nch = j * (TB / kKC);
-  auto load = [&](int c, int stage) {
-    double *sA = sm + stage * kColStage;
-    double *sB = sA + kColRows * kKLD;
-    const int col = c * kKC;
-    for (int idx = tid; idx < (kColRows + TB) * (kKC / 2); idx += kColThreads) {
-      const int r = idx / (kKC / 2), c2 = idx % (kKC / 2);
-      if (r < kColRows) {
-        if (r < arows) cp_async16(sA + r * kKLD + 2 * c2, gA + int64_t(r) * ld + col + 2 * c2);
-      } else {
-        const int rb = r - kColRows;
-        cp_async16(sB + rb * kKLD + 2 * c2, gB + int64_t(rb) * ld + col + 2 * c2);
-      }
-    }
-  };
+__device__ __forceinline__ void acc_neg(double (&acc)[4][4][2]) {
 #pragma unroll
-  for (int s = 0; s < kStages - 1; ++s) {
-    if (s < nch) load(s, s);
-    cp_async_commit();
-  }
-  const bool active = two || wr < TB;
-  double *C = a.W + sl.base + int64_t(i0) * TB * ld + int64_t(j) * TB;
-  double acc[4][4][2];
-  if (active) {
-    acc_load(acc, C, ld, wr, wc, lane);
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
-  }
-  for (int c = 0; c < nch; ++c) {
-    cp_async_wait<kStages - 2>();
-    __syncthreads();
-    if (c + kStages - 1 < nch) load(c + kStages - 1, (c + kStages - 1) % kStages);
-    cp_async_commit();
-    if (active) {
-      const double *sA = sm + (c % kStages) * kColStage;
-      mma_chunk_nt(sA, sA + kColRows * kKLD, acc, wr, wc, lane);
-    }
-  }
-  cp_async_wait<0>();
-  if (active) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
-    acc_store(acc, C, ld, wr, wc, lane);
-  }
+    for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
 }
 
-// Inverse Cholesky factor of diagonal tile (j, j) of every active slot and
-// y_j = X r_j.  The tile is eliminated as L D L^T with the identity carried
+// Inverse Cholesky factor X of one 64 x 64 tile D and y = X r (256 threads).  The tile is eliminated as L D L^T with the identity carried
 // along (Gauss-Jordan on [A | I]): at pivot p every row i > p gets
 // R_i -= (a_ip / a_pp) R_p, which leaves U = D L^T on the left and L^{-1} on
 // the right.  Each thread owns a 4 x 4 block of registers; slot (i, s) holds
@@ -130,19 +68,16 @@ __global__ void __launch_bounds__(kColThreads, 2)
 // of A below it) and all threads update their slots: one barrier per pivot.
 // Only X = L_c^{-1} = D^{-1/2} L^{-1} is kept (the trsm, the forward and the
 // backward substitution use nothing else).  Non-positive pivots set status 4.
-__global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *__restrict__ slots,
-                                                      int j) {
-  extern __shared__ double sm[];
-  double *Xs = sm;  // TB x LDS, the inverse factor at the end
-  __shared__ double cv[2][TB];
-  __shared__ double ys[TB][kMaxF];
-  const BigSlot sl = slots[blockIdx.x];
+// D: lower part at g (row stride ld, global or shared); r: the first F
+// columns of the residual tile at rg (row stride rld), overwritten with y; X
+// goes to gi (row stride TB).  Xs (TB x LDS), cv, dis and ys are shared
+// scratch.  Returns true on a non-positive pivot.
+__device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, double *gi,
+                          double *Xs,
+                          double (*cv)[TB], double *dis, double (*ys)[kMaxF]) {
   const int tid = threadIdx.x;
   const int bi = tid >> 4, bs = tid & 15;
   bool bad = false;
-  const int ld = sl.ld, F = a.F;
-  const double *g = a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB;
-  double *rg = a.W + sl.base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
   double v[4][4];
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -155,7 +90,7 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
   }
   for (int e = tid; e < TB * kMaxF; e += 256) {
     const int r = e / kMaxF, f = e % kMaxF;
-    ys[r][f] = f < F ? rg[int64_t(r) * ld + f] : 0.0;
+    ys[r][f] = f < F ? rg[int64_t(r) * rld + f] : 0.0;
   }
   for (int p = 0; p < TB; ++p) {
     double *c = cv[p & 1];
@@ -204,7 +139,6 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
     }
   }
   // X[i][s] = L^{-1}[i][s] / sqrt(d_i); d_i is the final diagonal slot.
-  __shared__ double dis[TB];
   if (bi == bs) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) dis[4 * bi + r] = 1.0 / sqrt(v[r][r]);
@@ -231,89 +165,238 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
     yv[ny++] = s;
   }
   ny = 0;
-  for (int e = tid; e < TB * F; e += 256) rg[int64_t(e / F) * ld + e % F] = yv[ny++];
-  double *gi = a.inv + sl.inv + int64_t(j) * TB * TB;
+  for (int e = tid; e < TB * F; e += 256) rg[int64_t(e / F) * rld + e % F] = yv[ny++];
   for (int idx = tid; idx < TB * TB / 2; idx += 256) {
     const int r = idx >> 5, c2 = idx & 31;
     *reinterpret_cast<double2 *>(gi + r * TB + 2 * c2) =
         *reinterpret_cast<const double2 *>(Xs + r * LDS + 2 * c2);
   }
-  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+  return bad;
 }
 
-// Triangular solve of step j for up to kTrsmStrip row tiles i > j of one
-// slot: L[i, j] = C[i, j] X^T (X = L[j, j]^{-1}), then r_i -= L[i, j] y_j.
-__global__ void __launch_bounds__(128, 2)
-    k_col_trsm(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
+// The diagonal tile of step 0 of every slot.
+__global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *__restrict__ slots,
+                                                      int j) {
+  extern __shared__ double sm[];
+  __shared__ double cv[2][TB];
+  __shared__ double dis[TB];
+  __shared__ double ys[TB][kMaxF];
+  const BigSlot sl = slots[blockIdx.x];
+  const int ld = sl.ld;
+  const double *g = a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB;
+  double *rg = a.W + sl.base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
+  const bool bad =
+      diag_tile(g, ld, rg, ld, a.F, a.inv + sl.inv + int64_t(j) * TB * TB, sm, cv, dis, ys);
+  if (threadIdx.x == 0 && bad) atomicOr(&a.status[sl.k], 4);
+}
+
+// Step j of the factorisation, one launch over all slots with T > j + 1.
+// CTA l of a slot owns row tiles i0 = j + 1 + 2l and i0 + 1 of tile column j:
+//  1. C = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T: eight warps hold 32 x 32
+//     accumulators (starting at -A) for the whole K loop, the L panels stream
+//     through a cp.async pipeline;
+//  2. L[i, j] = C X_j^T, the triangular solve with the inverse factor of the
+//     diagonal tile (made one step earlier), stored; then the forward
+//     substitution r_i -= L[i, j] y_j from the accumulator registers;
+//  3. CTA 0 (i0 = j + 1) forms the next diagonal tile
+//     D = A[j+1, j+1] - sum_{p<=j} L[j+1, p] L[j+1, p]^T and factors it:
+//     X_{j+1} and y_{j+1} = X_{j+1} r_{j+1} for step j + 1.
+__global__ void __launch_bounds__(kColThreads, 2)
+    k_col_step(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
                int j) {
   extern __shared__ double sm[];
-  double *sI = sm;
-  double *sX[2] = {sm + TB * LDS, sm + 2 * TB * LDS};
-  double *sY = sm + 3 * TB * LDS;  // TB x kMaxF
-  const int q = find_slot(pre, cnt, blockIdx.x);
+  // The first cnt CTAs are the slots' CTA 0 (the longest: they also form the
+  // next diagonal tile), so they start in the first wave; the other CTAs
+  // (l >= 1) follow, addressed through the prefix counts.
+  int q, l;
+  if (int(blockIdx.x) < cnt) {
+    q = blockIdx.x;
+    l = 0;
+  } else {
+    const int b = blockIdx.x - cnt;
+    q = find_slot(pre, cnt, b);
+    l = 1 + b - pre[q];
+  }
   const BigSlot sl = slots[q];
-  const int i0 = j + 1 + kTrsmStrip * (blockIdx.x - pre[q]);
-  const int count = min(kTrsmStrip, sl.T - i0);
+  const int i0 = j + 1 + 2 * l;
+  const bool two = i0 + 1 < sl.T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int g = lane >> 2, t = lane & 3;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int ld = sl.ld, F = a.F;
-  double *base = a.W + sl.base;
-  const double *xinv = a.inv + sl.inv + int64_t(j) * TB * TB;
-  for (int idx = tid; idx < TB * TB / 2; idx += 128) {
-    const int r = idx >> 5, c2 = idx & 31;
-    cp_async16(sI + r * LDS + 2 * c2, xinv + r * TB + 2 * c2);
-  }
-  async_tile(sX[0], base + int64_t(i0) * TB * ld + int64_t(j) * TB, ld, tid, 128);
-  cp_async_commit();
-  const double *yg = base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
-  for (int e = tid; e < TB * kMaxF; e += 128) {
-    const int r = e / kMaxF, f = e % kMaxF;
-    sY[e] = f < F ? yg[int64_t(r) * ld + f] : 0.0;
-  }
-  for (int u = 0; u < count; ++u) {
-    const int i = i0 + u;
-    if (u + 1 < count) {
-      async_tile(sX[(u + 1) & 1], base + int64_t(i + 1) * TB * ld + int64_t(j) * TB, ld, tid, 128);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  double *W = a.W + sl.base;
+  double *rcol = W + int64_t(sl.T) * TB;
+  const double *gA = W + int64_t(i0) * TB * ld;
+  const double *gB = W + int64_t(j) * TB * ld;
+  const int arows = two ? kColRows : TB;
+  const int nch = j * (TB / kKC);
+  auto load = [&](int c, int stage) {
+    double *sA = sm + stage * kColStage;
+    double *sB = sA + kColRows * kKLD;
+    const int col = c * kKC;
+    for (int idx = tid; idx < (kColRows + TB) * (kKC / 2); idx += kColThreads) {
+      const int r = idx / (kKC / 2), c2 = idx % (kKC / 2);
+      if (r < kColRows) {
+        if (r < arows) cp_async16(sA + r * kKLD + 2 * c2, gA + int64_t(r) * ld + col + 2 * c2);
+      } else {
+        const int rb = r - kColRows;
+        cp_async16(sB + rb * kKLD + 2 * c2, gB + int64_t(rb) * ld + col + 2 * c2);
+      }
     }
-    __syncthreads();
-    double *sC = sX[u & 1];
-    double acc[4][4][2];
-    acc_zero(acc);
-    mma64<false, true>(sC, sI, acc, 1.0, wr, wc, lane);
-    acc_store(acc, base + int64_t(i) * TB * ld + int64_t(j) * TB, ld, wr, wc, lane);
-    __syncthreads();
-    // The L tile into shared memory for the residual update.
+  };
 #pragma unroll
-    for (int ii = 0; ii < 4; ++ii)
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nch) load(s, s);
+    cp_async_commit();
+  }
+  const bool active = two || wr < TB;
+  double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
+  double acc[4][4][2];
+  if (active) {
+    acc_load(acc, C, ld, wr, wc, lane);
+    acc_neg(acc);
+  }
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    if (c + kStages - 1 < nch) load(c + kStages - 1, (c + kStages - 1) % kStages);
+    cp_async_commit();
+    if (active) {
+      const double *sA = sm + (c % kStages) * kColStage;
+      mma_chunk_nt(sA, sA + kColRows * kKLD, acc, wr, wc, lane);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // 2. L[i, j] = C X_j^T through shared memory.
+  double *sC = sm;                   // kColRows x LDS
+  double *sX = sm + kColRows * LDS;  // TB x LDS
+  {
+    const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
+    for (int idx = tid; idx < TB * TB / 2; idx += kColThreads) {
+      const int r = idx >> 5, c2 = idx & 31;
+      cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
+    }
+    cp_async_commit();
+  }
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj)
-        *reinterpret_cast<double2 *>(sC + (wr + 8 * ii + g) * LDS + wc + 8 * jj + 2 * t) =
-            make_double2(acc[ii][jj][0], acc[ii][jj][1]);
-    __syncthreads();
-    // out (64 x 8) = L y_j: warp w owns rows 16w .. 16w + 15.
-    double o[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-#pragma unroll 4
-    for (int k0 = 0; k0 < TB; k0 += 4) {
-      const double bf = sY[(k0 + t) * kMaxF + g];
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-        dmma(o[mi][0], o[mi][1], sC[(16 * warp + 8 * mi + g) * LDS + k0 + t], bf);
-    }
-    double *rg = base + int64_t(i) * TB * ld + int64_t(sl.T) * TB;
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = 16 * warp + 8 * mi + g, f = 2 * t + h;
-        if (f < F) rg[int64_t(r) * ld + f] -= o[mi][h];
-      }
-    __syncthreads();
+        *reinterpret_cast<double2 *>(sC + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
+            make_double2(-acc[i][jj][0], -acc[i][jj][1]);
   }
+  cp_async_wait<0>();
+  __syncthreads();
+  acc_zero(acc);
+  if (active) {
+    mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
+    acc_store(acc, C, ld, wr, wc, lane);
+  }
+  __syncthreads();  // sC and sX are free
+  double *ysh = sm;               // TB x kMaxF
+  double *red = sm + TB * kMaxF;  // 2 x kColRows x kMaxF
+  {
+    const double *yg = rcol + int64_t(j) * TB * ld;
+    for (int e = tid; e < TB * kMaxF; e += kColThreads) {
+      const int r = e / kMaxF, f = e % kMaxF;
+      ysh[e] = f < F ? yg[int64_t(r) * ld + f] : 0.0;
+    }
+  }
+  __syncthreads();
+  for (int f = 0; f < F; ++f) {
+    double pr[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      double s = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          s = __fma_rn(acc[i][jj][h], ysh[(wc + 8 * jj + 2 * t + h) * kMaxF + f], s);
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      pr[i] = s;
+    }
+    if (t == 0 && active) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) red[((wc >> 5) * kColRows + wr + 8 * i + g) * kMaxF + f] = pr[i];
+    }
+  }
+  __syncthreads();
+  {
+    double *rg = rcol + int64_t(i0) * TB * ld;
+    for (int e = tid; e < arows * F; e += kColThreads) {
+      const int r = e / F, f = e % F;
+      rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(kColRows + r) * kMaxF + f];
+    }
+  }
+  if (l != 0) return;
+
+  // 3. The diagonal tile of step j + 1 (this CTA's first row tile).
+  __syncthreads();
+  constexpr int kDStage = TB * kKLD;
+  double *sL = sm + 2 * kDStage;  // L[j+1, j], TB x LDS
+  if (wr < TB) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        *reinterpret_cast<double2 *>(sL + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
+            make_double2(acc[i][jj][0], acc[i][jj][1]);
+  }
+  auto loadd = [&](int c, int stage) {
+    double *sD = sm + stage * kDStage;
+    const int col = c * kKC;
+    for (int idx = tid; idx < TB * (kKC / 2); idx += kColThreads) {
+      const int r = idx / (kKC / 2), c2 = idx % (kKC / 2);
+      cp_async16(sD + r * kKLD + 2 * c2, gA + int64_t(r) * ld + col + 2 * c2);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nch) loadd(s, s);
+    cp_async_commit();
+  }
+  const bool dact = wr < TB;
+  double *Dg = W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB;
+  if (dact) {
+    acc_load(acc, Dg, ld, wr, wc, lane);
+    acc_neg(acc);
+  }
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    if (c + kStages - 1 < nch) loadd(c + kStages - 1, (c + kStages - 1) % kStages);
+    cp_async_commit();
+    if (dact) {
+      const double *sD = sm + (c % kStages) * kDStage;
+      mma_chunk_nt(sD, sD, acc, wr, wc, lane);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (dact) mma64<false, true>(sL, sL, acc, 1.0, wr, wc, lane);
+  double *Ds = sm;  // TB x LDS, over the finished stages
+  if (dact) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        *reinterpret_cast<double2 *>(Ds + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
+            make_double2(-acc[i][jj][0], -acc[i][jj][1]);
+  }
+  __syncthreads();
+  // Scratch of the factorisation over the consumed L[j+1, j] (sL).
+  double *Xs = sm + TB * LDS;
+  double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
+  double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
+  double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
+  const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
+                             a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
+  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
 // Backward sweep L^T z = y of one slot (CTA per slot), tile row by tile row
@@ -437,26 +520,24 @@ __global__ void __launch_bounds__(256) k_chol_eval(BigArgs a, const BigSlot *__r
 // ---------------------------------------------------------------------------
 
 CholPlan chol_prefix(const std::vector<BigSlot> &slots) {
+  // Step j serves the slots with T > j + 1 (a prefix: slots are sorted by
+  // decreasing T), ceil((T - j - 1) / 2) CTAs each: CTA 0 of every slot first,
+  // then the prefix counts of the others.
   CholPlan cp;
   const int ns = int(slots.size());
-  const int steps = ns ? slots.front().T : 0;
+  const int steps = ns ? std::max(0, slots.front().T - 1) : 0;
+  cp.ns = ns;
   cp.cnt.resize(steps);
   cp.off.resize(steps + 1);
   for (int j = 0; j < steps; ++j) {
     int c = 0;
-    while (c < ns && slots[c].T > j) ++c;
+    while (c < ns && slots[c].T > j + 1) ++c;
     cp.cnt[j] = c;
     cp.off[j] = int(cp.pre.size());
     int64_t acc = 0;
     cp.pre.push_back(0);
     for (int q = 0; q < c; ++q) {
-      acc += j > 0 ? (slots[q].T - j + 1) / 2 : 0;
-      cp.pre.push_back(int(acc));
-    }
-    acc = 0;
-    cp.pre.push_back(0);
-    for (int q = 0; q < c; ++q) {
-      acc += (slots[q].T - j - 1 + kTrsmStrip - 1) / kTrsmStrip;
+      acc += (slots[q].T - j) / 2 - 1;  // CTAs l >= 1
       cp.pre.push_back(int(acc));
     }
     if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
@@ -468,57 +549,57 @@ CholPlan chol_prefix(const std::vector<BigSlot> &slots) {
 void chol_set_smem_attributes() {
   static bool done = false;
   if (done) return;
-  PB_CUDA(cudaFuncSetAttribute(k_col_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  PB_CUDA(cudaFuncSetAttribute(k_col_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kColSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
-  PB_CUDA(cudaFuncSetAttribute(k_col_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(kTrsmSmem)));
   done = true;
 }
 
 void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,
-                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep) {
+                       const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep,
+                       cudaEvent_t tail_event) {
+  if (cp.ns == 0) return;
+  k_diag_chol<<<cp.ns, 256, kDiagSmem, st>>>(a, ds, 0);
+  note_launch();
   const int steps = int(cp.cnt.size());
   std::vector<cudaEvent_t> ev;
   if (rep.time_kernels) {
     ev.resize(2 * size_t(steps));
     for (auto &e : ev) PB_CUDA(cudaEventCreate(&e));
   }
+  int sms = 0;
+  PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+  bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
-    const int *pu = dpre + cp.off[j];
-    const int *pt = pu + c + 1;
-    const int nu = cp.pre[cp.off[j] + c];
-    const int nt = cp.pre[cp.off[j] + c + 1 + c];
-    if (nu) {
-      if (rep.time_kernels) PB_CUDA(cudaEventRecord(ev[2 * j], st));
-      k_col_update<<<nu, kColThreads, kColSmem, st>>>(a, ds, pu, c, j);
-      note_launch();
-      if (rep.time_kernels) {
-        PB_CUDA(cudaEventRecord(ev[2 * j + 1], st));
-        for (int q = 0; q < c; ++q)
-          rep.update_flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j);
-        ++rep.update_launches;
-      }
+    const int n = c + cp.pre[cp.off[j] + c];
+    if (!tail && n < 2 * sms) {  // from here on the steps leave SMs idle
+      PB_CUDA(cudaEventRecord(tail_event, st));
+      tail = true;
     }
-    k_diag_chol<<<c, 256, kDiagSmem, st>>>(a, ds, j);
+    if (rep.time_kernels) PB_CUDA(cudaEventRecord(ev[2 * j], st));
+    k_col_step<<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
     note_launch();
-    if (nt) {
-      k_col_trsm<<<nt, 128, kTrsmSmem, st>>>(a, ds, pt, c, j);
-      note_launch();
+    if (rep.time_kernels) {
+      PB_CUDA(cudaEventRecord(ev[2 * j + 1], st));
+      // Tile products: (T - j - 1) row tiles x (j + 1) (update + solve), and
+      // j + 1 for the next diagonal tile.
+      for (int q = 0; q < c; ++q)
+        rep.update_flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j + 1);
+      ++rep.update_launches;
     }
   }
   if (rep.time_kernels) {
     PB_CUDA(cudaStreamSynchronize(st));
     for (int j = 0; j < steps; ++j) {
-      if (cp.pre[cp.off[j] + cp.cnt[j]] == 0) continue;
       float ms = 0.f;
       PB_CUDA(cudaEventElapsedTime(&ms, ev[2 * j], ev[2 * j + 1]));
       rep.ms_update += ms;
     }
     for (auto &e : ev) cudaEventDestroy(e);
   }
+  if (!tail) PB_CUDA(cudaEventRecord(tail_event, st));
 }
 
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,

@@ -63,21 +63,28 @@ struct DevGrid {
   DevMem start, items;
 };
 
-// Extra streams of a plan for independent groups of large patches, created
-// on first use on the plan's device; every use joins them back into the
-// plan's stream with events before the call returns.
+// Extra streams of a plan, created on first use on the plan's device: one per
+// independent group of large patches (high priority) and one for the small
+// patches (low priority: they fill the SMs the large-patch steps leave idle).
+// Every use joins them back into the plan's stream with events before the
+// call returns.
 struct AuxStreams {
-  static constexpr int kN = 4;
-  cudaStream_t s[kN] = {};
-  cudaEvent_t ev[kN + 1] = {};
+  static constexpr int kN = 4;      // slot groups of the large-patch engine
+  static constexpr int kSmall = kN; // index of the small-patch stream
+  cudaStream_t s[kN + 1] = {};
+  cudaEvent_t ev[kN + 3] = {};      // per group, fork, small fork, small join
   bool made = false;
   void make() {
     if (made) return;
-    for (int i = 0; i < kN; ++i) {
-      if (cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking) != cudaSuccess)
-        throw Error{PACMAN_B200_ERR_CUDA, "cudaStreamCreateWithFlags failed"};
-    }
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess)
+      throw Error{PACMAN_B200_ERR_CUDA, "cudaDeviceGetStreamPriorityRange failed"};
     for (int i = 0; i <= kN; ++i) {
+      if (cudaStreamCreateWithPriority(&s[i], cudaStreamNonBlocking,
+                                       i == kSmall ? least : greatest) != cudaSuccess)
+        throw Error{PACMAN_B200_ERR_CUDA, "cudaStreamCreateWithPriority failed"};
+    }
+    for (int i = 0; i < kN + 3; ++i) {
       if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
         throw Error{PACMAN_B200_ERR_CUDA, "cudaEventCreateWithFlags failed"};
     }
@@ -87,9 +94,9 @@ struct AuxStreams {
   AuxStreams(const AuxStreams &) = delete;
   AuxStreams &operator=(const AuxStreams &) = delete;
   ~AuxStreams() {
-    for (int i = 0; i < kN; ++i)
-      if (s[i]) cudaStreamDestroy(s[i]);
     for (int i = 0; i <= kN; ++i)
+      if (s[i]) cudaStreamDestroy(s[i]);
+    for (int i = 0; i < kN + 3; ++i)
       if (ev[i]) cudaEventDestroy(ev[i]);
   }
 };
@@ -168,6 +175,9 @@ struct SolveReport {
   double ms_factor = 0.0;     // device time of the factorisation launches
   double factor_flops = 0.0;  // their algorithmic FLOPs
   bool time_kernels = false;  // input: event-time the column-update launches
+  // input: re-recorded by the large-patch engine where its steps stop filling
+  // the GPU (the small patches start there), or null
+  cudaEvent_t tail_event = nullptr;
   double ms_update = 0.0, update_flops = 0.0;
   int64_t update_launches = 0;
 };

@@ -357,9 +357,8 @@ static void launch(int mode, const PatchArgs &a, const int *plist, int np, int u
 // shared memory follows the bucket's largest patch; patches too large for
 // shared memory use the global workspace.
 static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &patches,
-                     SolveReport &rep) {
+                     SolveReport &rep, cudaStream_t st) {
   if (patches.empty()) return;
-  cudaStream_t st = p.stream;
   for (int k : patches) {
     const double n = p.n_host[k], m = p.m_host[k];
     rep.factor_flops += (mode == kLU ? 2.0 / 3.0 : 1.0 / 3.0) * n * n * n +
@@ -486,8 +485,19 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   PB_CUDA(cudaEventCreate(&ev0));
   PB_CUDA(cudaEventCreate(&ev1));
   PB_CUDA(cudaEventRecord(ev0, st));
-  run_list(p, a, mode, small, rep);
+  // Small patches on the low-priority stream, started where the large-patch
+  // steps stop filling the GPU (the engine re-records the event there; with
+  // no large patches it stays at this point of the plan's stream).
+  p.aux.make();
+  cudaStream_t ss = p.aux.s[AuxStreams::kSmall];
+  rep.tail_event = p.aux.ev[AuxStreams::kN + 1];
+  PB_CUDA(cudaEventRecord(rep.tail_event, st));
   solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep, ex);
+  PB_CUDA(cudaStreamWaitEvent(ss, rep.tail_event, 0));
+  run_list(p, a, mode, small, rep, ss);
+  PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN + 2], ss));
+  PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[AuxStreams::kN + 2], 0));
+  rep.tail_event = nullptr;
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
   PB_CUDA(cudaEventRecord(ev1, st));
@@ -505,7 +515,7 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   rep.patches_fp64 = int64_t(small.size() + big.size());
   if (!redo_small.empty() || !redo_big.empty()) {
     PB_CUDA(cudaEventRecord(ev0, st));
-    run_list(p, a, kLU, redo_small, rep);
+    run_list(p, a, kLU, redo_small, rep, st);
     solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep, ex);
     PB_CUDA(cudaEventRecord(ev1, st));
     PB_CUDA(cudaStreamSynchronize(st));
@@ -545,7 +555,7 @@ void solve_adjoint(Plan &p, int basis, int F, const double *h, double *g_out, So
     if (p.m_host[k] == 0) continue;  // h = 0 there: g = 0 (the caller zeroes g)
     (p.n_host[k] > nbig ? big : small).push_back(k);
   }
-  run_list(p, a, kAdj, small, rep);
+  run_list(p, a, kAdj, small, rep, p.stream);
   BigExtra ex;
   ex.mode = kBigAdjoint;
   ex.h = h;
