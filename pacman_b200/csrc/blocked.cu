@@ -728,18 +728,32 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       a.alpha_c = dalpha.as<double>();
     }
   }
+  // The forward Cholesky of precision "mixed" runs its column updates on the
+  // int8 tensor cores (k_col_step_oz); PACMAN_B200_INT8=0 keeps them in FP64.
+  const char *i8env = std::getenv("PACMAN_B200_INT8");
+  const bool oz = !lu && !adjoint && !(i8env && std::atoi(i8env) == 0);
+  if (oz) {
+    // sigma bounds every |L[r][c]| <= sqrt(A_rr) = sqrt(phi(0)) (1 for the
+    // identity padding), with margin for rounding and for d_1 <= 127.
+    const double phi0 = basis == 0x12 ? 3.0 : (basis == 0x14 ? 15.0 : 1.0);
+    const double sigma = std::sqrt(std::max(phi0, 1.0)) * (128.0 / 127.0) * (1.0 + std::ldexp(1.0, -20));
+    a.oz_mul = 128.0 / sigma;
+    a.oz_sig2 = sigma * sigma;
+  }
   HostArena &arena = HostArena::get();
   size_t pos = 0;
   while (pos < order.size()) {
     // One wave: as many patches as fit the workspace budget.
     std::vector<BigSlot> slots;
     size_t tot = 0;
-    int64_t tot_inv = 0, tot_z = 0;
+    int64_t tot_inv = 0, tot_z = 0, tot_sl = 0;
     while (pos < order.size()) {
       const int k = order[pos];
       const int n = p.n_host[k], m = p.m_host[k];
+      const int Tn = (n + TB - 1) / TB;
       const size_t d = slot_doubles(n, lu ? m : 0);
-      if (!slots.empty() && tot + d > budget) break;
+      const size_t dsl_doubles = oz ? (oz_slot_bytes(Tn) + 7) / 8 : 0;
+      if (!slots.empty() && tot + size_t(tot_sl) / 8 + d + dsl_doubles > budget) break;
       BigSlot q{};
       q.base = int64_t(tot);
       q.T = (n + TB - 1) / TB;
@@ -748,6 +762,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       q.q = int(slots.size());
       q.zoff = tot_z;
       tot_z += int64_t(q.T) * TB * F;
+      q.sli = tot_sl;
+      if (oz) tot_sl += int64_t(oz_slot_bytes(q.T));
       tot_inv += int64_t(q.T) * TB * TB;
       q.ld = (q.T + 1) * TB;
       q.k = k;
@@ -795,10 +811,15 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     }
     DevMem dW, dsmall;
     dW.alloc(sizeof(double) * tot, st);
-    DevMem dzc;
+    DevMem dzc, dsl;
     if (!lu) {
       dzc.alloc(sizeof(double) * size_t(tot_z), st);
       a.zc = dzc.as<double>();
+    }
+    a.slices = nullptr;
+    if (oz && tot_sl > 0) {
+      dsl.alloc(size_t(tot_sl), st);
+      a.slices = dsl.as<uint8_t>();
     }
     const size_t n_inv = lu ? size_t(2) * TB * TB * ns : size_t(tot_inv);
     const size_t n_beta = size_t(4) * kMaxF * ns;
@@ -824,14 +845,6 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     arena.upload(slots.data(), slots.size(), ds, st);
     arena.upload(pre_asm.data(), pre_asm.size(), dpre_asm, st);
     arena.upload(pre.data(), pre.size(), dpre, st);
-    k_assemble<<<pre_asm[ns], 256, 0, st>>>(a, ds, dpre_asm, ns, lu ? 1 : 0);
-    note_launch();
-    k_big_poly<<<ns, 256, 0, st>>>(a, ds);
-    note_launch();
-    if (adjoint) {
-      k_big_adj_rhs<<<ns, 256, 0, st>>>(a, ds);
-      note_launch();
-    }
     if (!lu) {
       // Interleaved groups of slots, each stepping in lockstep on its own
       // stream: the short diagonal and trsm launches and the tails of one
@@ -846,21 +859,39 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       std::vector<CholPlan> gp(G);
       std::vector<DevMem> gmem(G);
       std::vector<BigSlot *> gds(G);
-      std::vector<int *> gpre(G);
+      std::vector<int *> gpre(G), gasm(G);
+      std::vector<std::vector<int>> gpre_asm(G);
       for (int g = 0; g < G; ++g) {
         gp[g] = chol_prefix(gs[g]);
-        gmem[g].alloc(sizeof(BigSlot) * gs[g].size() + sizeof(int) * gp[g].pre.size() + 64, st);
+        const int ng = int(gs[g].size());
+        gpre_asm[g].assign(ng + 1, 0);
+        for (int q = 0; q < ng; ++q)
+          gpre_asm[g][q + 1] = gpre_asm[g][q] + int(count_assemble(false, gs[g][q]));
+        const size_t b0 = (sizeof(BigSlot) * ng + 15) & ~size_t(15);
+        const size_t b1 = (sizeof(int) * gp[g].pre.size() + 15) & ~size_t(15);
+        gmem[g].alloc(b0 + b1 + sizeof(int) * (ng + 1) + 64, st);
         gds[g] = gmem[g].as<BigSlot>();
-        gpre[g] = reinterpret_cast<int *>(gmem[g].as<char>() +
-                                          ((sizeof(BigSlot) * gs[g].size() + 15) & ~size_t(15)));
+        gpre[g] = reinterpret_cast<int *>(gmem[g].as<char>() + b0);
+        gasm[g] = reinterpret_cast<int *>(gmem[g].as<char>() + b0 + b1);
         arena.upload(gs[g].data(), gs[g].size(), gds[g], st);
         arena.upload(gp[g].pre.data(), gp[g].pre.size(), gpre[g], st);
+        arena.upload(gpre_asm[g].data(), gpre_asm[g].size(), gasm[g], st);
       }
       p.aux.make();
       PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN], st));
       for (int g = 0; g < G; ++g) {
         cudaStream_t sg = p.aux.s[g];
         PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
+        // Each group assembles its own slots, so group 0 starts its steps
+        // while the others still assemble.
+        const int ng = int(gs[g].size());
+        k_assemble<<<gpre_asm[g][ng], 256, 0, sg>>>(a, gds[g], gasm[g], ng, 0);
+        k_big_poly<<<ng, 256, 0, sg>>>(a, gds[g]);
+        note_launch(2);
+        if (adjoint) {
+          k_big_adj_rhs<<<ng, 256, 0, sg>>>(a, gds[g]);
+          note_launch();
+        }
         chol_launch_steps(a, gds[g], gs[g], gp[g], gpre[g], sg, rep,
                           g == 0 ? rep.tail_event : nullptr);
         chol_launch_finish(a, gds[g], int(gs[g].size()), adjoint, sg);
@@ -874,6 +905,10 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       PB_CUDA(cudaGetLastError());
       continue;
     }
+    k_assemble<<<pre_asm[ns], 256, 0, st>>>(a, ds, dpre_asm, ns, 1);
+    note_launch();
+    k_big_poly<<<ns, 256, 0, st>>>(a, ds);
+    note_launch();
     const size_t s3 = 3 * TB * LDS * sizeof(double), s2 = 2 * TB * LDS * sizeof(double);
     for (int s = 0; s < steps; ++s) {
       const int c = cnt[s];

@@ -25,6 +25,7 @@ struct BigSlot {
   int64_t inv;   // offset (doubles) of the slot's inverse tiles
   int q;         // index of the slot in its wave (per-slot arrays beta, act, red)
   int64_t zoff;  // offset (doubles) of the slot's backward-sweep solution in zc
+  int64_t sli;   // offset (bytes) of the slot's int8 slice tiles in slices
 };
 
 // Work of one launch is addressed by blockIdx.x through prefix counts over
@@ -163,6 +164,9 @@ struct BigArgs {
   double *red_out;     // adjoint: per slot reduced moments (kRedVals)
   double *alpha_c;     // Cholesky forward: RBF coefficients per (patch, source)
   double *zc;          // Cholesky: backward-sweep solution per slot (T*TB x F)
+  uint8_t *slices;     // mixed forward: int8 slices of the L tiles, or null (FP64 updates)
+  double oz_mul;       // 128 / sigma (sigma bounds |L|)
+  double oz_sig2;      // sigma^2
 };
 
 // Left-looking Cholesky steps, backward sweep and local evaluation of one
@@ -176,6 +180,8 @@ struct CholPlan {
 };
 CholPlan chol_prefix(const std::vector<BigSlot> &slots);
 void chol_set_smem_attributes();
+// Bytes of int8 slice tiles of a slot with T tile rows (strictly lower tiles).
+size_t oz_slot_bytes(int T);
 // tail_event (or null) is recorded on st at the first step that leaves SMs
 // idle (fewer than two CTAs per SM), else after the last step.
 void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,

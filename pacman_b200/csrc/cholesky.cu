@@ -18,6 +18,7 @@
 // the FP64 tensor cores (mma.sync m8n8k4 f64).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "blocked.cuh"
@@ -190,6 +191,304 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
   if (threadIdx.x == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
+// Phase 2 of a factorisation step.  sm holds C (the updated row tiles i0, and
+// i0 + 1 when arows = 2 TB; kColRows x LDS doubles).  L[i, j] = C X_j^T on the
+// FP64 tensor cores, stored over C in the workspace and left in acc; then the
+// forward substitution r_i -= L[i, j] y_j.  Uses sm[0, (kColRows + TB) LDS)
+// and ends with a barrier after which sm is free.  256 threads.
+__device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, int arows, bool active,
+                          double *sm, double (&acc)[4][4][2]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int ld = sl.ld, F = a.F;
+  double *W = a.W + sl.base;
+  double *rcol = W + int64_t(sl.T) * TB;
+  double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
+  double *sC = sm;                   // kColRows x LDS
+  double *sX = sm + kColRows * LDS;  // TB x LDS
+  {
+    const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
+    for (int idx = tid; idx < TB * TB / 2; idx += kColThreads) {
+      const int r = idx >> 5, c2 = idx & 31;
+      cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
+    }
+    cp_async_commit();
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  acc_zero(acc);
+  if (active) {
+    mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
+    acc_store(acc, C, ld, wr, wc, lane);
+  }
+  __syncthreads();  // sC and sX are free
+  double *ysh = sm;               // TB x kMaxF
+  double *red = sm + TB * kMaxF;  // 2 x kColRows x kMaxF
+  {
+    const double *yg = rcol + int64_t(j) * TB * ld;
+    for (int e = tid; e < TB * kMaxF; e += kColThreads) {
+      const int r = e / kMaxF, f = e % kMaxF;
+      ysh[e] = f < F ? yg[int64_t(r) * ld + f] : 0.0;
+    }
+  }
+  __syncthreads();
+  for (int f = 0; f < F; ++f) {
+    double pr[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      double s = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          s = __fma_rn(acc[i][jj][h], ysh[(wc + 8 * jj + 2 * t + h) * kMaxF + f], s);
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      pr[i] = s;
+    }
+    if (t == 0 && active) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) red[((wc >> 5) * kColRows + wr + 8 * i + g) * kMaxF + f] = pr[i];
+    }
+  }
+  __syncthreads();
+  {
+    double *rg = rcol + int64_t(i0) * TB * ld;
+    for (int e = tid; e < arows * F; e += kColThreads) {
+      const int r = e / F, f = e % F;
+      rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(kColRows + r) * kMaxF + f];
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Column updates on the int8 tensor cores (precision "mixed")
+// ---------------------------------------------------------------------------
+//
+// Every finished off-diagonal tile L[i, p] is also kept as kOzS int8 digit
+// slices of x = L / sigma (sigma >= sqrt(max_r A_rr) bounds every entry of L,
+// since the rows of L have norm sqrt(A_rr)): x = sum_s d_s 128^-s, d_1 in
+// [-127, 127], d_s in [-64, 64] after.  The update
+//   sum_p L[i, p] L[j, p]^T = sigma^2 sum_{a,b} 128^-(a+b) D_a[i] D_b[j]^T
+// keeps the slice pairs with a + b <= kOzS + 1 (27 levels of products dropped
+// below 128^-8 ~ 2^-56) and sums each level a + b exactly in int32 on the
+// tcgen05 tensor cores (kind::i8); the levels are combined in FP64 at the end.
+// This is the split-integer emulation of an FP64 product (Ozaki, Ogita, Oishi
+// and Rump 2012; Uchino, Ozaki and Imamura 2024 for integer tensor cores).
+//
+// Slice tile layout (28 KB): [16-byte K chunk (4)][slice (kOzS)][8-row group
+// (8)][8 rows x 16 bytes], i.e. the K-major core-matrix layout of the tensor
+// core, copied to shared memory with bulk async copies.
+constexpr int kOzS = 7;
+constexpr int kOzTileBytes = 4 * kOzS * 8 * 128;      // 28672
+constexpr int kOzStages = 4;                          // pipeline depth, K = 32 per stage
+constexpr int kOzStageA = 2 * kOzS * 16 * 128;        // two row tiles: 28672
+constexpr int kOzStageB = 2 * kOzS * 8 * 128;         // one row tile: 14336
+constexpr int kOzStage = kOzStageA + kOzStageB;       // 43008
+constexpr int kOzSLOff = kOzStages * kOzStage;        // L[j+1, j] (TB x LDS doubles)
+constexpr int kOzBarOff = kOzSLOff + TB * LDS * 8;    // barriers, TMEM address
+constexpr size_t kOzSmem = size_t(kOzBarOff) + 256;  // 2 x OzBars + TMEM address
+constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
+constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
+constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
+
+static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
+static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzSLOff, "staging overlaps L[j+1, j]");
+
+__device__ __forceinline__ uint32_t saddr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(b)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait for the phase with the given parity; false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+  uint32_t done = 0;
+  for (int it = 0; it < kOzWaitLimit && !done; ++it)
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          saddr(dst)),
+      "l"(src), "r"(bytes), "r"(saddr(b))
+      : "memory");
+}
+// Shared-memory matrix descriptor, K-major core matrices without swizzle
+// (layout type 0, descriptor version 1): lbo = byte step between 16-byte K
+// chunks, sbo = byte step between 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((addr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+// Instruction descriptor: D s32, A and B signed int8, both K-major, M = 128.
+__device__ __forceinline__ uint32_t umma_idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+__device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *b) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   saddr(b))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+
+struct OzBars {
+  uint64_t full[kOzStages], empty[kOzStages], done;
+};
+
+// K loop over the p < nump column tiles of one step on the int8 tensor cores:
+// TMEM columns 64 (l - 2) .. + 63 receive level l = 2..kOzS+1 of
+// [rows of tile rA0 (and rA1)] x [rows of tile rB]^T.  rA0, rA1, rB point to
+// the first slice tile of their tile row (tiles of a row are consecutive in
+// p).  Thread 0 issues the bulk copies, thread 32 the MMAs; every thread
+// returns after the MMAs completed.  false if a wait timed out.
+__device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint8_t *rA0,
+                         const uint8_t *rA1, const uint8_t *rB, int nump) {
+  const int tid = threadIdx.x;
+  // Earlier generic writes to the stage area before the async-proxy copies.
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (tid == 0) {
+    for (int i = 0; i < kOzStages; ++i) {
+      mbar_init(&bar->full[i], 1);
+      mbar_init(&bar->empty[i], 1);
+    }
+    mbar_init(&bar->done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  bool ok = true;
+  const int nh = 2 * nump;  // K = 32 halves of the column tiles
+  if (tid == 0) {
+    const uint32_t bytes = uint32_t((rA1 ? 2 : 1) * kOzTileBytes / 2 + kOzTileBytes / 2);
+    for (int hh = 0; hh < nh && ok; ++hh) {
+      const int st = hh % kOzStages, u = hh / kOzStages;
+      if (hh >= kOzStages) ok = mbar_wait(&bar->empty[st], uint32_t((u - 1) & 1));
+      if (!ok) break;
+      uint8_t *sA = stages + st * kOzStage;
+      uint8_t *sB = sA + kOzStageA;
+      mbar_expect_tx(&bar->full[st], bytes);
+      const int64_t toff = int64_t(hh >> 1) * kOzTileBytes + (hh & 1) * 2 * kOzS * 1024;
+      const uint8_t *a0 = rA0 + toff;
+      const uint8_t *a1 = rA1 ? rA1 + toff : nullptr;
+      for (int cs = 0; cs < 2 * kOzS; ++cs) {  // (K chunk, slice) pieces of 8 row groups
+        bulk_g2s(sA + cs * 16 * 128, a0 + cs * 1024, 1024, &bar->full[st]);
+        if (a1) bulk_g2s(sA + (cs * 16 + 8) * 128, a1 + cs * 1024, 1024, &bar->full[st]);
+      }
+      bulk_g2s(sB, rB + toff, 2 * kOzS * 1024, &bar->full[st]);
+    }
+  } else if (tid == 32) {
+    for (int hh = 0; hh < nh && ok; ++hh) {
+      const int st = hh % kOzStages, u = hh / kOzStages;
+      ok = mbar_wait(&bar->full[st], uint32_t(u & 1));
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t sA = saddr(stages + st * kOzStage);
+      const uint32_t sB = sA + kOzStageA;
+#pragma unroll
+      for (int a = 1; a <= kOzS; ++a) {
+        const uint64_t ad = umma_desc(sA + ((a - 1) * 16) * 128, kOzS * 16 * 128, 128);
+        const int nb = kOzS + 1 - a;  // slices b = 1 .. nb -> levels a + 1 .. kOzS + 1
+        const uint32_t accf = (hh > 0 || a > 1) ? 1u : 0u;
+        const int n1 = nb < 4 ? nb : 4;
+        umma_i8(tmem + 64 * (a - 1), ad, umma_desc(sB, kOzS * 8 * 128, 128),
+                umma_idesc_i8(64 * n1), accf);
+        if (nb > 4)
+          umma_i8(tmem + 64 * (a - 1) + 256, ad, umma_desc(sB + 4 * 8 * 128, kOzS * 8 * 128, 128),
+                  umma_idesc_i8(64 * (nb - 4)), accf);
+      }
+      umma_commit(&bar->empty[st]);
+    }
+    umma_commit(&bar->done);
+  }
+  __syncthreads();
+  if (!mbar_wait(&bar->done, 0u)) ok = false;
+  tc_fence_after();
+  return ok;
+}
+
+// Row r = 32 (warp % 4) + lane of the K loop's result, columns 32 h .. + 31
+// (h = warp / 4): v[c] = sum_l 128^-l Z_l[r][32 h + c].
+__device__ __forceinline__ void oz_levels(uint32_t tmem, double (&v)[32]) {
+  const int warp = threadIdx.x >> 5;
+  const uint32_t lane_base = uint32_t(32 * (warp & 3)) << 16;
+  const int h = warp >> 2;
+#pragma unroll
+  for (int c = 0; c < 32; ++c) v[c] = 0.0;
+#pragma unroll 1
+  for (int lev = 2; lev <= kOzS + 1; ++lev) {
+    uint32_t z[32];
+    const uint32_t addr = tmem + lane_base + uint32_t(64 * (lev - 2) + 32 * h);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(z[0]), "=r"(z[1]), "=r"(z[2]), "=r"(z[3]), "=r"(z[4]), "=r"(z[5]), "=r"(z[6]),
+          "=r"(z[7]), "=r"(z[8]), "=r"(z[9]), "=r"(z[10]), "=r"(z[11]), "=r"(z[12]), "=r"(z[13]),
+          "=r"(z[14]), "=r"(z[15])
+        : "r"(addr));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(z[16]), "=r"(z[17]), "=r"(z[18]), "=r"(z[19]), "=r"(z[20]), "=r"(z[21]),
+          "=r"(z[22]), "=r"(z[23]), "=r"(z[24]), "=r"(z[25]), "=r"(z[26]), "=r"(z[27]),
+          "=r"(z[28]), "=r"(z[29]), "=r"(z[30]), "=r"(z[31])
+        : "r"(addr + 16));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    const double sc = ldexp(1.0, -7 * lev);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = __fma_rn(double(int32_t(z[c])), sc, v[c]);
+  }
+}
+
+// The int8 digits of the FP64 tile values held in acc (rows wr.., columns
+// wc.. of a 128 x 64 pair) into the staging area stg (two slice tiles).
+__device__ __forceinline__ void oz_slice_acc(const double (&acc)[4][4][2], double mul, uint8_t *stg,
+                                             int wr, int wc, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wr + 8 * i + g, c = wc + 8 * jj + 2 * t + h;
+        const int r64 = r & 63;
+        uint8_t *dst = stg + (r >> 6) * kOzTileBytes + (c >> 4) * kOzS * 1024 +
+                       (r64 >> 3) * 128 + (r64 & 7) * 16 + (c & 15);
+        double x = acc[i][jj][h] * mul;
+#pragma unroll
+        for (int sl = 0; sl < kOzS; ++sl) {
+          double d = rint(x);
+          d = fmin(fmax(d, -127.0), 127.0);
+          dst[sl * 1024] = uint8_t(int8_t(int(d)));
+          x = (x - d) * 128.0;
+        }
+      }
+}
+
 // Step j of the factorisation, one launch over all slots with T > j + 1.
 // CTA l of a slot owns row tiles i0 = j + 1 + 2l and i0 + 1 of tile column j:
 //  1. C = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T: eight warps hold 32 x 32
@@ -201,6 +500,7 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
 //  3. CTA 0 (i0 = j + 1) forms the next diagonal tile
 //     D = A[j+1, j+1] - sum_{p<=j} L[j+1, p] L[j+1, p]^T and factors it:
 //     X_{j+1} and y_{j+1} = X_{j+1} r_{j+1} for step j + 1.
+template <bool SLICE>
 __global__ void __launch_bounds__(kColThreads, 2)
     k_col_step(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
                int j) {
@@ -269,68 +569,27 @@ __global__ void __launch_bounds__(kColThreads, 2)
   cp_async_wait<0>();
   __syncthreads();
 
-  // 2. L[i, j] = C X_j^T through shared memory.
-  double *sC = sm;                   // kColRows x LDS
-  double *sX = sm + kColRows * LDS;  // TB x LDS
-  {
-    const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
-    for (int idx = tid; idx < TB * TB / 2; idx += kColThreads) {
-      const int r = idx >> 5, c2 = idx & 31;
-      cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
-    }
-    cp_async_commit();
-  }
+  // 2. L[i, j] = C X_j^T through shared memory, then the forward substitution.
   if (active) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj)
-        *reinterpret_cast<double2 *>(sC + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
+        *reinterpret_cast<double2 *>(sm + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
             make_double2(-acc[i][jj][0], -acc[i][jj][1]);
   }
-  cp_async_wait<0>();
-  __syncthreads();
-  acc_zero(acc);
-  if (active) {
-    mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
-    acc_store(acc, C, ld, wr, wc, lane);
-  }
-  __syncthreads();  // sC and sX are free
-  double *ysh = sm;               // TB x kMaxF
-  double *red = sm + TB * kMaxF;  // 2 x kColRows x kMaxF
-  {
-    const double *yg = rcol + int64_t(j) * TB * ld;
-    for (int e = tid; e < TB * kMaxF; e += kColThreads) {
-      const int r = e / kMaxF, f = e % kMaxF;
-      ysh[e] = f < F ? yg[int64_t(r) * ld + f] : 0.0;
-    }
-  }
-  __syncthreads();
-  for (int f = 0; f < F; ++f) {
-    double pr[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      double s = 0.0;
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          s = __fma_rn(acc[i][jj][h], ysh[(wc + 8 * jj + 2 * t + h) * kMaxF + f], s);
-      s += __shfl_xor_sync(0xffffffffu, s, 1);
-      s += __shfl_xor_sync(0xffffffffu, s, 2);
-      pr[i] = s;
-    }
-    if (t == 0 && active) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) red[((wc >> 5) * kColRows + wr + 8 * i + g) * kMaxF + f] = pr[i];
-    }
-  }
-  __syncthreads();
-  {
-    double *rg = rcol + int64_t(i0) * TB * ld;
-    for (int e = tid; e < arows * F; e += kColThreads) {
-      const int r = e / F, f = e % F;
-      rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(kColRows + r) * kMaxF + f];
+  step_trsm(a, sl, j, i0, arows, active, sm, acc);
+  if (SLICE) {  // int8 slices of the new L tiles for the int8 steps that follow
+    uint8_t *stg = reinterpret_cast<uint8_t *>(sm) + kOzStgOff;
+    if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
+    __syncthreads();
+    const uint8_t *srow = a.slices + sl.sli;
+    for (int tt = 0; tt < arows / TB; ++tt) {
+      const int i = i0 + tt;
+      int4 *dst = reinterpret_cast<int4 *>(const_cast<uint8_t *>(srow) +
+                                           (int64_t(i) * (i - 1) / 2 + j) * kOzTileBytes);
+      const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
+      for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
     }
   }
   if (l != 0) return;
@@ -397,6 +656,137 @@ __global__ void __launch_bounds__(kColThreads, 2)
   const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
                              a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+}
+
+// Step j of the factorisation with the column update on the int8 tensor cores
+// (same work split as k_col_step; one CTA per SM: the K loop holds 448 TMEM
+// columns).  Phase 2 also writes the int8 slices of the new L tiles.
+__global__ void __launch_bounds__(kColThreads, 1)
+    k_col_step_oz(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
+                  int j) {
+  extern __shared__ __align__(1024) uint8_t smb[];
+  double *sm = reinterpret_cast<double *>(smb);
+  OzBars *bars = reinterpret_cast<OzBars *>(smb + kOzBarOff);           // phase 1
+  OzBars *bars3 = bars + 1;                                               // phase 3
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smb + kOzBarOff + 2 * sizeof(OzBars));
+  int q, l;
+  if (int(blockIdx.x) < cnt) {
+    q = blockIdx.x;
+    l = 0;
+  } else {
+    const int b = blockIdx.x - cnt;
+    q = find_slot(pre, cnt, b);
+    l = 1 + b - pre[q];
+  }
+  const BigSlot sl = slots[q];
+  const int i0 = j + 1 + 2 * l;
+  const bool two = i0 + 1 < sl.T;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int ld = sl.ld, F = a.F;
+  double *W = a.W + sl.base;
+  double *rcol = W + int64_t(sl.T) * TB;
+  const int arows = two ? kColRows : TB;
+  const bool active = two || wr < TB;
+  auto slice_row = [&](int i) {
+    return a.slices + sl.sli + (int64_t(i) * (i - 1) / 2) * kOzTileBytes;
+  };
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     saddr(tmem_slot)),
+                 "r"(kOzTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  bool ok = true;
+
+  // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l, into sm (kColRows x LDS).
+  if (j > 0)
+    ok = oz_kloop(smb, bars, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr, slice_row(j), j);
+  {
+    const int r = 32 * (warp & 3) + lane, h = warp >> 2;
+    double v[32];
+    if (j > 0) oz_levels(tmem, v);
+    if (j > 0) tc_fence_before();
+    __syncthreads();  // the stages are free (every MMA finished before oz_kloop returned)
+    if (r < arows) {
+      const double *Ar = W + int64_t(i0 * TB + r) * ld + int64_t(j) * TB + 32 * h;
+      double *Cr = sm + r * LDS + 32 * h;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) Cr[c] = j > 0 ? __fma_rn(-a.oz_sig2, v[c], Ar[c]) : Ar[c];
+    }
+  }
+  // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
+  double acc[4][4][2];
+  step_trsm(a, sl, j, i0, arows, active, sm, acc);
+  uint8_t *stg = smb + kOzStgOff;
+  if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
+  __syncthreads();
+  for (int tt = 0; tt < arows / TB; ++tt) {
+    int4 *dst = reinterpret_cast<int4 *>(slice_row(i0 + tt) + int64_t(j) * kOzTileBytes);
+    const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
+    for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
+  }
+
+  if (l == 0) {
+    // 3. The diagonal tile of step j + 1: D = A[j+1, j+1] - sigma^2 sum_l
+    //    128^-l Z_l (p < j, int8) - L[j+1, j] L[j+1, j]^T (FP64), factored.
+    double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
+    if (wr < TB) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+          *reinterpret_cast<double2 *>(sL + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
+              make_double2(acc[i][jj][0], acc[i][jj][1]);
+    }
+    __syncthreads();  // the staging area is copied out; sL is complete
+    if (j > 0 && ok) {
+      const uint8_t *rd = slice_row(j + 1);
+      ok = oz_kloop(smb, bars3, tmem, rd, nullptr, rd, j);
+    }
+    double *Ds = sm;
+    {
+      const int r = 32 * (warp & 3) + lane, h = warp >> 2;
+      double v[32];
+      if (j > 0) oz_levels(tmem, v);
+      if (j > 0) tc_fence_before();
+      __syncthreads();
+      if (r < TB) {
+        const double *Ar = W + int64_t((j + 1) * TB + r) * ld + int64_t(j + 1) * TB + 32 * h;
+        double *Dr = Ds + r * LDS + 32 * h;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Dr[c] = j > 0 ? __fma_rn(-a.oz_sig2, v[c], Ar[c]) : Ar[c];
+      }
+    }
+    __syncthreads();
+    if (wr < TB) {
+      acc_load(acc, Ds, LDS, wr, wc, lane);
+      mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
+    }
+    __syncthreads();
+    if (wr < TB) acc_store(acc, Ds, LDS, wr, wc, lane);
+    __syncthreads();
+    double *Xs = sm + TB * LDS;
+    double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
+    double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
+    double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
+    const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
+                               a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
+    if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+  }
+  if (tid == 0 && !ok) atomicOr(&a.status[sl.k], 8);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(kOzTmemCols)
+                 : "memory");
 }
 
 // Backward sweep L^T z = y of one slot (CTA per slot), tile row by tile row
@@ -549,8 +939,12 @@ CholPlan chol_prefix(const std::vector<BigSlot> &slots) {
 void chol_set_smem_attributes() {
   static bool done = false;
   if (done) return;
-  PB_CUDA(cudaFuncSetAttribute(k_col_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  PB_CUDA(cudaFuncSetAttribute(k_col_step<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kColSmem)));
+  PB_CUDA(cudaFuncSetAttribute(k_col_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kColSmem)));
+  PB_CUDA(cudaFuncSetAttribute(k_col_step_oz, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kOzSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
   done = true;
@@ -570,6 +964,9 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   }
   int sms = 0;
   PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+  // First step on the int8 tensor cores (PACMAN_B200_INT8_FROM overrides).
+  const char *ofe = std::getenv("PACMAN_B200_INT8_FROM");
+  const int oz_from = ofe ? std::max(1, std::atoi(ofe)) : 10;
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
@@ -579,7 +976,14 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       tail = true;
     }
     if (rep.time_kernels) PB_CUDA(cudaEventRecord(ev[2 * j], st));
-    k_col_step<<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
+    // With int8 slices: the FP64 kernel (two CTAs per SM) for the short K
+    // loops of the first steps, writing the slices; the int8 kernel after.
+    if (a.slices == nullptr)
+      k_col_step<false><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
+    else if (j < oz_from)
+      k_col_step<true><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
+    else
+      k_col_step_oz<<<n, kColThreads, kOzSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
     note_launch();
     if (rep.time_kernels) {
       PB_CUDA(cudaEventRecord(ev[2 * j + 1], st));
@@ -611,5 +1015,7 @@ void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoin
     note_launch();
   }
 }
+
+size_t oz_slot_bytes(int T) { return size_t(T) * size_t(T - 1) / 2 * size_t(kOzTileBytes); }
 
 }  // namespace pacman_b200

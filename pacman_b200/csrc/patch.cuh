@@ -17,6 +17,7 @@ enum PatchStatus : int {
   kStatusDropped = 1,     // the polynomial block lost at least one axis
   kStatusNonFinite = 2,   // a non-finite local value
   kStatusBreakdown = 4,   // non-positive Cholesky pivot
+  kStatusTimeout = 8,     // a bounded tensor-core pipeline wait gave up
 };
 
 struct PatchArgs {

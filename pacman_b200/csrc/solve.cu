@@ -509,7 +509,7 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   for (int k = 0; k < K; ++k) {
     if (p.m_host[k] == 0) continue;
     if (stat[k] & kStatusDropped) rep.dropped++;
-    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite)))
+    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite | kStatusTimeout)))
       (p.n_host[k] > nbig ? redo_big : redo_small).push_back(k);
   }
   rep.patches_fp64 = int64_t(small.size() + big.size());
