@@ -358,9 +358,9 @@ def main():
         extra["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(out_mixed - out64) / np.linalg.norm(out64))
         extra["fp64_ms_factor"] = f64_stats.get("ms_factor")
 
-    # Roofline of the dominant kernel, the column update of the large-patch
-    # Cholesky (k_col_update): one extra transfer after the timed region with
-    # CUDA events around each of its launches, on the stream it runs on.
+    # Roofline of the dominant kernel, the step kernel of the large-patch
+    # Cholesky: one extra transfer after the timed region with CUDA events
+    # around each of its launches, on the stream it runs on.
     peak = fp64_gemm_peak(torch, dev)
     kst = {}
     plan = pacman.rbf.Plan(3, S, T, precision=args.precision, **kw)
@@ -369,8 +369,9 @@ def main():
     ms_upd = kst.get("ms_update", 0.0)
     achieved = kst.get("update_flops", 0.0) / (ms_upd * 1e-3) / 1e12 if ms_upd else 0.0
     nl = max(1, int(kst.get("update_launches", 0)))
-    roofline = {"bound": "fp64", "kernel": "k_col_update (left-looking Cholesky column update, "
-                                           "FP64 tensor cores)",
+    roofline = {"bound": "fp64", "kernel": "k_col_step / k_col_step_oz (left-looking Cholesky "
+                                           "step: column update on the FP64 tensor cores, from "
+                                           "step 10 on the int8 tensor cores; trsm; next diagonal)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
                 "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 has no "
