@@ -283,19 +283,22 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
 // core, copied to shared memory with bulk async copies.
 constexpr int kOzS = 7;
 constexpr int kOzTileBytes = 4 * kOzS * 8 * 128;      // 28672
-constexpr int kOzStages = 4;                          // pipeline depth, K = 32 per stage
+constexpr int kOzStages = 5;                          // pipeline depth, K = 32 per stage
 constexpr int kOzStageA = 2 * kOzS * 16 * 128;        // two row tiles: 28672
 constexpr int kOzStageB = 2 * kOzS * 8 * 128;         // one row tile: 14336
 constexpr int kOzStage = kOzStageA + kOzStageB;       // 43008
-constexpr int kOzSLOff = kOzStages * kOzStage;        // L[j+1, j] (TB x LDS doubles)
-constexpr int kOzBarOff = kOzSLOff + TB * LDS * 8;    // barriers, TMEM address
+constexpr int kOzBarOff = kOzStages * kOzStage;       // barriers, TMEM address
 constexpr size_t kOzSmem = size_t(kOzBarOff) + 256;  // 2 x OzBars + TMEM address
+constexpr int kOzSLOff = 80 * 1024;                   // phase 3: L[j+1, j] (TB x LDS doubles)
 constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
 constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 
 static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
-static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzSLOff, "staging overlaps L[j+1, j]");
+static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzBarOff, "staging overlaps the barriers");
+static_assert(kOzSLOff >= (2 * TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps D, X");
+static_assert(kOzSLOff + TB * LDS * 8 <= kOzBarOff, "L[j+1, j] overlaps the barriers");
+static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 8 <= 256, "barrier area");
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -440,7 +443,7 @@ __device__ __forceinline__ void oz_levels(uint32_t tmem, double (&v)[32]) {
   const int h = warp >> 2;
 #pragma unroll
   for (int c = 0; c < 32; ++c) v[c] = 0.0;
-#pragma unroll 1
+#pragma unroll
   for (int lev = 2; lev <= kOzS + 1; ++lev) {
     uint32_t z[32];
     const uint32_t addr = tmem + lane_base + uint32_t(64 * (lev - 2) + 32 * h);
@@ -478,13 +481,16 @@ __device__ __forceinline__ void oz_slice_acc(const double (&acc)[4][4][2], doubl
         const int r64 = r & 63;
         uint8_t *dst = stg + (r >> 6) * kOzTileBytes + (c >> 4) * kOzS * 1024 +
                        (r64 >> 3) * 128 + (r64 & 7) * 16 + (c & 15);
-        double x = acc[i][jj][h] * mul;
+        // y = round(x 128^kOzS) as an integer; balanced base-128 digits from
+        // the top: d = round(y / 128^(kOzS-1-s)), y -= d 128^(kOzS-1-s).
+        const double xs = fmin(fmax(acc[i][jj][h] * mul, -127.49), 127.49);
+        long long y = __double2ll_rn(xs * 0x1p42);  // x * 128 * 128^(kOzS-1)
 #pragma unroll
         for (int sl = 0; sl < kOzS; ++sl) {
-          double d = rint(x);
-          d = fmin(fmax(d, -127.0), 127.0);
-          dst[sl * 1024] = uint8_t(int8_t(int(d)));
-          x = (x - d) * 128.0;
+          const int sh = 7 * (kOzS - 1 - sl);
+          const long long d = sh ? ((y + (1ll << (sh - 1))) >> sh) : y;
+          y -= d << sh;
+          dst[sl * 1024] = uint8_t(int8_t(d));
         }
       }
 }
@@ -709,16 +715,24 @@ __global__ void __launch_bounds__(kColThreads, 1)
   if (j > 0)
     ok = oz_kloop(smb, bars, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr, slice_row(j), j);
   {
+    // A[i, j] into sm with coalesced copies (the stages are free: every MMA
+    // finished before oz_kloop returned), then C = A - sigma^2 v per row.
+    const double *Ag = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
+    for (int idx = tid; idx < arows * TB / 2; idx += kColThreads) {
+      const int r = idx >> 5, c2 = idx & 31;
+      cp_async16(sm + r * LDS + 2 * c2, Ag + int64_t(r) * ld + 2 * c2);
+    }
+    cp_async_commit();
     const int r = 32 * (warp & 3) + lane, h = warp >> 2;
     double v[32];
     if (j > 0) oz_levels(tmem, v);
     if (j > 0) tc_fence_before();
-    __syncthreads();  // the stages are free (every MMA finished before oz_kloop returned)
-    if (r < arows) {
-      const double *Ar = W + int64_t(i0 * TB + r) * ld + int64_t(j) * TB + 32 * h;
+    cp_async_wait<0>();
+    __syncthreads();
+    if (j > 0 && r < arows) {
       double *Cr = sm + r * LDS + 32 * h;
 #pragma unroll
-      for (int c = 0; c < 32; ++c) Cr[c] = j > 0 ? __fma_rn(-a.oz_sig2, v[c], Ar[c]) : Ar[c];
+      for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
     }
   }
   // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
@@ -736,16 +750,7 @@ __global__ void __launch_bounds__(kColThreads, 1)
   if (l == 0) {
     // 3. The diagonal tile of step j + 1: D = A[j+1, j+1] - sigma^2 sum_l
     //    128^-l Z_l (p < j, int8) - L[j+1, j] L[j+1, j]^T (FP64), factored.
-    double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
-    if (wr < TB) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj)
-          *reinterpret_cast<double2 *>(sL + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
-              make_double2(acc[i][jj][0], acc[i][jj][1]);
-    }
-    __syncthreads();  // the staging area is copied out; sL is complete
+    __syncthreads();  // the staging area is copied out
     if (j > 0 && ok) {
       const uint8_t *rd = slice_row(j + 1);
       ok = oz_kloop(smb, bars3, tmem, rd, nullptr, rd, j);
@@ -756,14 +761,21 @@ __global__ void __launch_bounds__(kColThreads, 1)
       double v[32];
       if (j > 0) oz_levels(tmem, v);
       if (j > 0) tc_fence_before();
+      async_tile(Ds, W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, tid, kColThreads);
+      cp_async_commit();
+      cp_async_wait<0>();
       __syncthreads();
-      if (r < TB) {
-        const double *Ar = W + int64_t((j + 1) * TB + r) * ld + int64_t(j + 1) * TB + 32 * h;
+      if (j > 0 && r < TB) {
         double *Dr = Ds + r * LDS + 32 * h;
 #pragma unroll
-        for (int c = 0; c < 32; ++c) Dr[c] = j > 0 ? __fma_rn(-a.oz_sig2, v[c], Ar[c]) : Ar[c];
+        for (int c = 0; c < 32; ++c) Dr[c] = __fma_rn(-a.oz_sig2, v[c], Dr[c]);
       }
     }
+    // L[j+1, j] (stored in phase 2) into shared memory for the FP64 term.
+    double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
+    async_tile(sL, W + int64_t(j + 1) * TB * ld + int64_t(j) * TB, ld, tid, kColThreads);
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     if (wr < TB) {
       acc_load(acc, Ds, LDS, wr, wc, lane);
