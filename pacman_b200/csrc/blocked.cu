@@ -247,6 +247,11 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
     redf[tid] = s;
   }
   __syncthreads();
+  {  // the padding rows of the residual column are zero (there is no assembly pass for it)
+    double *rc = a.W + sl.base + int64_t(sl.T) * TB;
+    for (int e = tid; e < (sl.T * TB - n) * F; e += blockDim.x)
+      rc[int64_t(n + e / F) * sl.ld + e % F] = 0.0;
+  }
   if (a.mode == kBigAdjoint) {
     if (tid < nred + 6) a.red_out[int64_t(sl.q) * kRedVals + tid] = redf[tid];
     return;
@@ -859,35 +864,27 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       std::vector<CholPlan> gp(G);
       std::vector<DevMem> gmem(G);
       std::vector<BigSlot *> gds(G);
-      std::vector<int *> gpre(G), gasm(G);
-      std::vector<std::vector<int>> gpre_asm(G);
+      std::vector<int *> gpre(G);
       for (int g = 0; g < G; ++g) {
         gp[g] = chol_prefix(gs[g]);
         const int ng = int(gs[g].size());
-        gpre_asm[g].assign(ng + 1, 0);
-        for (int q = 0; q < ng; ++q)
-          gpre_asm[g][q + 1] = gpre_asm[g][q] + int(count_assemble(false, gs[g][q]));
         const size_t b0 = (sizeof(BigSlot) * ng + 15) & ~size_t(15);
-        const size_t b1 = (sizeof(int) * gp[g].pre.size() + 15) & ~size_t(15);
-        gmem[g].alloc(b0 + b1 + sizeof(int) * (ng + 1) + 64, st);
+        gmem[g].alloc(b0 + sizeof(int) * gp[g].pre.size() + 64, st);
         gds[g] = gmem[g].as<BigSlot>();
         gpre[g] = reinterpret_cast<int *>(gmem[g].as<char>() + b0);
-        gasm[g] = reinterpret_cast<int *>(gmem[g].as<char>() + b0 + b1);
         arena.upload(gs[g].data(), gs[g].size(), gds[g], st);
         arena.upload(gp[g].pre.data(), gp[g].pre.size(), gpre[g], st);
-        arena.upload(gpre_asm[g].data(), gpre_asm[g].size(), gasm[g], st);
       }
       p.aux.make();
       PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN], st));
       for (int g = 0; g < G; ++g) {
         cudaStream_t sg = p.aux.s[g];
         PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
-        // Each group assembles its own slots, so group 0 starts its steps
-        // while the others still assemble.
+        // The Wendland tiles are evaluated inside the step kernels; here only
+        // the polynomial block and the residual column.
         const int ng = int(gs[g].size());
-        k_assemble<<<gpre_asm[g][ng], 256, 0, sg>>>(a, gds[g], gasm[g], ng, 0);
         k_big_poly<<<ng, 256, 0, sg>>>(a, gds[g]);
-        note_launch(2);
+        note_launch();
         if (adjoint) {
           k_big_adj_rhs<<<ng, 256, 0, sg>>>(a, gds[g]);
           note_launch();

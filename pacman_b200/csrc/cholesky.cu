@@ -32,7 +32,7 @@ constexpr int kColRows = 2 * TB;        // rows of one column-update CTA (two ti
 constexpr int kColThreads = 256;
 constexpr int kColStage = (kColRows + TB) * kKLD;  // doubles per pipeline stage
 constexpr size_t kColSmem = size_t(kStages) * kColStage * sizeof(double);
-constexpr size_t kDiagSmem = size_t(TB) * LDS * sizeof(double);
+constexpr size_t kDiagSmem = (size_t(2) * TB * LDS + 6 * TB) * sizeof(double);
 
 // acc += A B^T over one K chunk: A rows wr.., B rows wc.. (both K-contiguous).
 __device__ __forceinline__ void mma_chunk_nt(const double *__restrict__ sA,
@@ -59,6 +59,49 @@ __device__ __forceinline__ void acc_neg(double (&acc)[4][4][2]) {
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) acc[i][jj][0] = -acc[i][jj][0], acc[i][jj][1] = -acc[i][jj][1];
 }
+
+// Rows [ti TB, ti TB + nrows) x columns [tj TB, tj TB + TB) of a slot's
+// Wendland matrix A (TeamFillA, team_ops.hpp:35-52; identity past n) into sT
+// (row stride LDS), by the threads t, t + nt, ...: the step kernels evaluate
+// their tiles instead of reading an assembled copy.  The row and column points
+// are staged in pts (3 (nrows + TB) doubles) first; sync() must be a barrier
+// over the nt threads.
+template <class Sync>
+__device__ __forceinline__ void gen_tile(const BigArgs &a, const BigSlot &sl, int ti, int tj,
+                                         int nrows, double *sT, double *pts, int t, int nt,
+                                         Sync sync) {
+  const int64_t s0 = a.soff[sl.k];
+  double *rx = pts, *ry = rx + nrows, *rz = ry + nrows;
+  double *cx = rz + nrows, *cy = cx + TB, *cz = cy + TB;
+  for (int e = t; e < nrows + TB; e += nt) {
+    const int gi = e < nrows ? ti * TB + e : tj * TB + (e - nrows);
+    double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (gi < sl.n) p = a.src[a.sidx[s0 + gi]];
+    if (e < nrows) {
+      rx[e] = p.x;
+      ry[e] = p.y;
+      rz[e] = p.z;
+    } else {
+      cx[e - nrows] = p.x;
+      cy[e - nrows] = p.y;
+      cz[e - nrows] = p.z;
+    }
+  }
+  sync();
+  for (int e = t; e < nrows * TB; e += nt) {
+    const int r = e >> 6, c = e & 63;
+    const int gi = ti * TB + r, gj = tj * TB + c;
+    double v;
+    if (gi < sl.n && gj < sl.n)
+      v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(rx[r], ry[r], rz[r], cx[c], cy[c], cz[c])),
+                           a.rinv);
+    else
+      v = (gi == gj) ? 1.0 : 0.0;
+    sT[r * LDS + c] = v;
+  }
+}
+
+__device__ __forceinline__ void sync_all() { __syncthreads(); }
 
 // Inverse Cholesky factor X of one 64 x 64 tile D and y = X r (256 threads).  The tile is eliminated as L D L^T with the identity carried
 // along (Gauss-Jordan on [A | I]): at pivot p every row i > p gets
@@ -184,20 +227,24 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
   __shared__ double ys[TB][kMaxF];
   const BigSlot sl = slots[blockIdx.x];
   const int ld = sl.ld;
-  const double *g = a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB;
+  double *gt = sm + TB * LDS;  // the evaluated tile A[j, j]
+  double *pts = sm + 2 * TB * LDS;
+  gen_tile(a, sl, j, j, TB, gt, pts, threadIdx.x, blockDim.x, sync_all);
+  __syncthreads();
   double *rg = a.W + sl.base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
   const bool bad =
-      diag_tile(g, ld, rg, ld, a.F, a.inv + sl.inv + int64_t(j) * TB * TB, sm, cv, dis, ys);
+      diag_tile(gt, LDS, rg, ld, a.F, a.inv + sl.inv + int64_t(j) * TB * TB, sm, cv, dis, ys);
   if (threadIdx.x == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
-// Phase 2 of a factorisation step.  sm holds C (the updated row tiles i0, and
+// Phase 2 of a factorisation step.  sC holds C (the updated row tiles i0, and
 // i0 + 1 when arows = 2 TB; kColRows x LDS doubles).  L[i, j] = C X_j^T on the
-// FP64 tensor cores, stored over C in the workspace and left in acc; then the
-// forward substitution r_i -= L[i, j] y_j.  Uses sm[0, (kColRows + TB) LDS)
-// and ends with a barrier after which sm is free.  256 threads.
+// FP64 tensor cores (X_j through sX, TB x LDS), stored in the workspace and
+// left in acc; then the forward substitution r_i -= L[i, j] y_j with scratch
+// at sm (TB kMaxF + 2 kColRows kMaxF doubles, after sX is consumed).  Ends
+// with a barrier.  256 threads.
 __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, int arows, bool active,
-                          double *sm, double (&acc)[4][4][2]) {
+                          double *sm, double *sC, double *sX, double (&acc)[4][4][2]) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
@@ -205,8 +252,6 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
   double *W = a.W + sl.base;
   double *rcol = W + int64_t(sl.T) * TB;
   double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
-  double *sC = sm;                   // kColRows x LDS
-  double *sX = sm + kColRows * LDS;  // TB x LDS
   {
     const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
     for (int idx = tid; idx < TB * TB / 2; idx += kColThreads) {
@@ -283,11 +328,13 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
 // core, copied to shared memory with bulk async copies.
 constexpr int kOzS = 7;
 constexpr int kOzTileBytes = 4 * kOzS * 8 * 128;      // 28672
-constexpr int kOzStages = 5;                          // pipeline depth, K = 32 per stage
+constexpr int kOzStages = 3;                          // pipeline depth, K = 32 per stage
 constexpr int kOzStageA = 2 * kOzS * 16 * 128;        // two row tiles: 28672
 constexpr int kOzStageB = 2 * kOzS * 8 * 128;         // one row tile: 14336
 constexpr int kOzStage = kOzStageA + kOzStageB;       // 43008
-constexpr int kOzBarOff = kOzStages * kOzStage;       // barriers, TMEM address
+constexpr int kOzGenOff = kOzStages * kOzStage;       // A[i, j] (then C), kColRows x LDS doubles
+constexpr int kOzPtsOff = kOzGenOff + kColRows * LDS * 8;  // points of the evaluated tile
+constexpr int kOzBarOff = kOzPtsOff + 3 * (kColRows + TB) * 8;  // barriers, TMEM address
 constexpr size_t kOzSmem = size_t(kOzBarOff) + 256;  // 2 x OzBars + TMEM address
 constexpr int kOzSLOff = 80 * 1024;                   // phase 3: L[j+1, j] (TB x LDS doubles)
 constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
@@ -295,9 +342,9 @@ constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 column
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 
 static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
-static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzBarOff, "staging overlaps the barriers");
+static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzGenOff, "staging overlaps the tile");
+static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the tile");
 static_assert(kOzSLOff >= (2 * TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps D, X");
-static_assert(kOzSLOff + TB * LDS * 8 <= kOzBarOff, "L[j+1, j] overlaps the barriers");
 static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 8 <= 256, "barrier area");
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
@@ -370,9 +417,11 @@ struct OzBars {
 // [rows of tile rA0 (and rA1)] x [rows of tile rB]^T.  rA0, rA1, rB point to
 // the first slice tile of their tile row (tiles of a row are consecutive in
 // p).  Thread 0 issues the bulk copies, thread 32 the MMAs; every thread
-// returns after the MMAs completed.  false if a wait timed out.
+// returns after the MMAs completed.  Threads 64.. run side(t, nt) meanwhile.
+// false if a wait timed out.
+template <class Side>
 __device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint8_t *rA0,
-                         const uint8_t *rA1, const uint8_t *rB, int nump) {
+                         const uint8_t *rA1, const uint8_t *rB, int nump, Side side) {
   const int tid = threadIdx.x;
   // Earlier generic writes to the stage area before the async-proxy copies.
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -428,6 +477,8 @@ __device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint
       umma_commit(&bar->empty[st]);
     }
     umma_commit(&bar->done);
+  } else if (tid >= 64) {
+    side(tid - 64, int(blockDim.x) - 64);  // warps 2.. are free during the K loop
   }
   __syncthreads();
   if (!mbar_wait(&bar->done, 0u)) ok = false;
@@ -550,17 +601,19 @@ __global__ void __launch_bounds__(kColThreads, 2)
       }
     }
   };
+  const bool active = two || wr < TB;
+  double acc[4][4][2];
+  gen_tile(a, sl, i0, j, arows, sm, sm + kColRows * LDS, tid, kColThreads, sync_all);  // A[i, j]
+  __syncthreads();
+  if (active) {
+    acc_load(acc, sm, LDS, wr, wc, lane);
+    acc_neg(acc);
+  }
+  __syncthreads();
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
     if (s < nch) load(s, s);
     cp_async_commit();
-  }
-  const bool active = two || wr < TB;
-  double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
-  double acc[4][4][2];
-  if (active) {
-    acc_load(acc, C, ld, wr, wc, lane);
-    acc_neg(acc);
   }
   for (int c = 0; c < nch; ++c) {
     cp_async_wait<kStages - 2>();
@@ -584,7 +637,7 @@ __global__ void __launch_bounds__(kColThreads, 2)
         *reinterpret_cast<double2 *>(sm + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
             make_double2(-acc[i][jj][0], -acc[i][jj][1]);
   }
-  step_trsm(a, sl, j, i0, arows, active, sm, acc);
+  step_trsm(a, sl, j, i0, arows, active, sm, sm, sm + kColRows * LDS, acc);
   if (SLICE) {  // int8 slices of the new L tiles for the int8 steps that follow
     uint8_t *stg = reinterpret_cast<uint8_t *>(sm) + kOzStgOff;
     if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
@@ -620,16 +673,19 @@ __global__ void __launch_bounds__(kColThreads, 2)
       cp_async16(sD + r * kKLD + 2 * c2, gA + int64_t(r) * ld + col + 2 * c2);
     }
   };
+  const bool dact = wr < TB;
+  double *Dgen = sm + 2 * kDStage + TB * LDS;  // A[j+1, j+1], after sL
+  gen_tile(a, sl, j + 1, j + 1, TB, Dgen, sm, tid, kColThreads, sync_all);
+  __syncthreads();
+  if (dact) {
+    acc_load(acc, Dgen, LDS, wr, wc, lane);
+    acc_neg(acc);
+  }
+  __syncthreads();
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
     if (s < nch) loadd(s, s);
     cp_async_commit();
-  }
-  const bool dact = wr < TB;
-  double *Dg = W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB;
-  if (dact) {
-    acc_load(acc, Dg, ld, wr, wc, lane);
-    acc_neg(acc);
   }
   for (int c = 0; c < nch; ++c) {
     cp_async_wait<kStages - 2>();
@@ -711,33 +767,34 @@ __global__ void __launch_bounds__(kColThreads, 1)
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
 
-  // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l, into sm (kColRows x LDS).
-  if (j > 0)
-    ok = oz_kloop(smb, bars, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr, slice_row(j), j);
+  // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l in sGen (kColRows x LDS); A[i, j]
+  //    is evaluated by warps 2.. while the K loop runs.
+  double *sGen = reinterpret_cast<double *>(smb + kOzGenOff);
+  double *pts = reinterpret_cast<double *>(smb + kOzPtsOff);
+  if (j > 0) {
+    ok = oz_kloop(smb, bars, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr, slice_row(j), j,
+                  [&](int t0, int nt) {
+                    gen_tile(a, sl, i0, j, arows, sGen, pts, t0, nt,
+                             [&] { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); });
+                  });
+  } else {
+    gen_tile(a, sl, i0, j, arows, sGen, pts, tid, kColThreads, sync_all);
+  }
   {
-    // A[i, j] into sm with coalesced copies (the stages are free: every MMA
-    // finished before oz_kloop returned), then C = A - sigma^2 v per row.
-    const double *Ag = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
-    for (int idx = tid; idx < arows * TB / 2; idx += kColThreads) {
-      const int r = idx >> 5, c2 = idx & 31;
-      cp_async16(sm + r * LDS + 2 * c2, Ag + int64_t(r) * ld + 2 * c2);
-    }
-    cp_async_commit();
     const int r = 32 * (warp & 3) + lane, h = warp >> 2;
     double v[32];
     if (j > 0) oz_levels(tmem, v);
     if (j > 0) tc_fence_before();
-    cp_async_wait<0>();
     __syncthreads();
     if (j > 0 && r < arows) {
-      double *Cr = sm + r * LDS + 32 * h;
+      double *Cr = sGen + r * LDS + 32 * h;
 #pragma unroll
       for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
     }
   }
   // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
   double acc[4][4][2];
-  step_trsm(a, sl, j, i0, arows, active, sm, acc);
+  step_trsm(a, sl, j, i0, arows, active, sm, sGen, sm, acc);
   uint8_t *stg = smb + kOzStgOff;
   if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
   __syncthreads();
@@ -751,19 +808,21 @@ __global__ void __launch_bounds__(kColThreads, 1)
     // 3. The diagonal tile of step j + 1: D = A[j+1, j+1] - sigma^2 sum_l
     //    128^-l Z_l (p < j, int8) - L[j+1, j] L[j+1, j]^T (FP64), factored.
     __syncthreads();  // the staging area is copied out
+    double *Ds = sGen;  // A[j+1, j+1], then D
     if (j > 0 && ok) {
       const uint8_t *rd = slice_row(j + 1);
-      ok = oz_kloop(smb, bars3, tmem, rd, nullptr, rd, j);
+      ok = oz_kloop(smb, bars3, tmem, rd, nullptr, rd, j, [&](int t0, int nt) {
+        gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, t0, nt,
+                 [&] { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); });
+      });
+    } else {
+      gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, tid, kColThreads, sync_all);
     }
-    double *Ds = sm;
     {
       const int r = 32 * (warp & 3) + lane, h = warp >> 2;
       double v[32];
       if (j > 0) oz_levels(tmem, v);
       if (j > 0) tc_fence_before();
-      async_tile(Ds, W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, tid, kColThreads);
-      cp_async_commit();
-      cp_async_wait<0>();
       __syncthreads();
       if (j > 0 && r < TB) {
         double *Dr = Ds + r * LDS + 32 * h;
@@ -784,7 +843,7 @@ __global__ void __launch_bounds__(kColThreads, 1)
     __syncthreads();
     if (wr < TB) acc_store(acc, Ds, LDS, wr, wc, lane);
     __syncthreads();
-    double *Xs = sm + TB * LDS;
+    double *Xs = sm;
     double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
     double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
     double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
@@ -978,7 +1037,7 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
   // First step on the int8 tensor cores (PACMAN_B200_INT8_FROM overrides).
   const char *ofe = std::getenv("PACMAN_B200_INT8_FROM");
-  const int oz_from = ofe ? std::max(1, std::atoi(ofe)) : 10;
+  const int oz_from = ofe ? std::max(1, std::atoi(ofe)) : 4;
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
