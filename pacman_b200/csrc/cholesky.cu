@@ -336,7 +336,7 @@ constexpr int kOzGenOff = kOzStages * kOzStage;       // A[i, j] (then C), kColR
 constexpr int kOzPtsOff = kOzGenOff + kColRows * LDS * 8;  // points of the evaluated tile
 constexpr int kOzBarOff = kOzPtsOff + 3 * (kColRows + TB) * 8;  // barriers, TMEM address
 constexpr size_t kOzSmem = size_t(kOzBarOff) + 256;  // 2 x OzBars + TMEM address
-constexpr int kOzSLOff = 80 * 1024;                   // phase 3: L[j+1, j] (TB x LDS doubles)
+constexpr int kOzSLOff = 40 * 1024;                   // phase 3: L[j+1, j] (TB x LDS doubles)
 constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
 constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
@@ -344,7 +344,7 @@ constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
 static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzGenOff, "staging overlaps the tile");
 static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the tile");
-static_assert(kOzSLOff >= (2 * TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps D, X");
+static_assert(kOzSLOff >= (TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps X");
 static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 8 <= 256, "barrier area");
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
