@@ -111,6 +111,33 @@ PACMAN_B200_API int pacman_b200_rbf_interpolate(int32_t dim, int32_t rbf_functio
                                  const pacman_b200_options *opts,
                                  pacman_b200_stats *stats);
 
+/* One problem of a batched call. */
+typedef struct pacman_b200_problem {
+  int32_t dim;                 /* 1, 2 or 3 */
+  int32_t rbf_function;        /* PACMAN_B200_WENDLAND_C0 .. C8 */
+  const double *source_points; /* n_source x dim, row-major (host or device) */
+  int64_t n_source;
+  const double *source_values; /* n_source x n_fields, row-major */
+  int32_t n_fields;            /* 1 .. 8 */
+  const double *target_points; /* n_target x dim, row-major */
+  int64_t n_target;
+  double *target_values;       /* out: n_target x n_fields (host or device) */
+} pacman_b200_problem;
+
+/*
+ * Many independent transfers in one call.  No counterpart in the reference,
+ * which runs one transfer per call: here the geometry is built per problem,
+ * then the patches of all problems that share (dim, rbf_function, n_fields)
+ * are solved together in one set of launches, and each problem's
+ * partition-of-unity sum is formed from them.  Results equal
+ * pacman_b200_rbf_interpolate on each problem.  opts (shared by all problems,
+ * may be NULL) and stats (totals, may be NULL) as there.
+ */
+PACMAN_B200_API int pacman_b200_rbf_interpolate_batch(const pacman_b200_problem *problems,
+                                                      int32_t count,
+                                                      const pacman_b200_options *opts,
+                                                      pacman_b200_stats *stats);
+
 /* Reusable transfer plan: the geometry (patch radius, centre cover, patch
  * membership lists; src/rbf_pum/interpolator.hpp:76-92 and solver.hpp:45-66)
  * is built once and each execute solves for new source values.  The plan

@@ -68,6 +68,20 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Problem(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32),
+        ("rbf_function", ctypes.c_int32),
+        ("source_points", ctypes.c_void_p),
+        ("n_source", ctypes.c_int64),
+        ("source_values", ctypes.c_void_p),
+        ("n_fields", ctypes.c_int32),
+        ("target_points", ctypes.c_void_p),
+        ("n_target", ctypes.c_int64),
+        ("target_values", ctypes.c_void_p),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/pacman_b200.h.
 _VP = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
@@ -76,6 +90,9 @@ SIGNATURES = {
     "pacman_b200_rbf_interpolate": (ctypes.c_int, [
         ctypes.c_int32, ctypes.c_int32, _VP, ctypes.c_int64, _VP, ctypes.c_int32, _VP,
         ctypes.c_int64, _VP, ctypes.POINTER(Options), ctypes.POINTER(Stats)]),
+    "pacman_b200_rbf_interpolate_batch": (ctypes.c_int, [
+        ctypes.POINTER(Problem), ctypes.c_int32, ctypes.POINTER(Options),
+        ctypes.POINTER(Stats)]),
     "pacman_b200_plan_create": (ctypes.c_int, [
         ctypes.c_int32, _VP, ctypes.c_int64, _VP, ctypes.c_int64, ctypes.POINTER(Options),
         ctypes.POINTER(_VP)]),

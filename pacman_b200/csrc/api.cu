@@ -289,6 +289,297 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
   return 0;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched transfers.  Each problem keeps its own geometry (radius, centres,
+// membership lists).  The patches of all problems with the same dimension and
+// basis are then concatenated into one merged plan: points, centres and lists
+// are copied side by side with the list entries shifted by the running point
+// and membership counts, the source values are laid out with the group's
+// largest field count (missing fields zero), and one solve covers every patch
+// of the group.  The local values of problem i are then the merged local
+// values from its first membership on, and its own partition-of-unity gather
+// turns them into its targets' values.
+
+__global__ void k_shift_i64(const int64_t *__restrict__ in, int64_t n, int64_t add,
+                            int64_t *__restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i] + add;
+}
+
+__global__ void k_shift_i32(const int *__restrict__ in, int64_t n, int add,
+                            int *__restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i] + add;
+}
+
+int shift_grid(int64_t n) {
+  return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)));
+}
+
+int check_problem(const pacman_b200_problem &q, int32_t i) {
+  const std::string at = "problem " + std::to_string(i) + ": ";
+  if (q.dim < 1 || q.dim > 3)
+    return fail(PACMAN_B200_ERR_DIMENSION,
+                at + "The dimension of the points can only be: 1, 2 or 3.");
+  if (int rc = check_basis(q.rbf_function)) return fail(rc, at + g_last_error);
+  if (q.n_fields < 1 || q.n_fields > 8)
+    return fail(PACMAN_B200_ERR_INVALID, at + "n_fields must be in [1, 8]");
+  if (q.n_source < 0 || q.n_target < 0)
+    return fail(PACMAN_B200_ERR_INVALID, at + "negative point count");
+  if ((q.source_points == nullptr || q.source_values == nullptr) && q.n_source > 0)
+    return fail(PACMAN_B200_ERR_INVALID, at + "source arrays are null but n_source > 0");
+  if ((q.target_points == nullptr || q.target_values == nullptr) && q.n_target > 0)
+    return fail(PACMAN_B200_ERR_INVALID, at + "target arrays are null but n_target > 0");
+  return 0;
+}
+
+struct PlanHandle {
+  pacman_b200_plan *h = nullptr;
+  PlanHandle() = default;
+  PlanHandle(const PlanHandle &) = delete;
+  PlanHandle &operator=(const PlanHandle &) = delete;
+  ~PlanHandle() {
+    if (h) pacman_b200_plan_destroy(h);
+  }
+};
+
+// Solves the patches of the problems `ids` (same dim and basis) as one merged
+// plan and writes every problem's target values.
+void solve_group(const pacman_b200_problem *qs, const std::vector<int> &ids,
+                 std::vector<PlanHandle> &plans, const pacman_b200_options &o, cudaStream_t st,
+                 int device, SolveReport &rep) {
+  HostArena::get().reset();  // the previous group has synchronised
+  Plan g;
+  g.device = device;
+  g.stream = st;
+  g.opts = o;
+  g.dim = qs[ids[0]].dim;
+  int Fg = 1;
+  int64_t N = 0, M = 0, K = 0, snnz = 0, tnnz = 0;
+  for (int i : ids) {
+    const Plan &p = plans[i].h->p;
+    Fg = std::max(Fg, int(qs[i].n_fields));
+    N += p.n;
+    M += p.m;
+    K += p.K;
+    snnz += p.snnz;
+    tnnz += p.tnnz;
+  }
+  if (N > 0x7fffffffll || M > 0x7fffffffll || K > 0x7fffffffll || snnz > 0x7fffffffll ||
+      tnnz > 0x7fffffffll)
+    throw Error{PACMAN_B200_ERR_LIMIT,
+                "a batch group is limited to 2^31 - 1 points, patches and memberships"};
+  g.n = N;
+  g.m = M;
+  g.K = int(K);
+  g.snnz = snnz;
+  g.tnnz = tnnz;
+  g.src4.alloc(sizeof(double4) * std::max<int64_t>(N, 1), st);
+  g.tgt4.alloc(sizeof(double4) * std::max<int64_t>(M, 1), st);
+  g.centers.alloc(sizeof(double4) * std::max<int64_t>(K, 1), st);
+  g.soff.alloc(sizeof(int64_t) * (K + 1), st);
+  g.toff.alloc(sizeof(int64_t) * (K + 1), st);
+  g.sidx.alloc(sizeof(int) * std::max<int64_t>(snnz, 1), st);
+  g.tidx.alloc(sizeof(int) * std::max<int64_t>(tnnz, 1), st);
+  DevMem vals;
+  vals.alloc(sizeof(double) * std::max<int64_t>(N, 1) * Fg, st);
+  PB_CUDA(cudaMemsetAsync(vals.p, 0, sizeof(double) * std::max<int64_t>(N, 1) * Fg, st));
+  g.n_host.reserve(size_t(K));
+  g.m_host.reserve(size_t(K));
+  std::vector<int64_t> toff_of(ids.size());
+  int64_t n0 = 0, m0 = 0, k0 = 0, s0 = 0, t0 = 0;
+  for (size_t u = 0; u < ids.size(); ++u) {
+    const int i = ids[u];
+    const Plan &p = plans[i].h->p;
+    const pacman_b200_problem &q = qs[i];
+    toff_of[u] = t0;
+    if (p.n > 0)
+      PB_CUDA(cudaMemcpy2DAsync(vals.as<double>() + n0 * Fg, sizeof(double) * Fg,
+                                q.source_values, sizeof(double) * q.n_fields,
+                                sizeof(double) * q.n_fields, size_t(p.n), cudaMemcpyDefault, st));
+    if (p.n > 0)
+      PB_CUDA(cudaMemcpyAsync(g.src4.as<double4>() + n0, p.src4.p, sizeof(double4) * p.n,
+                              cudaMemcpyDeviceToDevice, st));
+    if (p.m > 0)
+      PB_CUDA(cudaMemcpyAsync(g.tgt4.as<double4>() + m0, p.tgt4.p, sizeof(double4) * p.m,
+                              cudaMemcpyDeviceToDevice, st));
+    if (p.K > 0) {
+      PB_CUDA(cudaMemcpyAsync(g.centers.as<double4>() + k0, p.centers.p, sizeof(double4) * p.K,
+                              cudaMemcpyDeviceToDevice, st));
+      k_shift_i64<<<shift_grid(p.K + 1), 256, 0, st>>>(p.soff.as<int64_t>(), p.K + 1, s0,
+                                                       g.soff.as<int64_t>() + k0);
+      k_shift_i64<<<shift_grid(p.K + 1), 256, 0, st>>>(p.toff.as<int64_t>(), p.K + 1, t0,
+                                                       g.toff.as<int64_t>() + k0);
+      note_launch(2);
+      if (p.snnz > 0) {
+        k_shift_i32<<<shift_grid(p.snnz), 256, 0, st>>>(p.sidx.as<int>(), p.snnz, int(n0),
+                                                        g.sidx.as<int>() + s0);
+        note_launch();
+      }
+      if (p.tnnz > 0) {
+        k_shift_i32<<<shift_grid(p.tnnz), 256, 0, st>>>(p.tidx.as<int>(), p.tnnz, int(m0),
+                                                        g.tidx.as<int>() + t0);
+        note_launch();
+      }
+      g.n_host.insert(g.n_host.end(), p.n_host.begin(), p.n_host.end());
+      g.m_host.insert(g.m_host.end(), p.m_host.begin(), p.m_host.end());
+    }
+    n0 += p.n;
+    m0 += p.m;
+    k0 += p.K;
+    s0 += p.snnz;
+    t0 += p.tnnz;
+  }
+  PB_CUDA(cudaGetLastError());
+  g.local.alloc(sizeof(double) * std::max<int64_t>(tnnz, 1) * Fg, st);
+  solve_patches(g, qs[ids[0]].rbf_function, vals.as<double>(), Fg, o.precision,
+                g.local.as<double>(), rep, false);
+  DevMem obuf;
+  for (size_t u = 0; u < ids.size(); ++u) {
+    const int i = ids[u];
+    Plan &p = plans[i].h->p;
+    const pacman_b200_problem &q = qs[i];
+    if (p.m == 0) continue;
+    const bool direct = q.n_fields == Fg && is_device_ptr(q.target_values, device);
+    double *o = q.target_values;
+    if (!direct) {
+      obuf.alloc(sizeof(double) * size_t(p.m) * Fg, st);
+      o = obuf.as<double>();
+    }
+    pu_gather(p, g.local.as<double>() + toff_of[u] * Fg, Fg, o);
+    if (!direct)
+      PB_CUDA(cudaMemcpy2DAsync(q.target_values, sizeof(double) * q.n_fields, o,
+                                sizeof(double) * Fg, sizeof(double) * q.n_fields, size_t(p.m),
+                                cudaMemcpyDefault, st));
+  }
+  PB_CUDA(cudaStreamSynchronize(st));
+  g.stream = st;  // merged buffers are freed stream-ordered on the batch stream
+}
+
+int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_options *opts,
+              pacman_b200_stats *stats) {
+  if (count < 0) return fail(PACMAN_B200_ERR_INVALID, "count must be >= 0");
+  if (count > 0 && qs == nullptr) return fail(PACMAN_B200_ERR_INVALID, "problems is null");
+  pacman_b200_options o;
+  pacman_b200_options_init(&o);
+  if (opts) o = *opts;
+  if (int rc = check_opts(o)) return rc;
+  for (int32_t i = 0; i < count; ++i)
+    if (int rc = check_problem(qs[i], i)) return rc;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (count == 0) return 0;
+  cudaStream_t own = nullptr;
+  try {
+    DeviceScope ds(o.device);
+    o.device = ds.dev;
+    if (!o.stream) {
+      PB_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+      o.stream = own;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(o.stream);
+    cudaEvent_t e0, e1, e2;
+    PB_CUDA(cudaEventCreate(&e0));
+    PB_CUDA(cudaEventCreate(&e1));
+    PB_CUDA(cudaEventCreate(&e2));
+    PB_CUDA(cudaEventRecord(e0, st));
+    const int64_t launches0 = launch_counter();
+    std::vector<PlanHandle> plans(static_cast<size_t>(count));
+    int rc = 0;
+    for (int32_t i = 0; i < count && rc == 0; ++i) {
+      const pacman_b200_problem &q = qs[i];
+      rc = create_plan(q.dim, q.source_points, q.n_source, q.target_points, q.n_target, &o,
+                       &plans[i].h);
+      if (rc) g_last_error = "problem " + std::to_string(i) + ": " + g_last_error;
+    }
+    if (rc) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaEventDestroy(e2);
+      if (own) cudaStreamDestroy(own);
+      return rc;
+    }
+    PB_CUDA(cudaEventRecord(e1, st));
+    // Problems with targets but no patches get zeros; the rest are grouped by
+    // (dim, basis) in first-seen order.
+    std::vector<std::pair<int, int>> keys;
+    std::vector<std::vector<int>> groups;
+    for (int32_t i = 0; i < count; ++i) {
+      const Plan &p = plans[i].h->p;
+      const pacman_b200_problem &q = qs[i];
+      if (p.m == 0) continue;
+      if (p.n == 0 || p.K == 0) {
+        const size_t bytes = sizeof(double) * size_t(p.m) * q.n_fields;
+        if (is_device_ptr(q.target_values, ds.dev))
+          PB_CUDA(cudaMemsetAsync(q.target_values, 0, bytes, st));
+        else
+          std::memset(q.target_values, 0, bytes);
+        continue;
+      }
+      const std::pair<int, int> key(q.dim, q.rbf_function);
+      size_t gi = 0;
+      while (gi < keys.size() && keys[gi] != key) ++gi;
+      if (gi == keys.size()) {
+        keys.push_back(key);
+        groups.emplace_back();
+      }
+      groups[gi].push_back(i);
+    }
+    SolveReport rep;
+    for (const auto &ids : groups) solve_group(qs, ids, plans, o, st, ds.dev, rep);
+    PB_CUDA(cudaEventRecord(e2, st));
+    PB_CUDA(cudaEventSynchronize(e2));
+    PB_CUDA(cudaGetLastError());
+    if (stats) {
+      float ms_solve = 0.f, ms_total = 0.f;
+      cudaEventElapsedTime(&ms_solve, e1, e2);
+      cudaEventElapsedTime(&ms_total, e0, e2);
+      double rmax = 0.0;
+      for (int32_t i = 0; i < count; ++i) {
+        const Plan &p = plans[i].h->p;
+        rmax = std::max(rmax, p.radius);
+        stats->num_candidates += p.ncand;
+        stats->num_patches += p.K;
+        stats->sum_n += p.snnz;
+        stats->sum_m += p.tnnz;
+        for (int v : p.n_host) stats->max_n = std::max<int64_t>(stats->max_n, v);
+        stats->ms_geometry += p.ms_geometry;
+      }
+      stats->radius = rmax;
+      stats->patches_fp32 = rep.patches_fp32;
+      stats->patches_fp64 = rep.patches_fp64;
+      stats->patches_fallback = rep.patches_fallback;
+      stats->dropped_axis_patches = rep.dropped;
+      stats->ms_solve = ms_solve;
+      stats->ms_total = ms_total;
+      stats->kernel_launches = launch_counter() - launches0;
+      stats->ms_factor = rep.ms_factor;
+      stats->factor_flops = rep.factor_flops;
+      stats->ms_update = rep.ms_update;
+      stats->update_flops = rep.update_flops;
+      stats->update_launches = rep.update_launches;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    plans.clear();
+    if (own) {
+      cudaStreamSynchronize(own);
+      cudaStreamDestroy(own);
+      own = nullptr;
+    }
+  } catch (const Error &e) {
+    if (own) {
+      cudaStreamSynchronize(own);
+      cudaStreamDestroy(own);
+    }
+    return fail(e.code, e.msg);
+  }
+  return 0;
+}
+
 }  // namespace
 }  // namespace pacman_b200
 
@@ -475,6 +766,13 @@ int pacman_b200_rbf_interpolate(int32_t dim, int32_t basis, const double *src, i
   rc = execute_plan(plan, basis, vals, F, out, stats);
   pacman_b200_plan_destroy(plan);
   return rc;
+}
+
+int pacman_b200_rbf_interpolate_batch(const pacman_b200_problem *problems, int32_t count,
+                                      const pacman_b200_options *opts,
+                                      pacman_b200_stats *stats) {
+  g_last_error.clear();
+  return run_batch(problems, count, opts, stats);
 }
 
 }  // extern "C"

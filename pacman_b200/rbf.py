@@ -125,6 +125,80 @@ def interpolate(space_dimension, execspace, rbf_function, source_points, source_
     return out
 
 
+def interpolate_batch(problems, *, nodes_per_cluster=50, relative_overlap=0.15,
+                      support_radius=0.1, precision="fp64", device=None, stats=None,
+                      stream=None):
+    """Many independent transfers in one call (no counterpart in the
+    reference, which runs one transfer per call).  ``problems`` is a sequence
+    of ``(space_dimension, rbf_function, source_points, source_values,
+    target_points)`` with the meaning, shapes and checks of ``interpolate``;
+    all numpy or all CUDA torch tensors on one device.  The patches of every
+    problem that shares (space_dimension, rbf_function) are solved together in
+    one set of launches.  Returns the list of target values, each as
+    ``interpolate`` returns it; ``stats`` receives the totals."""
+    lib = _lib.load()
+    items = list(problems)
+    if not items:
+        return []
+    on_gpu = _is_cuda_tensor(items[0][2])
+    keep, outs = [], []
+    arr = (_lib.Problem * len(items))()
+    dev = None
+    for i, item in enumerate(items):
+        if len(item) != 5:
+            raise ValueError("each problem is (space_dimension, rbf_function, source_points, "
+                             "source_values, target_points)")
+        dim, fn, sp, sv, tp = item
+        if int(fn) not in vars(functions).values():
+            raise ValueError(f"Unsupported RBF function selector: {int(fn)}")
+        if _is_cuda_tensor(sp) != on_gpu:
+            raise ValueError("problems must be all numpy or all CUDA tensors")
+        if on_gpu:
+            import torch
+            sp = sp.to(torch.float64).contiguous()
+            if dev is None:
+                dev = sp.device
+            elif sp.device != dev:
+                raise ValueError("all CUDA problems must be on one device")
+            sv = sv.to(device=dev, dtype=torch.float64).contiguous()
+            tp = tp.to(device=dev, dtype=torch.float64).contiguous()
+            shapes = (tuple(sp.shape), tuple(sv.shape), tuple(tp.shape))
+        else:
+            sp = np.ascontiguousarray(sp, dtype=np.float64)
+            sv = np.ascontiguousarray(sv, dtype=np.float64)
+            tp = np.ascontiguousarray(tp, dtype=np.float64)
+            shapes = (sp.shape, sv.shape, tp.shape)
+        _check_shapes(int(dim), *shapes)
+        n, m = shapes[0][0], shapes[2][0]
+        F = 1 if len(shapes[1]) == 1 else shapes[1][1]
+        out_shape = (m,) if len(shapes[1]) == 1 else (m, F)
+        if on_gpu:
+            import torch
+            out = torch.empty(out_shape, dtype=torch.float64, device=dev)
+            ptrs = (sp.data_ptr(), sv.data_ptr(), tp.data_ptr(), out.data_ptr())
+        else:
+            out = np.zeros(out_shape, dtype=np.float64)
+            ptrs = (sp.ctypes.data, sv.ctypes.data, tp.ctypes.data, out.ctypes.data)
+        keep.append((sp, sv, tp))
+        outs.append(out)
+        arr[i] = _lib.Problem(int(dim), int(fn), ptrs[0] if n else None, n,
+                              ptrs[1] if n else None, F, ptrs[2] if m else None, m,
+                              ptrs[3] if m else None)
+    if on_gpu:
+        import torch
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        device = dev.index
+    opts = _options(nodes_per_cluster, relative_overlap, support_radius, precision, device,
+                    stream)
+    st = _lib.Stats()
+    rc = lib.pacman_b200_rbf_interpolate_batch(arr, len(items), ctypes.byref(opts),
+                                               ctypes.byref(st))
+    _lib.raise_for(rc, "pacman.rbf.interpolate_batch")
+    if stats is not None:
+        stats.update(st.as_dict())
+    return outs
+
+
 def _as_array(x):
     """(pointer, shape, kind, keep-alive) of a float64 C-contiguous view of x:
     CUDA torch tensors stay on the device, everything else becomes numpy."""
