@@ -371,7 +371,7 @@ def main():
     nl = max(1, int(kst.get("update_launches", 0)))
     roofline = {"bound": "fp64", "kernel": "k_col_step / k_col_step_oz (left-looking Cholesky "
                                            "step: column update on the FP64 tensor cores, from "
-                                           "step 10 on the int8 tensor cores; trsm; next diagonal)",
+                                           "step 4 on the int8 tensor cores; trsm; next diagonal)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
                 "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 has no "
@@ -386,7 +386,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/i8" if args.precision == "mixed" else "f64",
         "data": "synthetic (seeded numpy generators; no public data set)",
         "config": config_dict(args, w),
         "e2e": {"value": world * m / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),

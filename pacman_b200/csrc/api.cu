@@ -10,8 +10,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "plan.hpp"
 
@@ -315,8 +318,29 @@ __global__ void k_shift_i32(const int *__restrict__ in, int64_t n, int add,
     out[i] = in[i] + add;
 }
 
+// dst[r, f] = src[r, f] for the first `cols` fields of `rows` rows (row
+// strides sf and df doubles): field-count changes between a problem's arrays
+// and the merged layout.
+__global__ void k_copy_fields(const double *__restrict__ src, int sf, double *__restrict__ dst,
+                              int df, int cols, int64_t rows) {
+  const int64_t n = rows * cols;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / cols;
+    const int f = int(e - r * cols);
+    dst[r * df + f] = src[r * sf + f];
+  }
+}
+
 int shift_grid(int64_t n) {
   return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)));
+}
+
+void copy_fields(const double *src, int sf, double *dst, int df, int cols, int64_t rows,
+                 cudaStream_t st) {
+  if (rows <= 0) return;
+  k_copy_fields<<<shift_grid(rows * cols), 256, 0, st>>>(src, sf, dst, df, cols, rows);
+  note_launch();
 }
 
 int check_problem(const pacman_b200_problem &q, int32_t i) {
@@ -344,6 +368,56 @@ struct PlanHandle {
   ~PlanHandle() {
     if (h) pacman_b200_plan_destroy(h);
   }
+};
+
+// Host threads that build the per-problem geometry of a batch, one stream
+// each.  The plans keep those streams for their stream-ordered frees, so the
+// streams live until release(), after the plans are gone.
+struct GeometryWorkers {
+  std::vector<cudaStream_t> streams;
+  int run(const pacman_b200_problem *qs, int32_t count, const pacman_b200_options &o, int dev,
+          std::vector<PlanHandle> &plans) {
+    int nt = 8;
+    if (const char *e = std::getenv("PACMAN_B200_BATCH_THREADS")) nt = std::atoi(e);
+    nt = std::max(1, std::min<int>(nt, count));
+    streams.assign(size_t(nt), nullptr);
+    for (auto &s : streams) PB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::atomic<int> next{0};
+    std::atomic<bool> stop{false};
+    std::vector<int> rcs(size_t(count), 0);
+    std::vector<std::string> msgs(static_cast<size_t>(count));
+    auto work = [&](int w) {
+      cudaSetDevice(dev);
+      pacman_b200_options ow = o;
+      ow.stream = streams[size_t(w)];
+      for (int i = next++; i < count && !stop; i = next++) {
+        const pacman_b200_problem &q = qs[i];
+        const int rc = create_plan(q.dim, q.source_points, q.n_source, q.target_points,
+                                   q.n_target, &ow, &plans[size_t(i)].h);
+        if (rc) {
+          rcs[size_t(i)] = rc;
+          msgs[size_t(i)] = g_last_error;
+          stop = true;
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < nt; ++w) th.emplace_back(work, w);
+    work(0);
+    for (auto &t : th) t.join();
+    for (int32_t i = 0; i < count; ++i)
+      if (rcs[size_t(i)]) return fail(rcs[size_t(i)], "problem " + std::to_string(i) + ": " + msgs[size_t(i)]);
+    return 0;
+  }
+  void release() {
+    for (auto s : streams) {
+      if (!s) continue;
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+    streams.clear();
+  }
+  ~GeometryWorkers() { release(); }
 };
 
 // Solves the patches of the problems `ids` (same dim and basis) as one merged
@@ -396,10 +470,11 @@ void solve_group(const pacman_b200_problem *qs, const std::vector<int> &ids,
     const Plan &p = plans[i].h->p;
     const pacman_b200_problem &q = qs[i];
     toff_of[u] = t0;
-    if (p.n > 0)
-      PB_CUDA(cudaMemcpy2DAsync(vals.as<double>() + n0 * Fg, sizeof(double) * Fg,
-                                q.source_values, sizeof(double) * q.n_fields,
-                                sizeof(double) * q.n_fields, size_t(p.n), cudaMemcpyDefault, st));
+    if (p.n > 0) {
+      InBuf v;
+      v.stage(q.source_values, size_t(p.n) * q.n_fields, device, st);
+      copy_fields(v.ptr, q.n_fields, vals.as<double>() + n0 * Fg, Fg, q.n_fields, p.n, st);
+    }
     if (p.n > 0)
       PB_CUDA(cudaMemcpyAsync(g.src4.as<double4>() + n0, p.src4.p, sizeof(double4) * p.n,
                               cudaMemcpyDeviceToDevice, st));
@@ -437,23 +512,34 @@ void solve_group(const pacman_b200_problem *qs, const std::vector<int> &ids,
   g.local.alloc(sizeof(double) * std::max<int64_t>(tnnz, 1) * Fg, st);
   solve_patches(g, qs[ids[0]].rbf_function, vals.as<double>(), Fg, o.precision,
                 g.local.as<double>(), rep, false);
-  DevMem obuf;
+  DevMem obuf, obuf2;
   for (size_t u = 0; u < ids.size(); ++u) {
     const int i = ids[u];
     Plan &p = plans[i].h->p;
     const pacman_b200_problem &q = qs[i];
     if (p.m == 0) continue;
-    const bool direct = q.n_fields == Fg && is_device_ptr(q.target_values, device);
+    p.stream = st;  // the gather is ordered after the merged solve
+    const bool out_dev = is_device_ptr(q.target_values, device);
+    const bool direct = q.n_fields == Fg && out_dev;
     double *o = q.target_values;
     if (!direct) {
       obuf.alloc(sizeof(double) * size_t(p.m) * Fg, st);
       o = obuf.as<double>();
     }
     pu_gather(p, g.local.as<double>() + toff_of[u] * Fg, Fg, o);
-    if (!direct)
-      PB_CUDA(cudaMemcpy2DAsync(q.target_values, sizeof(double) * q.n_fields, o,
-                                sizeof(double) * Fg, sizeof(double) * q.n_fields, size_t(p.m),
-                                cudaMemcpyDefault, st));
+    if (direct) continue;
+    if (out_dev) {
+      copy_fields(o, Fg, q.target_values, q.n_fields, q.n_fields, p.m, st);
+      continue;
+    }
+    const double *h = o;
+    if (q.n_fields != Fg) {
+      obuf2.alloc(sizeof(double) * size_t(p.m) * q.n_fields, st);
+      copy_fields(o, Fg, obuf2.as<double>(), q.n_fields, q.n_fields, p.m, st);
+      h = obuf2.as<double>();
+    }
+    PB_CUDA(cudaMemcpyAsync(q.target_values, h, sizeof(double) * size_t(p.m) * q.n_fields,
+                            cudaMemcpyDeviceToHost, st));
   }
   PB_CUDA(cudaStreamSynchronize(st));
   g.stream = st;  // merged buffers are freed stream-ordered on the batch stream
@@ -486,15 +572,15 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
     PB_CUDA(cudaEventCreate(&e2));
     PB_CUDA(cudaEventRecord(e0, st));
     const int64_t launches0 = launch_counter();
+    // Geometry per problem on a few host threads, each with its own stream:
+    // the geometry phase waits on the device several times, and the threads
+    // overlap those waits and the small launches of different problems.
+    GeometryWorkers gw;  // declared first: its streams outlive the plans
     std::vector<PlanHandle> plans(static_cast<size_t>(count));
-    int rc = 0;
-    for (int32_t i = 0; i < count && rc == 0; ++i) {
-      const pacman_b200_problem &q = qs[i];
-      rc = create_plan(q.dim, q.source_points, q.n_source, q.target_points, q.n_target, &o,
-                       &plans[i].h);
-      if (rc) g_last_error = "problem " + std::to_string(i) + ": " + g_last_error;
-    }
+    int rc = gw.run(qs, count, o, ds.dev, plans);
     if (rc) {
+      plans.clear();
+      gw.release();
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
       cudaEventDestroy(e2);
@@ -555,6 +641,7 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
       stats->ms_solve = ms_solve;
       stats->ms_total = ms_total;
       stats->kernel_launches = launch_counter() - launches0;
+      for (int32_t i = 0; i < count; ++i) stats->kernel_launches += plans[i].h->p.launches_geometry;
       stats->ms_factor = rep.ms_factor;
       stats->factor_flops = rep.factor_flops;
       stats->ms_update = rep.ms_update;
@@ -565,6 +652,7 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
     plans.clear();
+    gw.release();
     if (own) {
       cudaStreamSynchronize(own);
       cudaStreamDestroy(own);
