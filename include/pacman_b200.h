@@ -189,6 +189,28 @@ PACMAN_B200_API int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, i
 PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local);
 
 /*
+ * Target sharding of one transfer over `world` GPUs, one process per GPU
+ * (no counterpart in the reference, which runs on one device).  Every rank
+ * creates the same plan (all sources, all targets: the patch cover depends on
+ * both) and calls this with its rank.  The targets are cut into `world`
+ * ranges of their Morton order over the source bounding box, balanced by the
+ * solve cost n^3 of the patches each range needs; the cut uses integer data
+ * only, so all ranks agree on it.  Afterwards an execute solves only the
+ * patches holding an owned target, writes the owned targets' values (bit-
+ * identical to the unsharded transfer) and zero elsewhere: the sum over the
+ * ranks (one all-reduce) is the whole result.  The adjoint of a sharded plan
+ * gives this shard's contribution to the source-value gradient and the
+ * owned targets' coordinate gradients.  A plan is sharded once.
+ */
+PACMAN_B200_API int pacman_b200_plan_shard(pacman_b200_plan *plan, int32_t rank, int32_t world);
+
+/* Targets of the plan's shard (all targets for an unsharded plan): their
+ * number in *count, and, when owned is not NULL, their indices ascending
+ * (*count entries). */
+PACMAN_B200_API int pacman_b200_plan_owned_targets(const pacman_b200_plan *plan, int64_t *count,
+                                                   int32_t *owned);
+
+/*
  * Patch radius (the transfer's cluster-size heuristic: 2*dim+1 sample points
  * projected onto their nearest source, k-th nearest source distance with
  * k = nodes_per_cluster, median) WITHOUT ANY DEVICE ALLOCATION.  No

@@ -201,15 +201,18 @@ __device__ __forceinline__ int64_t find_sorted(const int *a, int64_t n, int v) {
 }
 
 // d (sum_f G_f out_f) / d y per target.
-__global__ void k_target_grad(int64_t M, int dim, const double4 *__restrict__ tgt, GridView cg,
+__global__ void k_target_grad(int64_t M, const int *__restrict__ tlist, int dim,
+                              const double4 *__restrict__ tgt, GridView cg,
                               const double4 *__restrict__ centers, double r, double rinv,
                               const double *__restrict__ wsum, const double *__restrict__ wgrad,
                               const int64_t *__restrict__ toff, const int *__restrict__ tidx,
                               const double *__restrict__ local, const double *__restrict__ dloc,
                               const double *__restrict__ gout, int F, double *grad) {
   WeightTerm terms[kMaxC];
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < M;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  // M targets: all (tlist null) or those of a shard's list.
+  for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < M;
+       it += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = tlist ? tlist[it] : it;
     const double4 y = tgt[t];
     const double S = wsum[t];
     const double gS[3] = {wgrad[3 * t], wgrad[3 * t + 1], wgrad[3 * t + 2]};
@@ -343,11 +346,16 @@ void adjoint(Plan &p, const double *gout, double *grad_values, double *grad_targ
         p.toff.as<int64_t>(), p.tidx.as<int>(), p.alpha.as<double>(), p.beta.as<double>(),
         p.act.as<int>(), p.saved_basis, 1.0 / p.opts.support_radius, F, dloc.as<double>());
     note_launch();
-    k_target_grad<<<blocks_for(M, 128, 148 * 64), 128, 0, st>>>(
-        M, p.dim, p.tgt4.as<double4>(), p.cgrid.view, p.centers.as<double4>(), r, rinv,
-        wsum.as<double>(), wgrad.as<double>(), p.toff.as<int64_t>(), p.tidx.as<int>(),
-        p.local.as<double>(), dloc.as<double>(), gout, F, grad_targets);
-    note_launch();
+    const bool sharded = p.m_owned >= 0;
+    const int64_t Mg = sharded ? p.m_owned : M;
+    if (Mg > 0) {
+      k_target_grad<<<blocks_for(Mg, 128, 148 * 64), 128, 0, st>>>(
+          Mg, sharded ? p.tlist.as<int>() : nullptr, p.dim, p.tgt4.as<double4>(), p.cgrid.view,
+          p.centers.as<double4>(), r, rinv, wsum.as<double>(), wgrad.as<double>(),
+          p.toff.as<int64_t>(), p.tidx.as<int>(), p.local.as<double>(), dloc.as<double>(), gout,
+          F, grad_targets);
+      note_launch();
+    }
   }
   PB_CUDA(cudaGetLastError());
   PB_CUDA(cudaStreamSynchronize(st));

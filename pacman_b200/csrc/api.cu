@@ -839,6 +839,38 @@ int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local) {
   return 0;
 }
 
+int pacman_b200_plan_shard(pacman_b200_plan *plan, int32_t rank, int32_t world) {
+  if (!plan) return fail(PACMAN_B200_ERR_INVALID, "plan is null");
+  try {
+    DeviceScope ds(plan->p.device);
+    shard_plan(plan->p, rank, world);
+  } catch (const Error &e) {
+    return fail(e.code, e.msg);
+  }
+  return 0;
+}
+
+int pacman_b200_plan_owned_targets(const pacman_b200_plan *plan, int64_t *count, int32_t *owned) {
+  if (!plan || !count) return fail(PACMAN_B200_ERR_INVALID, "null argument");
+  const Plan &p = plan->p;
+  const bool sharded = p.m_owned >= 0;
+  *count = sharded ? p.m_owned : p.m;
+  if (!owned || *count == 0) return 0;
+  try {
+    DeviceScope ds(p.device);
+    if (sharded) {
+      PB_CUDA(cudaMemcpyAsync(owned, p.tlist.p, sizeof(int32_t) * size_t(*count),
+                              cudaMemcpyDefault, p.stream));
+      PB_CUDA(cudaStreamSynchronize(p.stream));
+    } else {
+      for (int64_t i = 0; i < *count; ++i) owned[i] = int32_t(i);
+    }
+  } catch (const Error &e) {
+    return fail(e.code, e.msg);
+  }
+  return 0;
+}
+
 int pacman_b200_rbf_interpolate(int32_t dim, int32_t basis, const double *src, int64_t n,
                                 const double *vals, int32_t F, const double *tgt, int64_t m,
                                 double *out, const pacman_b200_options *opts,

@@ -862,79 +862,221 @@ __global__ void __launch_bounds__(kColThreads, 1)
 
 // Backward sweep L^T z = y of one slot (CTA per slot), tile row by tile row
 // from the last: z_s = X_s^T (y_s - sum_{t>s} L[t, s]^T z_t), with the tile
-// inverses X_s of the factorisation.  Warp w takes the tiles t = s + 1 + w,
-// s + 9 + w, ... of column s and streams them from global memory (lane: two
-// columns, every row coalesced); the warps' partial sums meet in shared
-// memory.  z goes to zc (per slot) and, in the forward, to alpha_c per
-// (patch, source).
-__global__ void __launch_bounds__(256, 3) k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
-  __shared__ double part[8][TB][kMaxF];
-  __shared__ double accs[TB][kMaxF];
+// inverses X_s of the factorisation.  The sweep is a chain of T dependent
+// levels, so the time of a large slot is set by how fast its tiles reach the
+// SM: warp 8 streams them with bulk async copies, in sweep order and
+// independent of z, through a ring of kBkStages 32 KB stages (the tiles
+// L[t, s], t > s, as 64 row copies of 512 bytes, then X_s as one copy), up to
+// kBkStages tiles ahead of the arithmetic.  Warps 0..7 take the L tiles of a
+// level in turn (lane: two columns r of the tile, all rows c), then meet to
+// finish z_s.  z goes to zc (per slot) and, in the forward, to alpha_c per
+// (patch, source).  Every wait is bounded; a time-out marks the patch
+// (status 8), the CTA keeps its barrier sequence, stops issuing copies and
+// waits for the copies it issued before it returns.
+constexpr int kBkStages = 5;
+constexpr int kBkTile = TB * TB * 8;  // bytes of one stage
+
+size_t chol_back_smem(int F) {
+  // stages, part, accs, full/empty barriers, abort flag and issue counter
+  return size_t(kBkStages) * kBkTile + size_t(8 * TB * F + TB * F) * 8 + 2 * kBkStages * 8 + 16;
+}
+
+__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *b, uint32_t cnt) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(b)),
+               "r"(cnt)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for a phase that gives up early once the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t *b, uint32_t parity,
+                                                volatile int *abort_flag) {
+  for (int it = 0; it < kOzWaitLimit; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if (*abort_flag) return false;
+  }
+  return false;
+}
+
+// Bounded wait until item x is issued, then for its data.
+__device__ __forceinline__ bool bk_wait_item(volatile int *issued, volatile int *abort_flag,
+                                             uint64_t *full, int x) {
+  bool ok = false;
+  for (int it = 0; it < kOzWaitLimit && !ok; ++it) {
+    ok = *issued > x;
+    if (*abort_flag) return false;
+  }
+  return ok && mbar_wait_abort(&full[x % kBkStages], uint32_t((x / kBkStages) & 1), abort_flag);
+}
+
+__global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
+  extern __shared__ __align__(128) uint8_t smem[];
   const BigSlot sl = slots[blockIdx.x];
   const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ld = sl.ld;
+  double *stage0 = reinterpret_cast<double *>(smem);
+  double *part = reinterpret_cast<double *>(smem + size_t(kBkStages) * kBkTile);  // [8][TB][F]
+  double *accs = part + 8 * TB * F;                                                // [TB][F]
+  uint64_t *full = reinterpret_cast<uint64_t *>(accs + TB * F);
+  uint64_t *empty = full + kBkStages;
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kBkStages);
+  // Items the producer has issued.  A consumer waits on the full barrier of
+  // item x only once x is issued: x - kBkStages, the previous item of that
+  // stage, has then landed and been released, so the barrier is in the
+  // phase of x and the parity wait cannot match an older phase.
+  volatile int *issued = abort_flag + 1;
+  const int ld = sl.ld, T = sl.T;
   const double *W = a.W + sl.base;
-  const double *rcol = W + int64_t(sl.T) * TB;
+  const double *rcol = W + int64_t(T) * TB;
+  const double *X0 = a.inv + sl.inv;
   double *zc = a.zc + sl.zoff;
-  const int rr = tid & 63, quarter = tid >> 6;
-  for (int s = sl.T - 1; s >= 0; --s) {
-    double acc0[kMaxF], acc1[kMaxF];
-#pragma unroll
-    for (int f = 0; f < kMaxF; ++f) acc0[f] = acc1[f] = 0.0;
-    for (int t = s + 1 + warp; t < sl.T; t += 8) {
-      const double *tile = W + int64_t(t) * TB * ld + int64_t(s) * TB;
-      const double *zt = zc + int64_t(t) * TB * F;
-#pragma unroll 8
-      for (int c = 0; c < TB; ++c) {
-        const double l0 = tile[int64_t(c) * ld + lane], l1 = tile[int64_t(c) * ld + lane + 32];
-#pragma unroll
-        for (int f = 0; f < kMaxF; ++f)
-          if (f < F) {
-            const double z = zt[c * F + f];
-            acc0[f] = __fma_rn(l0, z, acc0[f]);
-            acc1[f] = __fma_rn(l1, z, acc1[f]);
-          }
+  if (tid == 0) {
+    for (int i = 0; i < kBkStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 8);
+    }
+    *abort_flag = 0;
+    *issued = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 8) {
+    // Producer: item g of the stream goes to stage g % kBkStages.
+    int g = 0;
+    bool ok = true;
+    for (int s = T - 1; s >= 0 && ok; --s) {
+      for (int t = s + 1; t <= T && ok; ++t, ++g) {  // t == T: X_s
+        const int st = g % kBkStages, u = g / kBkStages;
+        if (g >= kBkStages) {
+          if (lane == 0) ok = mbar_wait_abort(&empty[st], uint32_t((u - 1) & 1), abort_flag);
+          ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+          if (!ok) break;
+        }
+        uint8_t *dst = smem + size_t(st) * kBkTile;
+        if (lane == 0) mbar_expect_tx(&full[st], uint32_t(kBkTile));
+        __syncwarp();
+        if (t < T) {
+          const double *src = W + int64_t(t) * TB * ld + int64_t(s) * TB;
+          for (int r = lane; r < TB; r += 32)
+            bulk_g2s(dst + r * TB * 8, src + int64_t(r) * ld, TB * 8, &full[st]);
+        } else {
+          bulk_g2s(dst + lane * 1024, reinterpret_cast<const uint8_t *>(X0 + int64_t(s) * TB * TB) +
+                                          lane * 1024, 1024, &full[st]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          *issued = g + 1;
+        }
       }
     }
-#pragma unroll
-    for (int f = 0; f < kMaxF; ++f) {
-      part[warp][lane][f] = acc0[f];
-      part[warp][lane + 32][f] = acc1[f];
+    if (!ok && lane == 0) {
+      *abort_flag = 1;
+      atomicOr(&a.status[sl.k], 8);
     }
-    __syncthreads();
-    for (int e = tid; e < TB * F; e += 256) {
-      const int r = e / F, f = e % F;
-      double sum = 0.0;
+    // Wait (bounded) for every issued copy: the latest item of each stage.
+    if (lane == 0)
+      for (int st = 0; st < kBkStages && st < g; ++st) {
+        const int last = st + kBkStages * ((g - 1 - st) / kBkStages);
+        mbar_wait(&full[st], uint32_t((last / kBkStages) & 1));
+      }
+  } else {
+    int g = 0;
+    const int rr = tid & 63, quarter = tid >> 6;
+    for (int s = T - 1; s >= 0; --s) {
+      const int nt = T - 1 - s;
+      double acc0[kMaxF], acc1[kMaxF];
 #pragma unroll
-      for (int w = 0; w < 8; ++w) sum += part[w][r][f];
-      accs[r][f] = rcol[int64_t(s * TB + r) * ld + f] - sum;
-    }
-    __syncthreads();
-    // z_s[rr][f] = sum_{c >= rr} X_s[c][rr] acc_s[c][f]; quarters of c, then summed.
-    const double *xs = a.inv + sl.inv + int64_t(s) * TB * TB;
-    double zp[kMaxF];
+      for (int f = 0; f < kMaxF; ++f) acc0[f] = acc1[f] = 0.0;
+      for (int k = warp; k < nt; k += 8) {
+        const int gi = g + k, st = gi % kBkStages;
+        bool ok = !*abort_flag;
+        if (ok) ok = bk_wait_item(issued, abort_flag, full, gi);
+        if (!ok) {
+          *abort_flag = 1;
+          continue;
+        }
+        const double *tile = stage0 + size_t(st) * TB * TB;
+        const double *zt = zc + int64_t(s + 1 + k) * TB * F;
+#pragma unroll 8
+        for (int c = 0; c < TB; ++c) {
+          const double l0 = tile[c * TB + lane], l1 = tile[c * TB + lane + 32];
 #pragma unroll
-    for (int f = 0; f < kMaxF; ++f) zp[f] = 0.0;
-#pragma unroll 4
-    for (int c = quarter; c < TB; c += 4) {
-      if (c < rr) continue;
-      const double x = xs[c * TB + rr];
+          for (int f = 0; f < kMaxF; ++f)
+            if (f < F) {
+              const double z = zt[c * F + f];
+              acc0[f] = __fma_rn(l0, z, acc0[f]);
+              acc1[f] = __fma_rn(l1, z, acc1[f]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cnt(&empty[st], 8);
+      }
+      g += nt;
 #pragma unroll
       for (int f = 0; f < kMaxF; ++f)
-        if (f < F) zp[f] = __fma_rn(x, accs[c][f], zp[f]);
-    }
+        if (f < F) {
+          part[(warp * TB + lane) * F + f] = acc0[f];
+          part[(warp * TB + lane + 32) * F + f] = acc1[f];
+        }
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      for (int e = tid; e < TB * F; e += 256) {
+        const int r = e / F, f = e % F;
+        double sum = 0.0;
 #pragma unroll
-    for (int f = 0; f < kMaxF; ++f) part[quarter][rr][f] = zp[f];
-    __syncthreads();
-    for (int e = tid; e < TB * F; e += 256) {
-      const int r = e / F, f = e % F;
-      const double z = part[0][r][f] + part[1][r][f] + part[2][r][f] + part[3][r][f];
-      const int j = s * TB + r;
-      zc[int64_t(j) * F + f] = z;
-      if (a.alpha_c != nullptr && j < sl.n) a.alpha_c[(a.soff[sl.k] + j) * F + f] = z;
+        for (int w = 0; w < 8; ++w) sum += part[(w * TB + r) * F + f];
+        accs[r * F + f] = rcol[int64_t(s * TB + r) * ld + f] - sum;
+      }
+      // X_s: every consumer warp reads it, each releases one of 8 arrivals.
+      const int st = g % kBkStages;
+      bool okx = !*abort_flag;
+      if (okx) okx = bk_wait_item(issued, abort_flag, full, g);
+      if (!okx) *abort_flag = 1;
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      // z_s[rr][f] = sum_{c >= rr} X_s[c][rr] acc_s[c][f]; quarters of c, then summed.
+      const double *xs = stage0 + size_t(st) * TB * TB;
+      double zp[kMaxF];
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f) zp[f] = 0.0;
+      if (okx) {
+#pragma unroll 4
+        for (int c = quarter; c < TB; c += 4) {
+          if (c < rr) continue;
+          const double x = xs[c * TB + rr];
+#pragma unroll
+          for (int f = 0; f < kMaxF; ++f)
+            if (f < F) zp[f] = __fma_rn(x, accs[c * F + f], zp[f]);
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && okx) mbar_arrive_cnt(&empty[st], 1);
+      g += 1;
+#pragma unroll
+      for (int f = 0; f < kMaxF; ++f)
+        if (f < F) part[(quarter * TB + rr) * F + f] = zp[f];
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      for (int e = tid; e < TB * F; e += 256) {
+        const int r = e / F, f = e % F;
+        const double z = part[(0 * TB + r) * F + f] + part[(1 * TB + r) * F + f] +
+                         part[(2 * TB + r) * F + f] + part[(3 * TB + r) * F + f];
+        const int j = s * TB + r;
+        zc[int64_t(j) * F + f] = z;
+        if (a.alpha_c != nullptr && j < sl.n) a.alpha_c[(a.soff[sl.k] + j) * F + f] = z;
+      }
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
     }
-    __syncthreads();
+    if (tid == 0 && *abort_flag) atomicOr(&a.status[sl.k], 8);
   }
+  __syncthreads();
 }
 
 // local = E alpha + V beta for the targets of one slot (warp per target).
@@ -1018,6 +1160,8 @@ void chol_set_smem_attributes() {
                                int(kOzSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
+  PB_CUDA(cudaFuncSetAttribute(k_chol_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(chol_back_smem(kMaxF))));
   done = true;
 }
 
@@ -1079,7 +1223,7 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
 
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st) {
-  k_chol_back<<<ns, 256, 0, st>>>(a, ds);
+  k_chol_back<<<ns, 288, chol_back_smem(a.F), st>>>(a, ds);
   note_launch();
   if (!adjoint) {
     k_chol_eval<<<ns, 256, 0, st>>>(a, ds);

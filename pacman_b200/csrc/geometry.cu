@@ -614,12 +614,15 @@ __device__ __forceinline__ int64_t find_sorted(const int *a, int64_t n, int v) {
   return (lo < n && a[lo] == v) ? lo : -1;
 }
 
-__global__ void k_pu_gather(int64_t M, const double4 *__restrict__ tgt, GridView cg,
+__global__ void k_pu_gather(int64_t M, const int *__restrict__ tlist,
+                            const double4 *__restrict__ tgt, GridView cg,
                             const double4 *__restrict__ centers, double r, double rinv,
                             const int64_t *__restrict__ toff, const int *__restrict__ tidx,
                             const double *__restrict__ local, int F, double *out) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < M;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  // M targets: all (tlist null) or those of a shard's list.
+  for (int64_t it = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; it < M;
+       it += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = tlist ? tlist[it] : it;
     const double4 y = tgt[t];
     int ids[kMaxPatchesPerTarget];
     double ws[kMaxPatchesPerTarget];
@@ -909,14 +912,17 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
 
 void pu_gather(Plan &p, const double *local, int F, double *out_dev) {
   if (p.m == 0) return;
-  if (p.K == 0) {
+  const bool sharded = p.m_owned >= 0;
+  if (p.K == 0 || sharded)  // a shard writes its own targets only: zeros elsewhere
     PB_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double) * p.m * F, p.stream));
-    return;
-  }
+  if (p.K == 0) return;
+  const int64_t M = sharded ? p.m_owned : p.m;
+  if (M == 0) return;
   const double r = p.radius;
-  k_pu_gather<<<grid_for(p.m, 128, 148 * 64), 128, 0, p.stream>>>(
-      p.m, p.tgt4.as<double4>(), p.cgrid.view, p.centers.as<double4>(), r, 1.0 / r,
-      p.toff.as<int64_t>(), p.tidx.as<int>(), local, F, out_dev);
+  k_pu_gather<<<grid_for(M, 128, 148 * 64), 128, 0, p.stream>>>(
+      M, sharded ? p.tlist.as<int>() : nullptr, p.tgt4.as<double4>(), p.cgrid.view,
+      p.centers.as<double4>(), r, 1.0 / r, p.toff.as<int64_t>(), p.tidx.as<int>(), local, F,
+      out_dev);
   note_launch();
   PB_CUDA(cudaGetLastError());
 }

@@ -130,6 +130,11 @@ struct Plan {
   DevMem beta;               // K x 4*8 polynomial coefficients
   DevMem act;                // K x 3 active axes
   DevMem src_t_off, src_t_pos;  // sources -> (patch, slot) transpose of the membership lists
+  // Target shard (pacman_b200_plan_shard): the owned targets ascending, and
+  // their count; m_owned < 0 for an unsharded plan.
+  int shard_rank = 0, shard_world = 1;
+  int64_t m_owned = -1;
+  DevMem tlist;
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
   AuxStreams aux;
@@ -168,6 +173,8 @@ inline void note_launch(int k = 1) { launch_counter() += k; }
 // geometry.cu
 void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev);
 void pu_gather(Plan &p, const double *local, int F, double *out_dev);
+// Restricts the plan to target shard `rank` of `world` (shard.cu).
+void shard_plan(Plan &p, int rank, int world);
 
 // solve.cu
 struct SolveReport {

@@ -561,6 +561,14 @@ void solve_adjoint(Plan &p, int basis, int F, const double *h, double *g_out, So
   ex.h = h;
   ex.g_out = g_out;
   solve_big(p, basis, nullptr, F, false, big, nullptr, p.status.as<int>(), rep, ex);
+  // The adjoint has no second path: a pipeline wait that gave up is an error.
+  std::vector<int> stat(K);
+  PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
+  PB_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < K; ++k)
+    if (stat[k] & kStatusTimeout)
+      throw Error{PACMAN_B200_ERR_CUDA, "adjoint: a pipeline wait timed out in patch " +
+                                            std::to_string(k)};
 }
 
 }  // namespace pacman_b200

@@ -283,6 +283,25 @@ class Plan:
                                                                idx.ctypes.data))
         return off, idx[:nnz]
 
+    def shard(self, rank: int, world: int) -> "Plan":
+        """Keeps target shard ``rank`` of ``world`` (one process per GPU, each
+        with the same plan): executes then solve only the patches the shard's
+        targets need and return their values, bit-identical to the unsharded
+        transfer, with zeros at the other targets; the sum over the ranks is
+        the whole result.  See ``pacman_b200.distributed``."""
+        _lib.raise_for(self._lib.pacman_b200_plan_shard(self._h, int(rank), int(world)),
+                       "pacman.rbf.Plan.shard")
+        return self
+
+    def owned_targets(self) -> np.ndarray:
+        """Indices (ascending) of the targets of this plan's shard."""
+        cnt = ctypes.c_int64()
+        _lib.raise_for(self._lib.pacman_b200_plan_owned_targets(self._h, ctypes.byref(cnt), None))
+        out = np.zeros(max(cnt.value, 1), dtype=np.int32)
+        _lib.raise_for(self._lib.pacman_b200_plan_owned_targets(self._h, ctypes.byref(cnt),
+                                                                out.ctypes.data))
+        return out[: cnt.value]
+
     def local_values(self) -> np.ndarray:
         inf = self.info()
         out = np.zeros((max(inf["tgt_nnz"], 1), self.F or 1), dtype=np.float64)
