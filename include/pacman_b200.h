@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PACMAN_B200_ABI_VERSION 2
+#define PACMAN_B200_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PACMAN_B200_API __attribute__((visibility("default")))
@@ -92,6 +92,9 @@ typedef struct pacman_b200_stats {
   double ms_update;
   double update_flops;
   int64_t update_launches;
+  /* Patches solved from factorisations kept by an earlier execute
+   * (PACMAN_B200_KEEP_FACTORS). */
+  int64_t factors_reused;
 } pacman_b200_stats;
 
 /* Fills the reference's defaults (50, 0.15, 0.1, FP64, current device). */
@@ -165,6 +168,18 @@ PACMAN_B200_API void pacman_b200_plan_destroy(pacman_b200_plan *plan);
 /* Times every launch of the dominant kernel with CUDA events on its stream
  * (one slot group, no concurrent groups) and reports it in the stats. */
 #define PACMAN_B200_TIME_KERNELS 2u
+/* Reusable factorisations (precision PACMAN_B200_MIXED; no counterpart in
+ * the reference, which refactors every patch matrix on every call).  The
+ * patch matrices depend only on the geometry and the basis, so a coupling
+ * loop that transfers new values over fixed point sets factors them once:
+ * the first execute with this flag factors every patch and keeps the
+ * factors in the plan (device memory: about n^2 doubles per patch, n^2 / 2
+ * rounded up to 64 x 64 tiles for the large ones); later executes with the
+ * flag and the same basis run only the polynomial block, the triangular
+ * solves and the evaluation.  Another basis refactors and replaces them; an
+ * execute without the flag leaves them untouched; pacman_b200_plan_shard
+ * drops them.  Precision PACMAN_B200_FP64 keeps nothing. */
+#define PACMAN_B200_KEEP_FACTORS 4u
 PACMAN_B200_API int pacman_b200_plan_execute_ex(pacman_b200_plan *plan, int32_t rbf_function,
                                                 const double *source_values, int32_t n_fields,
                                                 double *target_values, uint32_t flags,

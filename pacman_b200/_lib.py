@@ -25,6 +25,7 @@ FP64 = 0
 MIXED = 1
 SAVE_FOR_ADJOINT = 1
 TIME_KERNELS = 2
+KEEP_FACTORS = 4
 
 _lock = threading.Lock()
 _lib = None
@@ -62,6 +63,7 @@ class Stats(ctypes.Structure):
         ("ms_update", ctypes.c_double),
         ("update_flops", ctypes.c_double),
         ("update_launches", ctypes.c_int64),
+        ("factors_reused", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:

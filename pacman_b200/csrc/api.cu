@@ -239,7 +239,8 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
         p.local.alloc(sizeof(double) * size_t(std::max<int64_t>(p.tnnz, 1)) * F, st);
         rep.time_kernels = (flags & PACMAN_B200_TIME_KERNELS) != 0;
         solve_patches(p, basis, v.ptr, F, p.opts.precision, p.local.as<double>(), rep,
-                      (flags & PACMAN_B200_SAVE_FOR_ADJOINT) != 0);
+                      (flags & PACMAN_B200_SAVE_FOR_ADJOINT) != 0,
+                      (flags & PACMAN_B200_KEEP_FACTORS) != 0);
         PB_CUDA(cudaEventRecord(e1, st));
         pu_gather(p, p.local.as<double>(), F, o);
       }
@@ -282,6 +283,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       stats->ms_update = rep.ms_update;
       stats->update_flops = rep.update_flops;
       stats->update_launches = rep.update_launches;
+      stats->factors_reused = rep.factors_reused;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -685,15 +685,17 @@ static void set_smem_attributes() {
 // launches are queued on p.stream without host synchronisation; the
 // workspace of each wave is released stream-ordered after its kernels, so the
 // next wave reuses it.
+void destroy_factor_cache(FactorCache *c) { delete c; }
+
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
-               const BigExtra &extra) {
+               const BigExtra &extra, FactorCache *keep) {
   if (patches.empty()) return;
   cudaStream_t st = p.stream;
   set_smem_attributes();
   size_t free_b = 0, total_b = 0;
   PB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  const size_t budget = std::max<size_t>(size_t(1) << 30, size_t(double(free_b) * 0.6)) / 8;
+  size_t budget = std::max<size_t>(size_t(1) << 30, size_t(double(free_b) * 0.6)) / 8;
   // Largest patches first: the slots active at step s are then a prefix.
   std::vector<int> order(patches);
   std::stable_sort(order.begin(), order.end(),
@@ -745,9 +747,16 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     a.oz_mul = 128.0 / sigma;
     a.oz_sig2 = sigma * sigma;
   }
+  if (lu || adjoint) keep = nullptr;  // only the mixed forward keeps its factors
   HostArena &arena = HostArena::get();
   size_t pos = 0;
   while (pos < order.size()) {
+    if (keep && pos > 0) {
+      // Kept waves stay allocated: size the next one by what is left.
+      PB_CUDA(cudaStreamSynchronize(st));
+      PB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      budget = std::max<size_t>(size_t(1) << 28, size_t(double(free_b) * 0.6)) / 8;
+    }
     // One wave: as many patches as fit the workspace budget.
     std::vector<BigSlot> slots;
     size_t tot = 0;
@@ -766,7 +775,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       q.inv = lu ? int64_t(slots.size()) * 2 * TB * TB : tot_inv;
       q.q = int(slots.size());
       q.zoff = tot_z;
-      tot_z += int64_t(q.T) * TB * F;
+      // Kept factors serve later executes with any field count: room for kMaxF.
+      tot_z += int64_t(q.T) * TB * (keep ? kMaxF : F);
       q.sli = tot_sl;
       if (oz) tot_sl += int64_t(oz_slot_bytes(q.T));
       tot_inv += int64_t(q.T) * TB * TB;
@@ -900,6 +910,21 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
         PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[g], 0));
       }
       PB_CUDA(cudaGetLastError());
+      if (keep) {
+        CholWaveCache w;
+        w.W = std::move(dW);
+        w.small = std::move(dsmall);
+        w.inv = a.inv;
+        w.beta = a.beta;
+        w.act = a.act;
+        w.red = a.red_out;
+        w.ns = ns;
+        for (const BigSlot &q : slots) w.sum_T += q.T;
+        w.gs = std::move(gs);
+        w.gmem = std::move(gmem);
+        w.gds = std::move(gds);
+        keep->waves.push_back(std::move(w));
+      }
       continue;
     }
     k_assemble<<<pre_asm[ns], 256, 0, st>>>(a, ds, dpre_asm, ns, 1);
@@ -925,6 +950,68 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       note_launch();
     }
     PB_CUDA(cudaGetLastError());
+  }
+}
+
+// Large patches from kept factorisations: per slot group, the polynomial
+// block and residual column (k_big_poly), the forward sweep from the kept
+// tiles (k_chol_fwd), the backward sweep and the evaluation.
+void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, int F,
+                      double *local, int *status, SolveReport &rep, const BigExtra &extra) {
+  if (c.waves.empty()) return;
+  cudaStream_t st = p.stream;
+  chol_set_smem_attributes();
+  BigArgs a{};
+  a.src = p.src4.as<double4>();
+  a.tgt = p.tgt4.as<double4>();
+  a.vals = vals;
+  a.soff = p.soff.as<int64_t>();
+  a.sidx = p.sidx.as<int>();
+  a.toff = p.toff.as<int64_t>();
+  a.tidx = p.tidx.as<int>();
+  a.centers = p.centers.as<double4>();
+  a.status = status;
+  a.local = local;
+  a.rinv = 1.0 / p.opts.support_radius;
+  a.F = F;
+  a.dim = p.dim;
+  a.basis = basis;
+  a.mode = extra.mode;
+  a.alpha_out = extra.alpha_out;
+  a.beta_out = extra.beta_out;
+  a.act_out = extra.act_out;
+  DevMem dalpha;
+  if (extra.alpha_out != nullptr) {
+    a.alpha_c = extra.alpha_out;
+  } else {
+    dalpha.alloc(sizeof(double) * size_t(std::max<int64_t>(p.snnz, 1)) * size_t(F), st);
+    a.alpha_c = dalpha.as<double>();
+  }
+  p.aux.make();
+  for (CholWaveCache &w : c.waves) {
+    DevMem dzc;
+    dzc.alloc(sizeof(double) * size_t(w.sum_T) * TB * kMaxF, st);  // slot offsets for kMaxF
+    a.zc = dzc.as<double>();
+    a.W = w.W.as<double>();
+    a.inv = w.inv;
+    a.beta = w.beta;
+    a.act = w.act;
+    a.red_out = w.red;
+    a.slices = nullptr;
+    PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN], st));
+    for (size_t g = 0; g < w.gs.size(); ++g) {
+      cudaStream_t sg = p.aux.s[g];
+      const int ng = int(w.gs[g].size());
+      PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
+      k_big_poly<<<ng, 256, 0, sg>>>(a, w.gds[g]);
+      note_launch();
+      chol_launch_forward(a, w.gds[g], ng, sg);
+      chol_launch_finish(a, w.gds[g], ng, false, sg);
+      PB_CUDA(cudaEventRecord(p.aux.ev[g], sg));
+      PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[g], 0));
+    }
+    PB_CUDA(cudaGetLastError());
+    rep.factors_reused += w.ns;
   }
 }
 

@@ -187,6 +187,39 @@ size_t oz_slot_bytes(int T);
 void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<BigSlot> &hs,
                        const CholPlan &cp, const int *dpre, cudaStream_t st, SolveReport &rep,
                        cudaEvent_t tail_event);
+// Factorisations kept in a plan by an execute with PACMAN_B200_KEEP_FACTORS
+// (precision "mixed"): later executes with the same basis run only the
+// polynomial block, the triangular solves and the evaluation.
+struct CholWaveCache {             // one wave of the large-patch engine
+  DevMem W;                        // L tiles; residual column tile (F <= 8 columns)
+  DevMem small;                    // tile inverses, beta, act, slot table
+  double *inv = nullptr, *beta = nullptr, *red = nullptr;
+  int *act = nullptr;
+  int ns = 0;
+  int64_t sum_T = 0;               // zc holds sum_T * TB * kMaxF doubles (slot offsets)
+  std::vector<std::vector<BigSlot>> gs;  // slot groups, one stream each
+  std::vector<DevMem> gmem;        // their device slot tables
+  std::vector<BigSlot *> gds;
+};
+struct SmallRange {                // one launch of the register kernel
+  size_t first = 0;                // offset into the cached patch list
+  int count = 0, nmax = 0;
+  size_t fac_off = 0;              // offset (doubles) of its factors
+};
+struct FactorCache {
+  int basis = -1;
+  std::vector<CholWaveCache> waves;
+  DevMem small_list;               // patch ids of the small launches
+  DevMem small_fac;                // their L^{-1} blocks and pivots
+  std::vector<SmallRange> ranges;
+  std::vector<int> redo_small, redo_big;  // re-solved by the FP64 LU every execute
+  int64_t patches = 0;
+};
+// Bytes of the kept factors of one register-kernel patch of size class N.
+inline size_t small_fac_doubles(int N) { return size_t(N) * N + N; }
+
+// Forward sweep L y = r from kept factors (an execute that reuses them).
+void chol_launch_forward(const BigArgs &a, const BigSlot *ds, int ns, cudaStream_t st);
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st);
 

@@ -1079,6 +1079,157 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
   __syncthreads();
 }
 
+// Forward sweep L y = r of one slot from kept factors (CTA per slot), for
+// an execute that reuses the factorisation: y_s = X_s (r_s - sum_{t<s}
+// L[s, t] y_t), tile row by tile row from the first, with the tile inverses
+// X_s of the factorisation.  r is the residual column (first F columns of
+// column tile T) and is overwritten with y, as the factorising steps leave
+// it.  Warp 8 streams the tiles L[s, t], t < s (64 row copies of 512 bytes),
+// then X_s, through the same ring as k_chol_back; every consumer warp reads
+// every tile: warp w owns rows 8w .. 8w + 7 and its lanes the columns c and
+// c + 32, so the partial sums stay in registers until the level ends.
+__global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *__restrict__ slots) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const BigSlot sl = slots[blockIdx.x];
+  const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double *stage0 = reinterpret_cast<double *>(smem);
+  double *accs = reinterpret_cast<double *>(smem + size_t(kBkStages) * kBkTile);  // [TB][F]
+  uint64_t *full = reinterpret_cast<uint64_t *>(accs + 9 * TB * F);
+  uint64_t *empty = full + kBkStages;
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kBkStages);
+  volatile int *issued = abort_flag + 1;  // as in k_chol_back
+  const int ld = sl.ld, T = sl.T;
+  const double *W = a.W + sl.base;
+  double *rcol = a.W + sl.base + int64_t(T) * TB;
+  const double *X0 = a.inv + sl.inv;
+  if (tid == 0) {
+    for (int i = 0; i < kBkStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 8);
+    }
+    *abort_flag = 0;
+    *issued = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 8) {
+    int g = 0;
+    bool ok = true;
+    for (int s = 0; s < T && ok; ++s) {
+      for (int t = 0; t <= s && ok; ++t, ++g) {  // t == s: X_s
+        const int st = g % kBkStages, u = g / kBkStages;
+        if (g >= kBkStages) {
+          if (lane == 0) ok = mbar_wait_abort(&empty[st], uint32_t((u - 1) & 1), abort_flag);
+          ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+          if (!ok) break;
+        }
+        uint8_t *dst = smem + size_t(st) * kBkTile;
+        if (lane == 0) mbar_expect_tx(&full[st], uint32_t(kBkTile));
+        __syncwarp();
+        if (t < s) {
+          const double *src = W + int64_t(s) * TB * ld + int64_t(t) * TB;
+          for (int r = lane; r < TB; r += 32)
+            bulk_g2s(dst + r * TB * 8, src + int64_t(r) * ld, TB * 8, &full[st]);
+        } else {
+          bulk_g2s(dst + lane * 1024, reinterpret_cast<const uint8_t *>(X0 + int64_t(s) * TB * TB) +
+                                          lane * 1024, 1024, &full[st]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          *issued = g + 1;
+        }
+      }
+    }
+    if (!ok && lane == 0) {
+      *abort_flag = 1;
+      atomicOr(&a.status[sl.k], 8);
+    }
+    if (lane == 0)
+      for (int st = 0; st < kBkStages && st < g; ++st) {
+        const int last = st + kBkStages * ((g - 1 - st) / kBkStages);
+        mbar_wait(&full[st], uint32_t((last / kBkStages) & 1));
+      }
+  } else {
+    int g = 0;
+    const int r0 = 8 * warp;
+    for (int s = 0; s < T; ++s) {
+      double part[8][kMaxF];
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int f = 0; f < kMaxF; ++f) part[r][f] = 0.0;
+      for (int t = 0; t < s; ++t, ++g) {
+        bool ok = !*abort_flag;
+        if (ok) ok = bk_wait_item(issued, abort_flag, full, g);
+        if (!ok) {
+          *abort_flag = 1;
+          continue;
+        }
+        const double *tile = stage0 + size_t(g % kBkStages) * TB * TB;
+        const double *yt = rcol + int64_t(t) * TB * ld;
+        double y0[kMaxF], y1[kMaxF];
+#pragma unroll
+        for (int f = 0; f < kMaxF; ++f) {
+          y0[f] = f < F ? yt[int64_t(lane) * ld + f] : 0.0;
+          y1[f] = f < F ? yt[int64_t(lane + 32) * ld + f] : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const double l0 = tile[(r0 + r) * TB + lane], l1 = tile[(r0 + r) * TB + lane + 32];
+#pragma unroll
+          for (int f = 0; f < kMaxF; ++f)
+            if (f < F) part[r][f] = __fma_rn(l1, y1[f], __fma_rn(l0, y0[f], part[r][f]));
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cnt(&empty[g % kBkStages], 1);
+      }
+      // acc_s = r_s - sum over the level, rows of this warp.
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int f = 0; f < kMaxF; ++f)
+          if (f < F) {
+            double v = part[r][f];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) accs[(r0 + r) * F + f] = rcol[int64_t(s * TB + r0 + r) * ld + f] - v;
+          }
+      bool okx = !*abort_flag;
+      if (okx) okx = bk_wait_item(issued, abort_flag, full, g);
+      if (!okx) *abort_flag = 1;
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+      // y_s[rr] = sum_{c <= rr} X_s[rr][c] acc_s[c], rows rr of this warp.
+      if (okx) {
+        const double *xs = stage0 + size_t(g % kBkStages) * TB * TB;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int rr = r0 + r;
+          const double x0 = lane <= rr ? xs[rr * TB + lane] : 0.0;
+          const double x1 = lane + 32 <= rr ? xs[rr * TB + lane + 32] : 0.0;
+#pragma unroll
+          for (int f = 0; f < kMaxF; ++f)
+            if (f < F) {
+              double v = __fma_rn(x1, accs[(lane + 32) * F + f], x0 * accs[lane * F + f]);
+              for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+              if (lane == 0) rcol[int64_t(s * TB + rr) * ld + f] = v;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cnt(&empty[g % kBkStages], 1);
+      }
+      g += 1;
+      asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    }
+    if (tid == 0 && *abort_flag) atomicOr(&a.status[sl.k], 8);
+  }
+  __syncthreads();
+}
+
+size_t chol_fwd_smem(int F) {
+  // stages, accs (with room), full/empty barriers, abort flag and issue counter
+  return size_t(kBkStages) * kBkTile + size_t(9 * TB * F) * 8 + 2 * kBkStages * 8 + 16;
+}
+
 // local = E alpha + V beta for the targets of one slot (warp per target).
 __global__ void __launch_bounds__(256) k_chol_eval(BigArgs a, const BigSlot *__restrict__ slots) {
   const BigSlot sl = slots[blockIdx.x];
@@ -1162,6 +1313,8 @@ void chol_set_smem_attributes() {
                                int(kDiagSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_chol_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(chol_back_smem(kMaxF))));
+  PB_CUDA(cudaFuncSetAttribute(k_chol_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(chol_fwd_smem(kMaxF))));
   done = true;
 }
 
@@ -1229,6 +1382,11 @@ void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoin
     k_chol_eval<<<ns, 256, 0, st>>>(a, ds);
     note_launch();
   }
+}
+
+void chol_launch_forward(const BigArgs &a, const BigSlot *ds, int ns, cudaStream_t st) {
+  k_chol_fwd<<<ns, 288, chol_fwd_smem(a.F), st>>>(a, ds);
+  note_launch();
 }
 
 size_t oz_slot_bytes(int T) { return size_t(T) * size_t(T - 1) / 2 * size_t(kOzTileBytes); }

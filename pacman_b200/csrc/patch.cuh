@@ -42,6 +42,11 @@ struct PatchArgs {
   int *act_out;           // forward: active axes, K x 3, or null
   const double *h;        // adjoint: weighted upstream gradient per (patch, target)
   double *g_out;          // adjoint: result per (patch, source)
+  // Register kernel (small.cu): 0 factor, 1 factor and store the eliminated
+  // blocks at fac (N * N doubles per list entry), 2 load them instead of
+  // assembling and factoring.
+  double *fac;
+  int fac_mode;
 };
 
 // Register-resident Cholesky of the patches with n <= 64 (small.cu); the

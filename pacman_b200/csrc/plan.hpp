@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,21 @@ struct DevMem {
   DevMem() = default;
   DevMem(const DevMem &) = delete;
   DevMem &operator=(const DevMem &) = delete;
+  DevMem(DevMem &&o) noexcept : p(o.p), bytes(o.bytes), s(o.s) {
+    o.p = nullptr;
+    o.bytes = 0;
+  }
+  DevMem &operator=(DevMem &&o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      s = o.s;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
   ~DevMem() { release(); }
   void release() {
     if (p) cudaFreeAsync(p, s);
@@ -101,6 +117,14 @@ struct AuxStreams {
   }
 };
 
+// Factorisations kept by an execute with PACMAN_B200_KEEP_FACTORS (defined
+// in blocked.cuh; destroyed through destroy_factor_cache).
+struct FactorCache;
+void destroy_factor_cache(FactorCache *c);
+struct FactorCacheDeleter {
+  void operator()(FactorCache *c) const { destroy_factor_cache(c); }
+};
+
 struct Plan {
   int dim = 3;
   int64_t n = 0, m = 0;
@@ -138,6 +162,7 @@ struct Plan {
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
   AuxStreams aux;
+  std::unique_ptr<FactorCache, FactorCacheDeleter> fcache;  // kept factorisations, or null
 };
 
 // Pinned host staging for the small host-to-device uploads of one call.  A
@@ -187,9 +212,11 @@ struct SolveReport {
   cudaEvent_t tail_event = nullptr;
   double ms_update = 0.0, update_flops = 0.0;
   int64_t update_launches = 0;
+  int64_t factors_reused = 0;  // patches solved from kept factorisations
 };
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
-                   double *local_dev, SolveReport &rep, bool save_state = false);
+                   double *local_dev, SolveReport &rep, bool save_state = false,
+                   bool keep_factors = false);
 
 // Extra inputs / outputs of the blocked engine beyond the forward transfer.
 enum { kBigForward = 0, kBigForwardSave = 1, kBigAdjoint = 2 };

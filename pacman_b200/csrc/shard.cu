@@ -137,6 +137,7 @@ void shard_plan(Plan &p, int rank, int world) {
   cudaStream_t st = p.stream;
   const int64_t M = p.m;
   const int K = p.K;
+  p.fcache.reset();  // kept factors were laid out for the unsharded target lists
   p.shard_rank = rank;
   p.shard_world = world;
   if (M == 0) {

@@ -159,28 +159,44 @@ __global__ void __launch_bounds__(SmallCfg<N>::kThreads)
     return;
   }
 
-  // Assembly (TeamFillA, team_ops.hpp:35-52) and elimination in registers.
+  // Assembly (TeamFillA, team_ops.hpp:35-52) and elimination in registers,
+  // or the eliminated blocks of an earlier execute (fac_mode 2).
   const int n = S.n;
   const int bi = lt / C::kG, bs = lt % C::kG;
   const int bar = 1 + team;
+  double *facp = (a.fac_mode != 0 && live) ? a.fac + size_t(e) * N * N + size_t(lt) * 16 : nullptr;
   double v[4][4];
+  const bool load = a.fac_mode == 2;
+  if (load && facp) {
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = 4 * bi + r, s = 4 * bs + b;
-      double val = 0.0;
-      if (s <= i) {
-        if (i < n && s < n)
-          val = wendland<double>(
-              a.basis, __dsqrt_rn(sqdist3(S.x[i], S.y[i], S.z[i], S.x[s], S.y[s], S.z[s])), a.rinv);
-        else
-          val = (i == s) ? 1.0 : 0.0;
-      }
-      v[r][b] = val;
+    for (int r = 0; r < 4; ++r) {
+      const double2 lo = *reinterpret_cast<const double2 *>(facp + 4 * r);
+      const double2 hi = *reinterpret_cast<const double2 *>(facp + 4 * r + 2);
+      v[r][0] = lo.x;
+      v[r][1] = lo.y;
+      v[r][2] = hi.x;
+      v[r][3] = hi.y;
     }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int i = 4 * bi + r, s = 4 * bs + b;
+        double val = 0.0;
+        if (s <= i) {
+          if (!load && i < n && s < n)
+            val = wendland<double>(
+                a.basis, __dsqrt_rn(sqdist3(S.x[i], S.y[i], S.z[i], S.x[s], S.y[s], S.z[s])),
+                a.rinv);
+          else
+            val = (i == s) ? 1.0 : 0.0;
+        }
+        v[r][b] = val;
+      }
+  }
   bool bad = false;
-  for (int p = 0; p < n; ++p) {
+  for (int p = 0; p < (load ? 0 : n); ++p) {
     double *c = S.cv[p & 1];
     const int pb = p >> 2, pr = p & 3;
     if (bi == pb) {  // row p: L^{-1}[p][s] for s < p, the pivot at s = p
@@ -224,6 +240,13 @@ __global__ void __launch_bounds__(SmallCfg<N>::kThreads)
           else if (s <= i) v[r][b] = __fma_rn(-mlt, cs[b], v[r][b]);
         }
       }
+    }
+  }
+  if (a.fac_mode == 1 && facp) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      *reinterpret_cast<double2 *>(facp + 4 * r) = make_double2(v[r][0], v[r][1]);
+      *reinterpret_cast<double2 *>(facp + 4 * r + 2) = make_double2(v[r][2], v[r][3]);
     }
   }
   if (bi == bs) {

@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <vector>
 
+#include "blocked.cuh"
 #include "patch.cuh"
 
 namespace pacman_b200 {
@@ -357,7 +358,7 @@ static void launch(int mode, const PatchArgs &a, const int *plist, int np, int u
 // shared memory follows the bucket's largest patch; patches too large for
 // shared memory use the global workspace.
 static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &patches,
-                     SolveReport &rep, cudaStream_t st) {
+                     SolveReport &rep, cudaStream_t st, FactorCache *keep = nullptr) {
   if (patches.empty()) return;
   for (int k : patches) {
     const double n = p.n_host[k], m = p.m_host[k];
@@ -393,12 +394,37 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
   DevMem list;
   list.alloc(sizeof(int) * host_list.size(), st);
   HostArena::get().upload(host_list.data(), host_list.size(), list.p, st);
+  if (keep) {
+    // Kept factors of the register kernel: N * N doubles per patch of the
+    // launch's size class, in launch order.
+    size_t tot = 0;
+    keep->ranges.clear();
+    for (auto &r : ranges) {
+      int nmax = 0;
+      for (size_t i = r.first; i < r.second; ++i) nmax = std::max(nmax, p.n_host[small[i]]);
+      if (mode != kChol || nmax > 64) continue;
+      SmallRange sr;
+      sr.first = r.first;
+      sr.count = int(r.second - r.first);
+      sr.nmax = nmax;
+      sr.fac_off = tot;
+      tot += size_t(sr.count) * small_fac_doubles(nmax <= 32 ? 32 : 64);
+      keep->ranges.push_back(sr);
+    }
+    keep->small_fac.alloc(sizeof(double) * std::max<size_t>(tot, 2), st);
+  }
+  size_t ri = 0;
   for (auto &r : ranges) {
     int nmax = 0;
     for (size_t i = r.first; i < r.second; ++i) nmax = std::max(nmax, p.n_host[small[i]]);
-    if (mode == kChol && nmax <= 64)
-      launch_small_chol(a, list.as<int>() + r.first, int(r.second - r.first), nmax, st);
-    else
+    if (mode == kChol && nmax <= 64) {
+      PatchArgs b = a;
+      if (keep) {
+        b.fac = keep->small_fac.as<double>() + keep->ranges[ri++].fac_off;
+        b.fac_mode = 1;
+      }
+      launch_small_chol(b, list.as<int>() + r.first, int(r.second - r.first), nmax, st);
+    } else
       launch(mode, a, list.as<int>() + r.first, int(r.second - r.first), 0,
              smem_bytes(nmax, F, true), st);
   }
@@ -422,11 +448,24 @@ static void run_list(Plan &p, PatchArgs a, int mode, const std::vector<int> &pat
     launch(mode, b, list.as<int>() + small.size(), int(big.size()), 1,
            smem_bytes(nmax, F, false), st);
   }
+  if (keep) keep->small_list = std::move(list);  // freed with the plan's cache
+}
+
+// The register-kernel patches from kept factors.
+static void run_small_cached(const FactorCache &c, PatchArgs a, cudaStream_t st) {
+  for (const SmallRange &r : c.ranges) {
+    PatchArgs b = a;
+    b.fac = const_cast<double *>(c.small_fac.as<double>()) + r.fac_off;
+    b.fac_mode = 2;
+    launch_small_chol(b, c.small_list.as<int>() + r.first, r.count, r.nmax, st);
+  }
 }
 
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
-               const BigExtra &extra);
+               const BigExtra &extra, FactorCache *keep = nullptr);
+void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, int F,
+                      double *local, int *status, SolveReport &rep, const BigExtra &extra);
 
 // Patches above this size use the blocked engine (blocked.cu): 64 for the
 // Cholesky path (the register kernels of small.cu take n <= 64), 128 for the
@@ -436,11 +475,23 @@ static int big_threshold(int mode) {
   return e ? std::max(1, std::atoi(e)) : (mode == kChol ? 64 : 128);
 }
 
-void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
-                   double *local_dev, SolveReport &rep, bool save) {
+static void solve_patches_impl(Plan &p, int basis, const double *vals_dev, int F, int precision,
+                               double *local_dev, SolveReport &rep, bool save, bool keep_factors) {
   cudaStream_t st = p.stream;
   const int K = p.K;
   if (K == 0) return;
+  const bool chol = precision != PACMAN_B200_FP64;
+  const FactorCache *cached =
+      (keep_factors && chol && p.fcache && p.fcache->basis == basis) ? p.fcache.get() : nullptr;
+  FactorCache *keep = nullptr;
+  if (keep_factors && !cached) {
+    p.fcache.reset();
+    if (chol) {
+      p.fcache.reset(new FactorCache());
+      p.fcache->basis = basis;
+      keep = p.fcache.get();
+    }
+  }
   p.status.alloc(sizeof(int) * K, st);
   PB_CUDA(cudaMemsetAsync(p.status.p, 0, sizeof(int) * K, st));
   BigExtra ex;
@@ -492,9 +543,19 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   cudaStream_t ss = p.aux.s[AuxStreams::kSmall];
   rep.tail_event = p.aux.ev[AuxStreams::kN + 1];
   PB_CUDA(cudaEventRecord(rep.tail_event, st));
-  solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep, ex);
-  PB_CUDA(cudaStreamWaitEvent(ss, rep.tail_event, 0));
-  run_list(p, a, mode, small, rep, ss);
+  if (cached) {
+    // Kept factors: the small patches start at once (no factorisation steps
+    // to wait for), the large ones run their sweeps on the group streams.
+    PB_CUDA(cudaStreamWaitEvent(ss, rep.tail_event, 0));
+    run_small_cached(*cached, a, ss);
+    solve_big_cached(p, *p.fcache, basis, vals_dev, F, local_dev, p.status.as<int>(), rep, ex);
+    for (const SmallRange &r : cached->ranges) rep.factors_reused += r.count;
+  } else {
+    solve_big(p, basis, vals_dev, F, mode == kLU, big, local_dev, p.status.as<int>(), rep, ex,
+              keep);
+    PB_CUDA(cudaStreamWaitEvent(ss, rep.tail_event, 0));
+    run_list(p, a, mode, small, rep, ss, keep);
+  }
   PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN + 2], ss));
   PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[AuxStreams::kN + 2], 0));
   rep.tail_event = nullptr;
@@ -506,11 +567,21 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   rep.ms_factor += ms;
   std::vector<int> redo_small, redo_big;
+  std::vector<char> redo_mark(cached ? K : 0, 0);
+  if (cached) {  // patches the factorising execute sent to the LU path
+    for (int k : cached->redo_small) redo_mark[k] = 1;
+    for (int k : cached->redo_big) redo_mark[k] = 2;
+  }
   for (int k = 0; k < K; ++k) {
     if (p.m_host[k] == 0) continue;
     if (stat[k] & kStatusDropped) rep.dropped++;
-    if (mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite | kStatusTimeout)))
+    if ((mode == kChol && (stat[k] & (kStatusBreakdown | kStatusNonFinite | kStatusTimeout))) ||
+        (cached && redo_mark[k]))
       (p.n_host[k] > nbig ? redo_big : redo_small).push_back(k);
+  }
+  if (keep) {
+    keep->redo_small = redo_small;
+    keep->redo_big = redo_big;
   }
   rep.patches_fp64 = int64_t(small.size() + big.size());
   if (!redo_small.empty() || !redo_big.empty()) {
@@ -525,6 +596,16 @@ void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precis
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
+}
+
+void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
+                   double *local_dev, SolveReport &rep, bool save, bool keep_factors) {
+  try {
+    solve_patches_impl(p, basis, vals_dev, F, precision, local_dev, rep, save, keep_factors);
+  } catch (...) {
+    if (keep_factors) p.fcache.reset();  // a half-built cache is never reused
+    throw;
+  }
 }
 
 // Per-patch adjoint solves: g (per patch, source) from h (per patch, target).

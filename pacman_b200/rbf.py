@@ -309,10 +309,14 @@ class Plan:
         return out[: inf["tgt_nnz"]]
 
     def execute(self, rbf_function, source_values, stats=None, save_for_adjoint=False,
-                time_kernels=False):
+                time_kernels=False, keep_factors=False):
         """Transfer of source_values ((N,) or (N, F)); with save_for_adjoint the
         per-patch coefficients are kept for ``adjoint``; with time_kernels the
-        dominant kernel's launches are timed with CUDA events into ``stats``."""
+        dominant kernel's launches are timed with CUDA events into ``stats``;
+        with keep_factors (precision "mixed") the patch factorisations are kept
+        by the first such execute and reused by the later ones with the same
+        basis (only the polynomial block, the triangular solves and the
+        evaluation run again)."""
         ptr, shape, kind, keep = _as_array(source_values)
         if shape[0] != self.n:
             raise ValueError("source values must have one row per source point")
@@ -320,7 +324,7 @@ class Plan:
         out_ptr, out = _empty_like_kind(kind, (self.m,) if len(shape) == 1 else (self.m, F), keep)
         st = _lib.Stats()
         flags = (_lib.SAVE_FOR_ADJOINT if save_for_adjoint else 0) | (
-            _lib.TIME_KERNELS if time_kernels else 0)
+            _lib.TIME_KERNELS if time_kernels else 0) | (_lib.KEEP_FACTORS if keep_factors else 0)
         rc = self._lib.pacman_b200_plan_execute_ex(self._h, int(rbf_function), ptr, F, out_ptr,
                                                    flags, ctypes.byref(st))
         _lib.raise_for(rc, "pacman.rbf.Plan.execute")
