@@ -901,6 +901,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
         }
         chol_launch_steps(a, gds[g], gs[g], gp[g], gpre[g], sg, rep,
                           g == 0 ? rep.tail_event : nullptr);
+        // Each group sweeps and evaluates as soon as its own steps end, so
+        // the sweeps overlap the other groups' last steps.
         chol_launch_finish(a, gds[g], int(gs[g].size()), adjoint, sg);
         if (adjoint) {
           k_big_adj_finish<<<int(gs[g].size()), 256, 0, sg>>>(a, gds[g]);
@@ -920,9 +922,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
         w.red = a.red_out;
         w.ns = ns;
         for (const BigSlot &q : slots) w.sum_T += q.T;
-        w.gs = std::move(gs);
-        w.gmem = std::move(gmem);
-        w.gds = std::move(gds);
+        w.ds = ds;
         keep->waves.push_back(std::move(w));
       }
       continue;
@@ -953,9 +953,10 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   }
 }
 
-// Large patches from kept factorisations: per slot group, the polynomial
-// block and residual column (k_big_poly), the forward sweep from the kept
-// tiles (k_chol_fwd), the backward sweep and the evaluation.
+// Large patches from kept factorisations, one launch each over all slots of
+// a wave (largest first): the polynomial block and residual column
+// (k_big_poly), the forward sweep from the kept tiles (k_chol_fwd), the
+// backward sweep and the evaluation.
 void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, int F,
                       double *local, int *status, SolveReport &rep, const BigExtra &extra) {
   if (c.waves.empty()) return;
@@ -998,18 +999,16 @@ void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, in
     a.act = w.act;
     a.red_out = w.red;
     a.slices = nullptr;
+    // On the high-priority stream, ahead of the small patches' kernel.
+    cudaStream_t hs = p.aux.s[0];
     PB_CUDA(cudaEventRecord(p.aux.ev[AuxStreams::kN], st));
-    for (size_t g = 0; g < w.gs.size(); ++g) {
-      cudaStream_t sg = p.aux.s[g];
-      const int ng = int(w.gs[g].size());
-      PB_CUDA(cudaStreamWaitEvent(sg, p.aux.ev[AuxStreams::kN], 0));
-      k_big_poly<<<ng, 256, 0, sg>>>(a, w.gds[g]);
-      note_launch();
-      chol_launch_forward(a, w.gds[g], ng, sg);
-      chol_launch_finish(a, w.gds[g], ng, false, sg);
-      PB_CUDA(cudaEventRecord(p.aux.ev[g], sg));
-      PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[g], 0));
-    }
+    PB_CUDA(cudaStreamWaitEvent(hs, p.aux.ev[AuxStreams::kN], 0));
+    k_big_poly<<<w.ns, 256, 0, hs>>>(a, w.ds);
+    note_launch();
+    chol_launch_forward(a, w.ds, w.ns, hs);
+    chol_launch_finish(a, w.ds, w.ns, false, hs);
+    PB_CUDA(cudaEventRecord(p.aux.ev[0], hs));
+    PB_CUDA(cudaStreamWaitEvent(st, p.aux.ev[0], 0));
     PB_CUDA(cudaGetLastError());
     rep.factors_reused += w.ns;
   }

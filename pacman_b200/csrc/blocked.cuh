@@ -192,14 +192,12 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
 // polynomial block, the triangular solves and the evaluation.
 struct CholWaveCache {             // one wave of the large-patch engine
   DevMem W;                        // L tiles; residual column tile (F <= 8 columns)
-  DevMem small;                    // tile inverses, beta, act, slot table
+  DevMem small;                    // tile inverses, beta, act, slot tables
   double *inv = nullptr, *beta = nullptr, *red = nullptr;
   int *act = nullptr;
   int ns = 0;
   int64_t sum_T = 0;               // zc holds sum_T * TB * kMaxF doubles (slot offsets)
-  std::vector<std::vector<BigSlot>> gs;  // slot groups, one stream each
-  std::vector<DevMem> gmem;        // their device slot tables
-  std::vector<BigSlot *> gds;
+  BigSlot *ds = nullptr;           // device slot table (in small), largest first
 };
 struct SmallRange {                // one launch of the register kernel
   size_t first = 0;                // offset into the cached patch list

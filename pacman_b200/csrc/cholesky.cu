@@ -864,21 +864,27 @@ __global__ void __launch_bounds__(kColThreads, 1)
 // from the last: z_s = X_s^T (y_s - sum_{t>s} L[t, s]^T z_t), with the tile
 // inverses X_s of the factorisation.  The sweep is a chain of T dependent
 // levels, so the time of a large slot is set by how fast its tiles reach the
-// SM: warp 8 streams them with bulk async copies, in sweep order and
+// SM: warp 8 streams them with 16-byte cp.async (one 512-byte row per
+// instruction, completion counted on an mbarrier), in sweep order and
 // independent of z, through a ring of kBkStages 32 KB stages (the tiles
-// L[t, s], t > s, as 64 row copies of 512 bytes, then X_s as one copy), up to
-// kBkStages tiles ahead of the arithmetic.  Warps 0..7 take the L tiles of a
+// L[t, s], t > s, then X_s), up to kBkStages tiles ahead of the arithmetic.
+// (Bulk copies of the 512-byte rows were slower: the per-request cost of the
+// bulk-copy engine capped one SM near 20 GB/s.)  Warps 0..7 take the L tiles of a
 // level in turn (lane: two columns r of the tile, all rows c), then meet to
 // finish z_s.  z goes to zc (per slot) and, in the forward, to alpha_c per
 // (patch, source).  Every wait is bounded; a time-out marks the patch
 // (status 8), the CTA keeps its barrier sequence, stops issuing copies and
 // waits for the copies it issued before it returns.
-constexpr int kBkStages = 5;
 constexpr int kBkTile = TB * TB * 8;  // bytes of one stage
+// Ring depth: 3 stages for one or two fields, two CTAs per SM (the many short
+// slots are latency-bound, and a second CTA hides it); 5 stages, one CTA per
+// SM, for more fields (registers).
+constexpr int bk_stages(int F) { return F <= 2 ? 3 : 5; }
 
 size_t chol_back_smem(int F) {
   // stages, part, accs, full/empty barriers, abort flag and issue counter
-  return size_t(kBkStages) * kBkTile + size_t(8 * TB * F + TB * F) * 8 + 2 * kBkStages * 8 + 16;
+  const int S = bk_stages(F);
+  return size_t(S) * kBkTile + size_t(8 * TB * F + TB * F) * 8 + 2 * S * 8 + 16;
 }
 
 __device__ __forceinline__ void mbar_arrive_cnt(uint64_t *b, uint32_t cnt) {
@@ -908,7 +914,20 @@ __device__ __forceinline__ bool mbar_wait_abort(uint64_t *b, uint32_t parity,
   return false;
 }
 
+// One 64 x 64 FP64 tile (rows ld doubles apart) into a pipeline stage by the
+// 32 lanes of a warp, 16-byte cp.async each (row r: the lane's 16 bytes, so
+// every instruction moves one 512-byte row); the stage's full barrier
+// (initialised to 32 arrivals) counts this lane once its copies have landed.
+__device__ __forceinline__ void warp_tile_g2s(double *dst, const double *src, int64_t ld,
+                                              int lane, uint64_t *full) {
+#pragma unroll 8
+  for (int r = 0; r < TB; ++r) cp_async16(dst + r * TB + 2 * lane, src + r * ld + 2 * lane);
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(saddr(full))
+               : "memory");
+}
+
 // Bounded wait until item x is issued, then for its data.
+template <int kBkStages>
 __device__ __forceinline__ bool bk_wait_item(volatile int *issued, volatile int *abort_flag,
                                              uint64_t *full, int x) {
   bool ok = false;
@@ -919,7 +938,9 @@ __device__ __forceinline__ bool bk_wait_item(volatile int *issued, volatile int 
   return ok && mbar_wait_abort(&full[x % kBkStages], uint32_t((x / kBkStages) & 1), abort_flag);
 }
 
-__global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
+template <int KF, int kBkStages>  // fields held in registers (F <= KF), ring depth
+__global__ void __launch_bounds__(288, kBkStages == 3 ? 2 : 1)
+    k_chol_back(BigArgs a, const BigSlot *__restrict__ slots) {
   extern __shared__ __align__(128) uint8_t smem[];
   const BigSlot sl = slots[blockIdx.x];
   const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -941,7 +962,7 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
   double *zc = a.zc + sl.zoff;
   if (tid == 0) {
     for (int i = 0; i < kBkStages; ++i) {
-      mbar_init(&full[i], 1);
+      mbar_init(&full[i], 32);  // one arrival per producer lane
       mbar_init(&empty[i], 8);
     }
     *abort_flag = 0;
@@ -961,17 +982,11 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
           ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
           if (!ok) break;
         }
-        uint8_t *dst = smem + size_t(st) * kBkTile;
-        if (lane == 0) mbar_expect_tx(&full[st], uint32_t(kBkTile));
-        __syncwarp();
-        if (t < T) {
-          const double *src = W + int64_t(t) * TB * ld + int64_t(s) * TB;
-          for (int r = lane; r < TB; r += 32)
-            bulk_g2s(dst + r * TB * 8, src + int64_t(r) * ld, TB * 8, &full[st]);
-        } else {
-          bulk_g2s(dst + lane * 1024, reinterpret_cast<const uint8_t *>(X0 + int64_t(s) * TB * TB) +
-                                          lane * 1024, 1024, &full[st]);
-        }
+        double *dst = reinterpret_cast<double *>(smem + size_t(st) * kBkTile);
+        if (t < T)
+          warp_tile_g2s(dst, W + int64_t(t) * TB * ld + int64_t(s) * TB, ld, lane, &full[st]);
+        else
+          warp_tile_g2s(dst, X0 + int64_t(s) * TB * TB, TB, lane, &full[st]);
         __syncwarp();
         if (lane == 0) {
           __threadfence_block();
@@ -989,31 +1004,58 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
         const int last = st + kBkStages * ((g - 1 - st) / kBkStages);
         mbar_wait(&full[st], uint32_t((last / kBkStages) & 1));
       }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   } else {
     int g = 0;
     const int rr = tid & 63, quarter = tid >> 6;
     for (int s = T - 1; s >= 0; --s) {
       const int nt = T - 1 - s;
-      double acc0[kMaxF], acc1[kMaxF];
+      double acc0[KF], acc1[KF];
 #pragma unroll
-      for (int f = 0; f < kMaxF; ++f) acc0[f] = acc1[f] = 0.0;
+      for (int f = 0; f < KF; ++f) acc0[f] = acc1[f] = 0.0;
+      // z_t of the warp's next tile, one coalesced load per lane and field
+      // (rows lane and lane + 32), issued before the wait for the tile; the
+      // rows c are then broadcast from the lanes by shuffles.
+      double zn0[KF], zn1[KF];
+      if (warp < nt) {
+        const double *zt = zc + int64_t(s + 1 + warp) * TB * F;
+#pragma unroll
+        for (int f = 0; f < KF; ++f) {
+          zn0[f] = f < F ? zt[lane * F + f] : 0.0;
+          zn1[f] = f < F ? zt[(lane + 32) * F + f] : 0.0;
+        }
+      }
       for (int k = warp; k < nt; k += 8) {
         const int gi = g + k, st = gi % kBkStages;
+        double z0[KF], z1[KF];
+#pragma unroll
+        for (int f = 0; f < KF; ++f) {
+          z0[f] = zn0[f];
+          z1[f] = zn1[f];
+        }
+        if (k + 8 < nt) {
+          const double *zt = zc + int64_t(s + 1 + k + 8) * TB * F;
+#pragma unroll
+          for (int f = 0; f < KF; ++f)
+            if (f < F) {
+              zn0[f] = zt[lane * F + f];
+              zn1[f] = zt[(lane + 32) * F + f];
+            }
+        }
         bool ok = !*abort_flag;
-        if (ok) ok = bk_wait_item(issued, abort_flag, full, gi);
+        if (ok) ok = bk_wait_item<kBkStages>(issued, abort_flag, full, gi);
         if (!ok) {
           *abort_flag = 1;
           continue;
         }
         const double *tile = stage0 + size_t(st) * TB * TB;
-        const double *zt = zc + int64_t(s + 1 + k) * TB * F;
 #pragma unroll 8
         for (int c = 0; c < TB; ++c) {
           const double l0 = tile[c * TB + lane], l1 = tile[c * TB + lane + 32];
 #pragma unroll
-          for (int f = 0; f < kMaxF; ++f)
+          for (int f = 0; f < KF; ++f)
             if (f < F) {
-              const double z = zt[c * F + f];
+              const double z = __shfl_sync(0xffffffffu, c < 32 ? z0[f] : z1[f], c & 31);
               acc0[f] = __fma_rn(l0, z, acc0[f]);
               acc1[f] = __fma_rn(l1, z, acc1[f]);
             }
@@ -1023,7 +1065,7 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
       }
       g += nt;
 #pragma unroll
-      for (int f = 0; f < kMaxF; ++f)
+      for (int f = 0; f < KF; ++f)
         if (f < F) {
           part[(warp * TB + lane) * F + f] = acc0[f];
           part[(warp * TB + lane + 32) * F + f] = acc1[f];
@@ -1039,21 +1081,21 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
       // X_s: every consumer warp reads it, each releases one of 8 arrivals.
       const int st = g % kBkStages;
       bool okx = !*abort_flag;
-      if (okx) okx = bk_wait_item(issued, abort_flag, full, g);
+      if (okx) okx = bk_wait_item<kBkStages>(issued, abort_flag, full, g);
       if (!okx) *abort_flag = 1;
       asm volatile("bar.sync 1, 256;\n" ::: "memory");
       // z_s[rr][f] = sum_{c >= rr} X_s[c][rr] acc_s[c][f]; quarters of c, then summed.
       const double *xs = stage0 + size_t(st) * TB * TB;
-      double zp[kMaxF];
+      double zp[KF];
 #pragma unroll
-      for (int f = 0; f < kMaxF; ++f) zp[f] = 0.0;
+      for (int f = 0; f < KF; ++f) zp[f] = 0.0;
       if (okx) {
 #pragma unroll 4
         for (int c = quarter; c < TB; c += 4) {
           if (c < rr) continue;
           const double x = xs[c * TB + rr];
 #pragma unroll
-          for (int f = 0; f < kMaxF; ++f)
+          for (int f = 0; f < KF; ++f)
             if (f < F) zp[f] = __fma_rn(x, accs[c * F + f], zp[f]);
         }
       }
@@ -1061,7 +1103,7 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
       if (lane == 0 && okx) mbar_arrive_cnt(&empty[st], 1);
       g += 1;
 #pragma unroll
-      for (int f = 0; f < kMaxF; ++f)
+      for (int f = 0; f < KF; ++f)
         if (f < F) part[(quarter * TB + rr) * F + f] = zp[f];
       asm volatile("bar.sync 1, 256;\n" ::: "memory");
       for (int e = tid; e < TB * F; e += 256) {
@@ -1084,11 +1126,13 @@ __global__ void __launch_bounds__(288, 1) k_chol_back(BigArgs a, const BigSlot *
 // L[s, t] y_t), tile row by tile row from the first, with the tile inverses
 // X_s of the factorisation.  r is the residual column (first F columns of
 // column tile T) and is overwritten with y, as the factorising steps leave
-// it.  Warp 8 streams the tiles L[s, t], t < s (64 row copies of 512 bytes),
-// then X_s, through the same ring as k_chol_back; every consumer warp reads
+// it.  Warp 8 streams the tiles L[s, t], t < s, then X_s, through the same
+// cp.async ring as k_chol_back; every consumer warp reads
 // every tile: warp w owns rows 8w .. 8w + 7 and its lanes the columns c and
 // c + 32, so the partial sums stay in registers until the level ends.
-__global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *__restrict__ slots) {
+template <int KF, int kBkStages>  // fields held in registers (F <= KF), ring depth
+__global__ void __launch_bounds__(288, kBkStages == 3 ? 2 : 1)
+    k_chol_fwd(BigArgs a, const BigSlot *__restrict__ slots) {
   extern __shared__ __align__(128) uint8_t smem[];
   const BigSlot sl = slots[blockIdx.x];
   const int F = a.F, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1104,7 +1148,7 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
   const double *X0 = a.inv + sl.inv;
   if (tid == 0) {
     for (int i = 0; i < kBkStages; ++i) {
-      mbar_init(&full[i], 1);
+      mbar_init(&full[i], 32);  // one arrival per producer lane
       mbar_init(&empty[i], 8);
     }
     *abort_flag = 0;
@@ -1123,17 +1167,11 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
           ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
           if (!ok) break;
         }
-        uint8_t *dst = smem + size_t(st) * kBkTile;
-        if (lane == 0) mbar_expect_tx(&full[st], uint32_t(kBkTile));
-        __syncwarp();
-        if (t < s) {
-          const double *src = W + int64_t(s) * TB * ld + int64_t(t) * TB;
-          for (int r = lane; r < TB; r += 32)
-            bulk_g2s(dst + r * TB * 8, src + int64_t(r) * ld, TB * 8, &full[st]);
-        } else {
-          bulk_g2s(dst + lane * 1024, reinterpret_cast<const uint8_t *>(X0 + int64_t(s) * TB * TB) +
-                                          lane * 1024, 1024, &full[st]);
-        }
+        double *dst = reinterpret_cast<double *>(smem + size_t(st) * kBkTile);
+        if (t < s)
+          warp_tile_g2s(dst, W + int64_t(s) * TB * ld + int64_t(t) * TB, ld, lane, &full[st]);
+        else
+          warp_tile_g2s(dst, X0 + int64_t(s) * TB * TB, TB, lane, &full[st]);
         __syncwarp();
         if (lane == 0) {
           __threadfence_block();
@@ -1150,35 +1188,51 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
         const int last = st + kBkStages * ((g - 1 - st) / kBkStages);
         mbar_wait(&full[st], uint32_t((last / kBkStages) & 1));
       }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   } else {
     int g = 0;
     const int r0 = 8 * warp;
     for (int s = 0; s < T; ++s) {
-      double part[8][kMaxF];
+      double part[8][KF];
 #pragma unroll
       for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int f = 0; f < kMaxF; ++f) part[r][f] = 0.0;
+        for (int f = 0; f < KF; ++f) part[r][f] = 0.0;
+      // y_t of the lane's columns, loaded one tile ahead of its use.
+      double yn0[KF], yn1[KF];
+#pragma unroll
+      for (int f = 0; f < KF; ++f) {
+        yn0[f] = (s > 0 && f < F) ? rcol[int64_t(lane) * ld + f] : 0.0;
+        yn1[f] = (s > 0 && f < F) ? rcol[int64_t(lane + 32) * ld + f] : 0.0;
+      }
       for (int t = 0; t < s; ++t, ++g) {
+        double y0[KF], y1[KF];
+#pragma unroll
+        for (int f = 0; f < KF; ++f) {
+          y0[f] = yn0[f];
+          y1[f] = yn1[f];
+        }
+        if (t + 1 < s) {
+          const double *yt = rcol + int64_t(t + 1) * TB * ld;
+#pragma unroll
+          for (int f = 0; f < KF; ++f)
+            if (f < F) {
+              yn0[f] = yt[int64_t(lane) * ld + f];
+              yn1[f] = yt[int64_t(lane + 32) * ld + f];
+            }
+        }
         bool ok = !*abort_flag;
-        if (ok) ok = bk_wait_item(issued, abort_flag, full, g);
+        if (ok) ok = bk_wait_item<kBkStages>(issued, abort_flag, full, g);
         if (!ok) {
           *abort_flag = 1;
           continue;
         }
         const double *tile = stage0 + size_t(g % kBkStages) * TB * TB;
-        const double *yt = rcol + int64_t(t) * TB * ld;
-        double y0[kMaxF], y1[kMaxF];
-#pragma unroll
-        for (int f = 0; f < kMaxF; ++f) {
-          y0[f] = f < F ? yt[int64_t(lane) * ld + f] : 0.0;
-          y1[f] = f < F ? yt[int64_t(lane + 32) * ld + f] : 0.0;
-        }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           const double l0 = tile[(r0 + r) * TB + lane], l1 = tile[(r0 + r) * TB + lane + 32];
 #pragma unroll
-          for (int f = 0; f < kMaxF; ++f)
+          for (int f = 0; f < KF; ++f)
             if (f < F) part[r][f] = __fma_rn(l1, y1[f], __fma_rn(l0, y0[f], part[r][f]));
         }
         __syncwarp();
@@ -1188,14 +1242,14 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
 #pragma unroll
       for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int f = 0; f < kMaxF; ++f)
+        for (int f = 0; f < KF; ++f)
           if (f < F) {
             double v = part[r][f];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if (lane == 0) accs[(r0 + r) * F + f] = rcol[int64_t(s * TB + r0 + r) * ld + f] - v;
           }
       bool okx = !*abort_flag;
-      if (okx) okx = bk_wait_item(issued, abort_flag, full, g);
+      if (okx) okx = bk_wait_item<kBkStages>(issued, abort_flag, full, g);
       if (!okx) *abort_flag = 1;
       asm volatile("bar.sync 1, 256;\n" ::: "memory");
       // y_s[rr] = sum_{c <= rr} X_s[rr][c] acc_s[c], rows rr of this warp.
@@ -1207,7 +1261,7 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
           const double x0 = lane <= rr ? xs[rr * TB + lane] : 0.0;
           const double x1 = lane + 32 <= rr ? xs[rr * TB + lane + 32] : 0.0;
 #pragma unroll
-          for (int f = 0; f < kMaxF; ++f)
+          for (int f = 0; f < KF; ++f)
             if (f < F) {
               double v = __fma_rn(x1, accs[(lane + 32) * F + f], x0 * accs[lane * F + f]);
               for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -1227,7 +1281,8 @@ __global__ void __launch_bounds__(288, 1) k_chol_fwd(BigArgs a, const BigSlot *_
 
 size_t chol_fwd_smem(int F) {
   // stages, accs (with room), full/empty barriers, abort flag and issue counter
-  return size_t(kBkStages) * kBkTile + size_t(9 * TB * F) * 8 + 2 * kBkStages * 8 + 16;
+  const int S = bk_stages(F);
+  return size_t(S) * kBkTile + size_t(9 * TB * F) * 8 + 2 * S * 8 + 16;
 }
 
 // local = E alpha + V beta for the targets of one slot (warp per target).
@@ -1311,10 +1366,20 @@ void chol_set_smem_attributes() {
                                int(kOzSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
-  PB_CUDA(cudaFuncSetAttribute(k_chol_back, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(chol_back_smem(kMaxF))));
-  PB_CUDA(cudaFuncSetAttribute(k_chol_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(chol_fwd_smem(kMaxF))));
+  {
+#define PB_SWEEP_ATTR(K, F)                                                                   \
+  PB_CUDA(cudaFuncSetAttribute(K<F, bk_stages(F)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               int(std::max(chol_back_smem(F), chol_fwd_smem(F)))))
+    PB_SWEEP_ATTR(k_chol_back, 1);
+    PB_SWEEP_ATTR(k_chol_back, 2);
+    PB_SWEEP_ATTR(k_chol_back, 4);
+    PB_SWEEP_ATTR(k_chol_back, kMaxF);
+    PB_SWEEP_ATTR(k_chol_fwd, 1);
+    PB_SWEEP_ATTR(k_chol_fwd, 2);
+    PB_SWEEP_ATTR(k_chol_fwd, 4);
+    PB_SWEEP_ATTR(k_chol_fwd, kMaxF);
+#undef PB_SWEEP_ATTR
+  }
   done = true;
 }
 
@@ -1376,7 +1441,11 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
 
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st) {
-  k_chol_back<<<ns, 288, chol_back_smem(a.F), st>>>(a, ds);
+  const size_t smem = chol_back_smem(a.F);
+  if (a.F == 1) k_chol_back<1, bk_stages(1)><<<ns, 288, smem, st>>>(a, ds);
+  else if (a.F <= 2) k_chol_back<2, bk_stages(2)><<<ns, 288, smem, st>>>(a, ds);
+  else if (a.F <= 4) k_chol_back<4, bk_stages(4)><<<ns, 288, smem, st>>>(a, ds);
+  else k_chol_back<kMaxF, bk_stages(kMaxF)><<<ns, 288, smem, st>>>(a, ds);
   note_launch();
   if (!adjoint) {
     k_chol_eval<<<ns, 256, 0, st>>>(a, ds);
@@ -1385,7 +1454,11 @@ void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoin
 }
 
 void chol_launch_forward(const BigArgs &a, const BigSlot *ds, int ns, cudaStream_t st) {
-  k_chol_fwd<<<ns, 288, chol_fwd_smem(a.F), st>>>(a, ds);
+  const size_t smem = chol_fwd_smem(a.F);
+  if (a.F == 1) k_chol_fwd<1, bk_stages(1)><<<ns, 288, smem, st>>>(a, ds);
+  else if (a.F <= 2) k_chol_fwd<2, bk_stages(2)><<<ns, 288, smem, st>>>(a, ds);
+  else if (a.F <= 4) k_chol_fwd<4, bk_stages(4)><<<ns, 288, smem, st>>>(a, ds);
+  else k_chol_fwd<kMaxF, bk_stages(kMaxF)><<<ns, 288, smem, st>>>(a, ds);
   note_launch();
 }
 

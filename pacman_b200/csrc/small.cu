@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(SmallCfg<N>::kThreads)
     }
     team_sync(bar, C::kTeam);
   }
-  if (a.alpha_out != nullptr) {
+  if (a.alpha_out != nullptr && live) {  // teams past the end of the list hold no patch
     for (int e2 = lt; e2 < n * F; e2 += C::kTeam) {
       const int j = e2 / F, f = e2 % F;
       a.alpha_out[(S.s0 + j) * F + f] = S.w[f][j];
