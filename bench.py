@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the many-uneven-transfers measurement (256 problems per call)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--kernels-only", action="store_true",
                     help="run warmup + steps transfers and exit (for ncu launch lists)")
@@ -392,6 +394,24 @@ def main():
             "factors_reused": rst.get("factors_reused"),
             "what": "Plan.execute(keep_factors=True) after a factorising execute: geometry "
                     "and patch factorisations kept, values new each step"}
+
+    # Many uneven transfers in one call: 256 independent problems (sources
+    # log-uniform in [1000, 50000], uniform in boxes of side 0.5-2, bases
+    # C0..C8, 1-4 fields), device-resident, through interpolate_batch.
+    if world == 1 and not args.no_batch and args.scale == 1.0:
+        probs = W.many_problems(count=256)
+        bP = [(3, q["basis"], torch.tensor(q["src"], device=dev),
+               torch.tensor(q["values"] if q["values"].shape[1] > 1 else q["values"][:, 0],
+                            device=dev),
+               torch.tensor(q["tgt"], device=dev)) for q in probs]
+        btot = sum(q["tgt"].shape[0] for q in probs)
+        batch = {"problems": len(probs), "targets": int(btot), "unit": UNIT}
+        for prec in ("mixed", "fp64"):
+            pacman.rbf.interpolate_batch(bP, precision=prec)
+            bt = timed(lambda: pacman.rbf.interpolate_batch(bP, precision=prec), 2)
+            bms = sum(bt) / len(bt)
+            batch[prec] = {"value": btot / (bms * 1e-3), "ms_per_call": bms}
+        extra["many_uneven_256"] = batch
 
     # Roofline of the dominant kernel, the step kernel of the large-patch
     # Cholesky: one extra transfer after the timed region with CUDA events
