@@ -217,6 +217,25 @@ PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, 
  * gives this shard's contribution to the source-value gradient and the
  * owned targets' coordinate gradients.  A plan is sharded once.
  */
+/*
+ * Finite-element transfer of the reference's PACMAN::fe_interpolate
+ * (src/interface.hpp:76-80, src/interface.cpp:89-121) for the method
+ * NEAREST_NEAREST (0xF0, src/common/types.hpp:29-37; FTNearest.hpp:27-56):
+ * target_values[t] = source_values[nearest source] (lowest index on ties), 0
+ * without sources; target_status[t] = 0 (OUTSIDE: the reference's
+ * NEAREST_NEAREST leaves the zero-initialised status as it is; may be NULL).
+ * The point-based method reads no connectivity, so none is passed.  Other
+ * methods return PACMAN_B200_ERR_INVALID.  Arrays may be host or device
+ * memory of opts->device; opts (device, stream) may be NULL.
+ */
+#define PACMAN_B200_FE_NEAREST_NEAREST 0xF0
+PACMAN_B200_API int pacman_b200_fe_interpolate(int32_t dim, int32_t method,
+                                               const double *source_points, int64_t n_source,
+                                               const double *source_values,
+                                               const double *target_points, int64_t n_target,
+                                               double *target_values, int32_t *target_status,
+                                               const pacman_b200_options *opts);
+
 PACMAN_B200_API int pacman_b200_plan_shard(pacman_b200_plan *plan, int32_t rank, int32_t world);
 
 /* Targets of the plan's shard (all targets for an unsharded plan): their

@@ -51,4 +51,40 @@ __attribute__((visibility("default"))) RbfInterpolateResult rbf_interpolate(int_
                                      int_t nSourcePoints, fp_t *sourceValues,
                                      coordinates_t *targetPoints, int_t nTargetPoints);
 
+typedef int32_t offset_t;  // src/common/types.hpp:21
+typedef int32_t method_t;  // src/common/types.hpp:24
+typedef int32_t cell_t;    // src/common/types.hpp:25
+
+// Finite-element method selectors (src/common/types.hpp:29-37).  The B200
+// engine runs NEAREST_NEAREST; the others throw std::invalid_argument.
+enum class TransferMethods : method_t {
+  NEAREST_NEAREST = 0xF0,
+  INTERP_CLAMP = 0xF1,
+  INTERP_NEAREST = 0xF2,
+  INTERP_ZEROFILL = 0xF3,
+  INTERP_EXTRAP = 0xF4,
+  RBF_PUM = 0xF5,
+  MLS = 0xF6,
+};
+
+// src/interface.hpp:33-40.
+struct FeInterpolateResult {
+  std::vector<fp_t> targetValues;   ///< Value per target point.
+  std::vector<int_t> targetStatus;  ///< TransferStatus per target (0 = OUTSIDE).
+};
+
+/// Finite-element interpolation (src/interface.hpp:76-80) for
+/// NEAREST_NEAREST: every target takes its nearest source's value (lowest
+/// index on ties); the point-based method ignores connectivity and cell types,
+/// and the status stays OUTSIDE as in the reference.
+/// @throws std::invalid_argument on null pointers with non-zero counts or a
+///         method other than NEAREST_NEAREST.
+/// @throws std::runtime_error if spaceDimension is not 1, 2 or 3, or on a
+///         device error.
+__attribute__((visibility("default"))) FeInterpolateResult fe_interpolate(
+    int_t spaceDimension, unsigned char execSpace, method_t method, coordinates_t *sourcePoints,
+    int_t nSourcePoints, fp_t *sourceValues, int_t *connVal, int_t connValSize,
+    offset_t *connOff, int_t connOffSize, cell_t *cellTypes, coordinates_t *targetPoints,
+    int_t nTargetPoints, bool fortranIndexing = false);
+
 }  // namespace PACMAN

@@ -8,6 +8,7 @@ from .oracle import (  # noqa: F401
     OraclePlan,
     build,
     ensure_built,
+    fe_nearest,
     interpolate,
     set_threads,
     wendland,

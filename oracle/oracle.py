@@ -60,6 +60,9 @@ def _load():
         lib.orc_set_threads.argtypes = [ctypes.c_int]
         lib.orc_set_threads.restype = ctypes.c_int
         lib.orc_last_error.restype = ctypes.c_char_p
+        lib.orc_fe_nearest.argtypes = [ctypes.c_int, _f64p, ctypes.c_int64, _f64p, _f64p,
+                                       ctypes.c_int64, _f64p, _i32p]
+        lib.orc_fe_nearest.restype = ctypes.c_int
         _lib = lib
         return lib
 
@@ -176,3 +179,20 @@ def interpolate(dim, basis, src, values, tgt, nodes_per_cluster=50, relative_ove
     plan = build(dim, src, tgt, nodes_per_cluster, relative_overlap)
     out, _, _ = plan.solve(basis, values, support_radius)
     return out
+
+
+def fe_nearest(dim, src, values, tgt):
+    """NEAREST_NEAREST finite-element transfer (FTNearest.hpp:27-56): (values
+    at the targets, nearest source index or -1)."""
+    lib = _load()
+    src = np.ascontiguousarray(src, dtype=np.float64).reshape(-1, dim)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64).reshape(-1, dim)
+    vals = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    out = np.zeros(tgt.shape[0], dtype=np.float64)
+    idx = np.zeros(max(tgt.shape[0], 1), dtype=np.int32)
+    rc = lib.orc_fe_nearest(int(dim), _ptr(src) if src.size else None, src.shape[0],
+                            _ptr(vals) if vals.size else None, _ptr(tgt) if tgt.size else None,
+                            tgt.shape[0], _ptr(out) if out.size else None, _ptr(idx, _i32p))
+    if rc != 0:
+        raise RuntimeError(f"oracle fe_nearest failed ({rc}): {lib.orc_last_error().decode()}")
+    return out, idx[: tgt.shape[0]]

@@ -958,3 +958,44 @@ int orc_solve(const orc_plan *p, int basis, double support_radius, const double 
   free(done);
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Finite-element transfer NEAREST_NEAREST (src/finite_elements/FTNearest.hpp:27-56):
+ * every target takes the value of its nearest source (ArborX nearest(1) on a
+ * BVH of the sources, src/finite_elements/utils/ArborXCallbacks.hpp:172-182).
+ * Brute force here, squared distances as the kernels form them (t = b - a,
+ * acc = t_x^2, then fma per further axis), ties toward the lowest source index
+ * (ArborX's tie order is not reproducible; this is the documented convention).
+ * Targets with no source keep 0 (SetupTransferClass zero-fills,
+ * common/transfer.hxx:100-110); the status stays OUTSIDE (0), which FTNearest
+ * never changes.
+ * ---------------------------------------------------------------------- */
+int orc_fe_nearest(int dim, const double *src, int64_t n, const double *vals,
+                   const double *tgt, int64_t m, double *out, int32_t *nearest) {
+  if (dim < 1 || dim > 3) {
+    set_err("dimension must be 1, 2 or 3");
+    return -2;
+  }
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t t = 0; t < m; ++t) {
+    double y[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < dim; ++d) y[d] = tgt[t * dim + d];
+    double best = 0.0;
+    int64_t bi = -1;
+    for (int64_t i = 0; i < n; ++i) {
+      double x[3] = {0.0, 0.0, 0.0};
+      for (int d = 0; d < dim; ++d) x[d] = src[i * dim + d];
+      const double tx = x[0] - y[0], ty = x[1] - y[1], tz = x[2] - y[2];
+      double acc = tx * tx;
+      acc = fma(ty, ty, acc);
+      acc = fma(tz, tz, acc);
+      if (bi < 0 || acc < best) {
+        best = acc;
+        bi = i;
+      }
+    }
+    out[t] = bi >= 0 ? vals[bi] : 0.0;
+    if (nearest) nearest[t] = (int32_t)bi;
+  }
+  return 0;
+}

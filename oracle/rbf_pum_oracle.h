@@ -74,6 +74,12 @@ double orc_wendland(int basis, double r, double rho);
 int orc_set_threads(int nthreads);
 const char *orc_last_error(void);
 
+/* Finite-element NEAREST_NEAREST transfer: out[t] = vals[nearest source]
+ * (lowest index on ties), 0 without sources; nearest (may be NULL) receives
+ * the source index or -1. */
+int orc_fe_nearest(int dim, const double *src, int64_t n, const double *vals,
+                   const double *tgt, int64_t m, double *out, int32_t *nearest);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,9 @@ SIGNATURES = {
     "pacman_b200_plan_patch_lists": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP]),
     "pacman_b200_plan_local_values": (ctypes.c_int, [_VP, _VP]),
     "pacman_b200_plan_shard": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "pacman_b200_fe_interpolate": (ctypes.c_int, [
+        ctypes.c_int32, ctypes.c_int32, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_int64, _VP, _VP,
+        ctypes.POINTER(Options)]),
     "pacman_b200_plan_owned_targets": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _VP]),
     "pacman_b200_patch_radius_noalloc": (ctypes.c_int, [
         ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int32, _VP, _VP]),

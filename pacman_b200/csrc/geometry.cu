@@ -910,6 +910,39 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   cudaEventDestroy(e1);
 }
 
+// Packed double4 copy of row-major points and their exact bounding box.
+void pack_points(const double *in_dev, int dim, int64_t n, DevMem &out4, double lo[3],
+                 double hi[3], cudaStream_t st) {
+  out4.alloc(sizeof(double4) * std::max<int64_t>(n, 1), st);
+  for (int d = 0; d < 3; ++d) lo[d] = hi[d] = 0.0;
+  if (n == 0) return;
+  DevMem bb;
+  bb.alloc(sizeof(unsigned long long) * 6, st);
+  unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+  PB_CUDA(cudaMemcpyAsync(bb.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_pack<<<grid_for(n), kThreads, 0, st>>>(in_dev, dim, n, out4.as<double4>(),
+                                           bb.as<unsigned long long>());
+  note_launch();
+  unsigned long long h[6];
+  PB_CUDA(cudaMemcpyAsync(h, bb.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  PB_CUDA(cudaStreamSynchronize(st));
+  auto to_dbl = [](unsigned long long b) {
+    b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+    double d;
+    std::memcpy(&d, &b, sizeof(d));
+    return d;
+  };
+  for (int d = 0; d < dim; ++d) {
+    lo[d] = to_dbl(h[d]);
+    hi[d] = to_dbl(h[3 + d]);
+  }
+}
+
+void build_point_grid(DevGrid &out, const double4 *pts, int64_t n, int dim, const double *lo,
+                      const double *hi, double cell, cudaStream_t st) {
+  build_grid(out, pts, n, dim, lo, hi, cell, st);
+}
+
 void pu_gather(Plan &p, const double *local, int F, double *out_dev) {
   if (p.m == 0) return;
   const bool sharded = p.m_owned >= 0;

@@ -198,6 +198,15 @@ inline void note_launch(int k = 1) { launch_counter() += k; }
 // geometry.cu
 void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev);
 void pu_gather(Plan &p, const double *local, int F, double *out_dev);
+// Packed double4 points with their exact bounding box, and the uniform cell
+// grid over them (geometry.cu; used by nearest.cu).
+void pack_points(const double *in_dev, int dim, int64_t n, DevMem &out4, double lo[3],
+                 double hi[3], cudaStream_t st);
+void build_point_grid(DevGrid &out, const double4 *pts, int64_t n, int dim, const double *lo,
+                      const double *hi, double cell, cudaStream_t st);
+// Finite-element NEAREST_NEAREST transfer (nearest.cu).
+void fe_nearest(int dim, const double *src_dev, int64_t n, const double *vals_dev,
+                const double *tgt_dev, int64_t m, double *out_dev, cudaStream_t st);
 // Restricts the plan to target shard `rank` of `world` (shard.cu).
 void shard_plan(Plan &p, int rank, int world);
 

@@ -43,4 +43,39 @@ RbfInterpolateResult rbf_interpolate(int_t spaceDimension, unsigned char execSpa
   return result;
 }
 
+// PACMAN::fe_interpolate (src/interface.cpp:89-121) for NEAREST_NEAREST.
+FeInterpolateResult fe_interpolate(int_t spaceDimension, unsigned char execSpace,
+                                   method_t method, coordinates_t *sourcePoints,
+                                   int_t nSourcePoints, fp_t *sourceValues, int_t *connVal,
+                                   int_t connValSize, offset_t *connOff, int_t connOffSize,
+                                   cell_t *cellTypes, coordinates_t *targetPoints,
+                                   int_t nTargetPoints, bool fortranIndexing) {
+  (void)connVal;
+  (void)connValSize;
+  (void)connOff;
+  (void)connOffSize;
+  (void)cellTypes;
+  (void)fortranIndexing;
+  if (sourcePoints == nullptr && nSourcePoints > 0)
+    throw std::invalid_argument("sourcePoints is null but nSourcePoints > 0");
+  if (targetPoints == nullptr && nTargetPoints > 0)
+    throw std::invalid_argument("targetPoints is null but nTargetPoints > 0");
+  if (sourceValues == nullptr && nSourcePoints > 0)
+    throw std::invalid_argument("sourceValues is null but nSourcePoints > 0");
+  if (spaceDimension < 1 || spaceDimension > 3)
+    throw std::runtime_error("The dimension of the points can only be: 1, 2 or 3.\n");
+  if (execSpace > ExecSpaces::SYCL)
+    throw std::invalid_argument("execspace: Serial, OpenMP, Threads, Cuda, HIP, SYCL");
+  FeInterpolateResult result;
+  const size_t m = nTargetPoints > 0 ? size_t(nTargetPoints) : 0;
+  result.targetValues.assign(m, 0.0);
+  result.targetStatus.assign(m, 0);
+  const int rc = pacman_b200_fe_interpolate(
+      spaceDimension, method, sourcePoints, nSourcePoints > 0 ? nSourcePoints : 0, sourceValues,
+      targetPoints, int64_t(m), result.targetValues.data(), result.targetStatus.data(), nullptr);
+  if (rc == PACMAN_B200_ERR_INVALID) throw std::invalid_argument(pacman_b200_last_error());
+  if (rc != 0) throw std::runtime_error(pacman_b200_last_error());
+  return result;
+}
+
 }  // namespace PACMAN
