@@ -9,7 +9,10 @@
 // on [A | I]): slot (i, s) holds A[i][s] until pivot s and L^{-1}[i][s]
 // afterwards; one team barrier per pivot.  Then alpha = L^{-T} D^{-1} L^{-1} r
 // by two team reductions.  The polynomial block (moments, condition test,
-// least squares; poly.cuh) runs meanwhile on a separate warp.
+// least squares; poly.cuh) runs meanwhile on a separate warp.  For a plan
+// that keeps its factorisations the eliminated blocks are stored after the
+// elimination (fac_mode 1) and later loaded in place of assembly and
+// elimination (fac_mode 2): N * N doubles per patch, thread-block order.
 #include "patch.cuh"
 
 namespace pacman_b200 {
