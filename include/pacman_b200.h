@@ -58,8 +58,12 @@ extern "C" {
 
 /* Precision of the per-patch solves. */
 #define PACMAN_B200_FP64 0  /* the reference algorithm: unpivoted LU in FP64 */
-#define PACMAN_B200_MIXED 1 /* FP32 factor + FP64 refinement where the patch is
-                               well conditioned, FP64 Cholesky elsewhere */
+#define PACMAN_B200_MIXED 1 /* Cholesky (A is symmetric positive definite):
+                               small patches in FP64 registers, the column
+                               updates of large patches as split-integer
+                               products on the int8 tensor cores (FP64-level
+                               accuracy); a failed patch is re-solved by the
+                               FP64 LU */
 
 typedef struct pacman_b200_options {
   int32_t nodes_per_cluster; /* 50: RbfPumInterpolator default, src/rbf_pum/interpolator.hxx:39 */
@@ -76,9 +80,13 @@ typedef struct pacman_b200_stats {
   int64_t num_patches;      /* K, surviving centres */
   int64_t sum_n, sum_m;     /* total patch sources / targets */
   int64_t max_n;            /* largest patch */
-  int64_t patches_fp32;     /* patches solved by FP32 factor + FP64 refinement */
-  int64_t patches_fp64;     /* patches solved by an FP64 factorisation */
-  int64_t patches_fallback; /* FP32 attempts that fell back to FP64 */
+  int64_t patches_fp32;     /* patches factored in FP32: always 0 (the mixed
+                               path emulates FP64 products on the int8 tensor
+                               cores instead; FP32 factors of these matrices
+                               do not refine to the 1e-10 bound) */
+  int64_t patches_fp64;     /* patches solved at FP64 accuracy */
+  int64_t patches_fallback; /* mixed-path patches re-solved by the FP64 LU
+                               (non-positive pivot or a pipeline time-out) */
   int64_t dropped_axis_patches; /* patches whose linear polynomial lost an axis */
   double ms_geometry;       /* device time of radius + centres + membership */
   double ms_solve;          /* device time of the patch solves */
@@ -204,20 +212,6 @@ PACMAN_B200_API int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, i
 PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local);
 
 /*
- * Target sharding of one transfer over `world` GPUs, one process per GPU
- * (no counterpart in the reference, which runs on one device).  Every rank
- * creates the same plan (all sources, all targets: the patch cover depends on
- * both) and calls this with its rank.  The targets are cut into `world`
- * ranges of their Morton order over the source bounding box, balanced by the
- * solve cost n^3 of the patches each range needs; the cut uses integer data
- * only, so all ranks agree on it.  Afterwards an execute solves only the
- * patches holding an owned target, writes the owned targets' values (bit-
- * identical to the unsharded transfer) and zero elsewhere: the sum over the
- * ranks (one all-reduce) is the whole result.  The adjoint of a sharded plan
- * gives this shard's contribution to the source-value gradient and the
- * owned targets' coordinate gradients.  A plan is sharded once.
- */
-/*
  * Finite-element transfer of the reference's PACMAN::fe_interpolate
  * (src/interface.hpp:76-80, src/interface.cpp:89-121) for the method
  * NEAREST_NEAREST (0xF0, src/common/types.hpp:29-37; FTNearest.hpp:27-56):
@@ -236,6 +230,20 @@ PACMAN_B200_API int pacman_b200_fe_interpolate(int32_t dim, int32_t method,
                                                double *target_values, int32_t *target_status,
                                                const pacman_b200_options *opts);
 
+/*
+ * Target sharding of one transfer over `world` GPUs, one process per GPU
+ * (no counterpart in the reference, which runs on one device).  Every rank
+ * creates the same plan (all sources, all targets: the patch cover depends on
+ * both) and calls this with its rank.  The targets are cut into `world`
+ * ranges of their Morton order over the source bounding box, balanced by the
+ * solve cost n^3 of the patches each range needs; the cut uses integer data
+ * only, so all ranks agree on it.  Afterwards an execute solves only the
+ * patches holding an owned target, writes the owned targets' values (bit-
+ * identical to the unsharded transfer) and zero elsewhere: the sum over the
+ * ranks (one all-reduce) is the whole result.  The adjoint of a sharded plan
+ * gives this shard's contribution to the source-value gradient and the
+ * owned targets' coordinate gradients.  A plan is sharded once.
+ */
 PACMAN_B200_API int pacman_b200_plan_shard(pacman_b200_plan *plan, int32_t rank, int32_t world);
 
 /* Targets of the plan's shard (all targets for an unsharded plan): their
@@ -252,14 +260,18 @@ PACMAN_B200_API int pacman_b200_plan_owned_targets(const pacman_b200_plan *plan,
  * library allocate device memory, e.g. a coupled code that reserves the GPU
  * for its own pool allocator at start-up.  Its working memory is one fixed
  * 16 KiB file-scope __device__ array, present on every GPU that loads this
- * library until the process exits; the first call on a device resolves that
- * array's address (cudaGetSymbolAddress) with the device current, so make the
+ * library until the process exits.  Every call resolves that array's address
+ * (cudaGetSymbolAddress) in the context current on the calling thread, so a
+ * cudaDeviceReset or a context the caller made current is followed; the
+ * first call on a device also loads this library's kernels there, so make the
  * first call before any stream capture.  Calls share the array: calls that
  * overlap on the GPU race and must be serialised by the caller.
  * source_points: device memory of the current device, row-major [n x dim];
  * limits: dim <= 3 (the array holds at most 7 samples), 1 <= n <= 2^31 - 1.
  * stream: cudaStream_t (NULL = default stream); the call returns after
- * *radius (host or device pointer) has been written.
+ * *radius (host or device pointer) has been written.  A radius that is zero
+ * or not finite (all sources coincide) is written and reported as
+ * PACMAN_B200_ERR_DEGENERATE, as the full transfer reports it.
  */
 PACMAN_B200_API int pacman_b200_patch_radius_noalloc(int32_t dim, const double *source_points,
                                                      int64_t n_source, int32_t nodes_per_cluster,

@@ -17,7 +17,7 @@
 // caller.  What has to start at zero or at an extreme is reset by each call.
 #include <cstdint>
 #include <cstring>
-#include <mutex>
+#include <cmath>
 #include <string>
 
 #include "../../include/pacman_b200.h"
@@ -257,25 +257,23 @@ int sr_fail(int code, const std::string &m) {
   return code;
 }
 
-// Device address of the scratch array, resolved once per device.
-std::mutex g_sr_mu;
-void *g_sr_addr[64] = {nullptr};
-
-int scratch_address(int device, StaticRadiusState **out) {
-  if (device < 0 || device >= 64) return sr_fail(PACMAN_B200_ERR_CUDA, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_sr_mu);
-  if (!g_sr_addr[device]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_radius_scratch);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return sr_fail(PACMAN_B200_ERR_CUDA,
-                     std::string("cudaGetSymbolAddress of the radius scratch failed: ") +
-                         cudaGetErrorString(e));
-    }
-    g_sr_addr[device] = p;
+// Device address of the scratch array in the CUDA context that is current on
+// the calling thread.  A __device__ symbol's address belongs to one context:
+// after cudaDeviceReset, or when the caller makes a context of its own
+// current (driver API), an address cached from an earlier call would point
+// into memory this call does not own.  So every call resolves it again; the
+// lookup is cheap and allocates nothing.  The first call on a device also
+// loads this file's kernels into the context.
+int scratch_address(StaticRadiusState **out) {
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_radius_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return sr_fail(PACMAN_B200_ERR_CUDA,
+                   std::string("cudaGetSymbolAddress of the radius scratch failed: ") +
+                       cudaGetErrorString(e));
   }
-  *out = static_cast<StaticRadiusState *>(g_sr_addr[device]);
+  *out = static_cast<StaticRadiusState *>(p);
   return 0;
 }
 
@@ -312,7 +310,7 @@ extern "C" PACMAN_B200_API int pacman_b200_patch_radius_noalloc(
                    "allocates nothing, so it cannot stage host arrays)");
   }
   StaticRadiusState *st = nullptr;
-  if (int rc = scratch_address(device, &st)) return rc;
+  if (int rc = scratch_address(&st)) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const long long k = nodes_per_cluster < n_source ? nodes_per_cluster : n_source;
   const int ns = 2 * dim + 1;
@@ -329,11 +327,18 @@ extern "C" PACMAN_B200_API int pacman_b200_patch_radius_noalloc(
     k_sr_select<<<1, 32, 0, s>>>(st, pass);
   }
   k_sr_final<<<1, 32, 0, s>>>(st);
+  double r_host = 0.0;
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(radius, &st->radius, sizeof(double), cudaMemcpyDefault, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&r_host, &st->radius, sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess)
     return sr_fail(PACMAN_B200_ERR_CUDA, std::string("radius kernels: ") + cudaGetErrorString(e));
+  // The full transfer rejects the same radius (all sources coincide, or a
+  // coordinate is not finite); so does this entry point, after writing it.
+  if (!(r_host > 0.0) || !std::isfinite(r_host))
+    return sr_fail(PACMAN_B200_ERR_DEGENERATE, "degenerate patch radius (zero or non-finite)");
   return 0;
 }

@@ -9,8 +9,9 @@ types, returning a float64 array of length ``len(target_points)``.
 Superset keywords: ``nodes_per_cluster``, ``relative_overlap`` and
 ``support_radius`` (the reference's hard-coded defaults 50 / 0.15 / 0.1,
 src/rbf_pum/interpolator.hxx:39-41), ``precision`` ("fp64": the reference's
-unpivoted-LU algorithm; "mixed": FP32 factor + FP64 refinement where the
-patch allows it, FP64 Cholesky elsewhere), multi-field ``source_values`` of
+unpivoted-LU algorithm; "mixed": Cholesky with the column updates of large
+patches as split-integer products on the int8 tensor cores, FP64-level
+accuracy, small patches in FP64 registers), multi-field ``source_values`` of
 shape (N, F) with F <= 8, and CUDA torch tensors (device-resident inputs and
 output, ordered on torch's current stream).
 """

@@ -64,6 +64,28 @@ def test_noalloc_radius_equals_transfer_radius_on_consecutive_calls():
         assert out.item() == expected[1]
 
 
+def test_noalloc_leaves_device_memory_untouched():
+    """The point of the entry point: repeated calls take no device memory.
+    The free memory the driver reports (cudaMemGetInfo) and torch's own
+    allocator are read before and after, once the kernels are loaded (the
+    first launch of a kernel may load its module into device memory)."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    dim, S, _, npc = _cases()[1]
+    pts = torch.tensor(S, device="cuda")
+    r = ctypes.c_double()
+    _noalloc(torch, lib, dim, pts, npc, ctypes.addressof(r))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(5):
+        _noalloc(torch, lib, dim, pts, npc, ctypes.addressof(r))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert torch.cuda.memory_allocated() == alloc0
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_rejects_what_it_cannot_serve():
     torch = pytest.importorskip("torch")
     lib = _lib.load()
@@ -80,3 +102,11 @@ def test_noalloc_rejects_what_it_cannot_serve():
     rc = lib.pacman_b200_patch_radius_noalloc(3, dpts.data_ptr(), 0, 10, None,
                                               ctypes.addressof(r))
     assert rc == _lib.ERR_INVALID
+    # Coincident sources give a zero radius, which the full transfer rejects
+    # as degenerate too.
+    same = torch.full((50, 3), 0.25, dtype=torch.float64, device="cuda")
+    rc = lib.pacman_b200_patch_radius_noalloc(3, same.data_ptr(), 50, 10, None,
+                                              ctypes.addressof(r))
+    assert rc == _lib.ERR_DEGENERATE and r.value == 0.0
+    with pytest.raises(Exception):
+        pacman.rbf.Plan(3, same.cpu().numpy(), same.cpu().numpy(), nodes_per_cluster=10)
