@@ -12,12 +12,15 @@ and the host copy of the result inside the timed region.  Inputs (56 MB) are
 smaller than L2, so L2 is flushed (a 512 MB write) between timed steps,
 outside the CUDA-event brackets.
 
-N > 1 (torchrun): every rank runs its own transfer of the same workload
-(independent replicas, weak scaling); value = all ranks' targets / max time.
+N > 1 (torchrun): one transfer of the same workload sharded over the ranks
+by target ranges (every rank builds the whole geometry and solves the patches
+its targets need; one sum all-reduce assembles the result): strong scaling,
+value = the transfer's targets / max-over-ranks time.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference itself cannot be built here: it needs Kokkos, KokkosKernels and
-ArborX) on all host threads, on a stratified sample of the patch solves.
+ArborX) on all host threads; each step times a bounded, stratified sample of
+the patch solves and estimates the whole transfer from it.
 """
 from __future__ import annotations
 
@@ -55,6 +58,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--kernels-only", action="store_true",
                     help="run warmup + steps transfers and exit (for ncu launch lists)")
+    ap.add_argument("--configs", action="store_true",
+                    help="one line per configuration of the baseline table (GPU in both "
+                         "precisions, the CPU restatement in Serial and OpenMP, errors)")
     return ap.parse_args()
 
 
@@ -69,19 +75,33 @@ def dist_info():
 # CPU baseline: the oracle (CPU restatement), bounded sample
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(w, seconds_budget: float):
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(w, seconds_budget: float, threads: int | None = None):
     """Times the CPU restatement on a bounded sample: the full geometry phase,
     then the patch solves of a stratified random sample (by patch size), whose
     time is scaled by the inverse sampling fraction of each stratum, plus one
-    partition-of-unity pass.  Returns (pts_per_s, description, threads)."""
+    partition-of-unity pass.  Returns (pts_per_s, description, threads,
+    seconds spent, estimated seconds per transfer)."""
     import oracle
-    threads = oracle.set_threads(os.cpu_count() or 1)
+    threads = oracle.set_threads(threads or os.cpu_count() or 1)
+    t_start = time.perf_counter()
     t0 = time.perf_counter()
     plan = oracle.build(3, w["src"], w["tgt"], w["nodes_per_cluster"])
     t_geom = time.perf_counter() - t0
     off, _ = plan.src_csr()
+    toff, _ = plan.tgt_csr()
     n = np.diff(off)
-    K = len(n)
+    live = np.diff(toff) > 0
+    K = int(live.sum())
     rng = np.random.default_rng(0)
     edges = [0, 64, 128, 256, 512, 1024, 2048, 1 << 30]
     total = 0.0
@@ -89,7 +109,7 @@ def cpu_baseline(w, seconds_budget: float):
     budget_each = seconds_budget / (len(edges) - 1)
     vals = w["values"]
     for lo, hi in zip(edges[:-1], edges[1:]):
-        ids = np.where((n > lo) & (n <= hi))[0]
+        ids = np.where((n > lo) & (n <= hi) & live)[0]
         if len(ids) == 0:
             continue
         rng.shuffle(ids)
@@ -112,37 +132,47 @@ def cpu_baseline(w, seconds_budget: float):
     t_pu = time.perf_counter() - t1
     est = t_geom + total + t_pu
     m = w["tgt"].shape[0]
-    desc = (f"CPU restatement of the reference algorithm (FP64, unpivoted LU), {threads} threads: "
-            f"full geometry ({t_geom:.2f}s) + patch solves of a stratified sample of {sampled}/{K} "
-            f"patches scaled per size stratum ({total:.1f}s est.) + PU pass ({t_pu:.2f}s); "
-            f"estimated {est:.1f}s per transfer")
-    return m / est, desc, threads
+    desc = (f"CPU restatement of the reference algorithm (FP64, unpivoted LU; the reference "
+            f"itself needs Kokkos/KokkosKernels/ArborX), {threads} thread(s) on {cpu_model()}: "
+            f"full geometry ({t_geom:.2f}s) + patch solves of a stratified sample of "
+            f"{sampled}/{K} patches ({100.0 * sampled / max(K, 1):.1f}%) scaled per size stratum "
+            f"({total:.1f}s est.) + PU pass ({t_pu:.2f}s); estimated {est:.1f}s per transfer")
+    return m / est, desc, threads, time.perf_counter() - t_start, est
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement on all host threads.  A warm-up
+    step solves a small sample untimed; each timed step is one bounded
+    estimator pass (a stratified sample of the patch solves, about
+    min(30, 150 / steps) seconds), whose estimate of the whole transfer gives
+    the step's throughput.  ms_per_step is the time a step actually took."""
     rank, world, _ = dist_info()
     if rank != 0:
         return
     args.world = world
     from pacman_b200 import workloads as W
     w = W.make(args.workload, args.scale)
-    vals = []
     for _ in range(args.warmup):
-        pass  # the oracle has no warm state worth priming beyond the first build
-    desc = ""
-    threads = 1
+        cpu_baseline(w, 0.5)
+    budget = max(3.0, min(args.cpu_seconds, 30.0, 150.0 / max(args.steps, 1)))
+    vals, spent, ests = [], [], []
+    desc, threads = "", 1
     for _ in range(max(args.steps, 1)):
-        v, desc, threads = cpu_baseline(w, min(args.cpu_seconds, 30.0))
+        v, desc, threads, sec, est = cpu_baseline(w, budget)
         vals.append(v)
+        spent.append(sec)
+        ests.append(est)
     value = statistics.median(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": w["tgt"].shape[0] / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(spent) / len(spent),
+        "estimated_ms_per_transfer": 1e3 * statistics.median(ests),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy generators)",
         "config": config_dict(args, w),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": desc},
+                         "sample": f"each step: {desc}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -243,13 +273,42 @@ def fp64_gemm_peak(torch, dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def read_traffic(kernel_key: str):
-    """dram bytes per launch of the dominant kernel from the committed ncu
-    summary (line 'dram_bytes_per_launch[<key>]: <bytes>'), or None."""
+def measured_peaks():
+    """HBM GB/s and dense bf16 TFLOP/s (burst, sustained) measured on this
+    pool's B200s (MEASURED_PEAKS.json, written beside this file by the
+    pipeline), else the pool's earlier measurement; with the source named."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+
+        def pick(*keys):
+            for k in keys:
+                v = d.get(k)
+                if isinstance(v, dict):
+                    v = v.get("value")
+                if isinstance(v, (int, float)) and v > 0:
+                    return float(v)
+            return None
+        hbm = pick("hbm_gbs", "hbm_GBs", "hbm_copy_gbs")
+        bf16 = pick("bf16_tflops", "bf16_dense_tflops")
+        bf16s = pick("bf16_tflops_sustained") or bf16
+        if hbm and bf16:
+            return {"hbm_gbs": hbm, "bf16_tflops": bf16, "bf16_tflops_sustained": bf16s,
+                    "source": "measured (MEASURED_PEAKS.json)"}
+    except (OSError, ValueError):
+        pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback (earlier measurement on this pool: 6.65 TB/s copy, 1.59 PFLOP/s "
+                      "bf16 burst, ~1.4 sustained)"}
+
+
+def read_profile_value(key: str):
+    """A figure from the committed ncu summaries (a line '<key>: <number>'
+    in profiles/*.txt), or None."""
     import glob
-    for path in glob.glob(os.path.join(ROOT, "profiles", "*.txt")):
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.txt"))):
         for line in open(path):
-            if line.startswith(f"dram_bytes_per_launch[{kernel_key}]:"):
+            if line.startswith(key + ":"):
                 try:
                     return float(line.split(":", 1)[1].strip().split()[0])
                 except ValueError:
@@ -257,10 +316,141 @@ def read_traffic(kernel_key: str):
     return None
 
 
+def run_configs(args):
+    """The five configurations of the baseline table, one JSON line each: GPU
+    time per transfer in both precisions (device-resident inputs, CUDA events,
+    median after warm-up), the CPU restatement of the reference algorithm with
+    1 thread (Serial) and all host threads (OpenMP) -- in full where it runs in
+    seconds, else estimated from a bounded stratified sample -- and relative L2
+    errors (against the oracle in full where it runs, else mixed vs FP64)."""
+    import torch
+    import oracle
+    import pacman_b200 as pacman
+    from pacman_b200 import workloads as W
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nthreads = os.cpu_count() or 1
+    base = {"cpu_model": cpu_model(), "host_threads": nthreads}
+
+    def gpu_ms(fn, reps, warm=3):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    def transfer_case(name, w, basis, reps, full_oracle):
+        S = torch.tensor(w["src"], device=dev)
+        T = torch.tensor(w["tgt"], device=dev)
+        vals = w["values"][:, 0] if w["values"].shape[1] == 1 else w["values"]
+        V = torch.tensor(vals, device=dev)
+        npc = w["nodes_per_cluster"]
+        line = dict(base, config=name, n_source=int(S.shape[0]), n_target=int(T.shape[0]),
+                    fields=int(w["values"].shape[1]), basis=hex(basis))
+        outs = {}
+        for prec in ("mixed", "fp64"):
+            f = lambda: pacman.rbf.interpolate(3, 3, basis, S, V, T, nodes_per_cluster=npc,
+                                               precision=prec)
+            line[f"gpu_{prec}_ms"] = gpu_ms(f, reps)
+            outs[prec] = f().cpu().numpy()
+        m = w["tgt"].shape[0]
+        line["gpu_mixed_pts_s"] = m / (line["gpu_mixed_ms"] * 1e-3)
+        line["gpu_fp64_pts_s"] = m / (line["gpu_fp64_ms"] * 1e-3)
+        line["mixed_over_fp64"] = line["gpu_fp64_ms"] / line["gpu_mixed_ms"]
+        line["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(outs["mixed"] - outs["fp64"]) /
+                                             np.linalg.norm(outs["fp64"]))
+        ww = dict(w, basis=basis)
+        if full_oracle:
+            for label, th in (("serial", 1), ("openmp", nthreads)):
+                oracle.set_threads(th)
+                t0 = time.perf_counter()
+                ref = oracle.interpolate(3, basis, w["src"], vals, w["tgt"], npc)
+                line[f"oracle_{label}_s"] = time.perf_counter() - t0
+            for prec in ("mixed", "fp64"):
+                line[f"rel_l2_{prec}_vs_oracle"] = float(np.linalg.norm(outs[prec] - ref) /
+                                                         np.linalg.norm(ref))
+            line["oracle_kind"] = "full transfer"
+        else:
+            _, desc, _, _, est = cpu_baseline(ww, 20.0)
+            _, desc1, _, _, est1 = cpu_baseline(ww, 10.0, threads=1)
+            line["oracle_openmp_s"] = est
+            line["oracle_serial_s"] = est1
+            line["oracle_kind"] = "estimated: " + desc + " | " + desc1
+        print(json.dumps(line), flush=True)
+        return line
+
+    transfer_case("1: 20k -> 20k uniform, C2", W.make("uniform_20k"), W.WENDLANDC2, 10, True)
+    transfer_case("2: 1M -> 1M grid + blobs, C4", W.make("grid_blobs_1m"), W.WENDLANDC4, 5,
+                  False)
+    shell = W.make("shell_4m")
+    for b in (W.WENDLANDC2, W.WENDLANDC4, W.WENDLANDC6):
+        transfer_case(f"3: 4M -> 2M shell + cube, 8 fields, {hex(b)}", shell, b, 3, False)
+    # 4: adjoint workload: forward (saved) + adjoint of values and target
+    # coordinates; the oracle times the forward transfer.
+    w = W.make("uniform_500k")
+    S = torch.tensor(w["src"], device=dev)
+    T = torch.tensor(w["tgt"], device=dev)
+    V = torch.tensor(w["values"], device=dev)
+    G = torch.randn(T.shape[0], V.shape[1], dtype=torch.float64, device=dev,
+                    generator=torch.Generator(device=dev).manual_seed(7))
+    line = dict(base, config="4: 500k -> 500k uniform, C4, 4 fields, adjoint")
+    grads = {}
+    for prec in ("mixed", "fp64"):
+        plan = pacman.rbf.Plan(3, S, T, precision=prec)
+        line[f"gpu_{prec}_forward_ms"] = gpu_ms(
+            lambda: plan.execute(W.WENDLANDC4, V, save_for_adjoint=True), 5)
+        line[f"gpu_{prec}_adjoint_ms"] = gpu_ms(lambda: plan.adjoint(G), 5)
+        grads[prec] = [g.cpu().numpy() for g in plan.adjoint(G)]
+        plan.close()
+    line["rel_l2_grad_values_mixed_vs_fp64"] = float(
+        np.linalg.norm(grads["mixed"][0] - grads["fp64"][0]) / np.linalg.norm(grads["fp64"][0]))
+    line["rel_l2_grad_targets_mixed_vs_fp64"] = float(
+        np.linalg.norm(grads["mixed"][1] - grads["fp64"][1]) / np.linalg.norm(grads["fp64"][1]))
+    for label, th in (("serial", 1), ("openmp", nthreads)):
+        oracle.set_threads(th)
+        t0 = time.perf_counter()
+        oracle.interpolate(3, W.WENDLANDC4, w["src"], w["values"], w["tgt"], 50)
+        line[f"oracle_forward_{label}_s"] = time.perf_counter() - t0
+    print(json.dumps(line), flush=True)
+    # 5: many uneven problems in one batched call; the oracle runs a random
+    # 32 of them in full, scaled by the targets of all.
+    probs = W.many_problems(count=256)
+    bP = [(3, q["basis"], torch.tensor(q["src"], device=dev),
+           torch.tensor(q["values"] if q["values"].shape[1] > 1 else q["values"][:, 0],
+                        device=dev), torch.tensor(q["tgt"], device=dev)) for q in probs]
+    tot = sum(q["tgt"].shape[0] for q in probs)
+    line = dict(base, config="5: 256 uneven problems, C0-C8, 1-4 fields", targets=int(tot))
+    for prec in ("mixed", "fp64"):
+        ms = gpu_ms(lambda: pacman.rbf.interpolate_batch(bP, precision=prec), 3, warm=1)
+        line[f"gpu_{prec}_ms"] = ms
+        line[f"gpu_{prec}_pts_s"] = tot / (ms * 1e-3)
+    pick = np.random.default_rng(3).choice(len(probs), size=32, replace=False)
+    sub = sum(probs[i]["tgt"].shape[0] for i in pick)
+    for label, th in (("serial", 1), ("openmp", nthreads)):
+        oracle.set_threads(th)
+        t0 = time.perf_counter()
+        for i in pick:
+            q = probs[i]
+            oracle.interpolate(3, q["basis"], q["src"], q["values"], q["tgt"], 50)
+        line[f"oracle_{label}_s"] = (time.perf_counter() - t0) * tot / sub
+    line["oracle_kind"] = f"32 of 256 problems in full, scaled by targets ({sub} of {tot})"
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.configs:
+        return run_configs(args)
     import torch
     import torch.distributed as dist
     import pacman_b200 as pacman
@@ -352,7 +542,7 @@ def main():
         o_np[...] = out
 
     e2e_step()
-    e2e_times = timed(e2e_step, max(1, min(args.steps, 3)))
+    e2e_times = timed(e2e_step, args.steps)
     e2e_ms = sum(e2e_times) / len(e2e_times)
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
@@ -361,20 +551,27 @@ def main():
     h2d = (w["src"].nbytes + w["tgt"].nbytes + np.ascontiguousarray(vals_np).nbytes)
     d2h = o_np.nbytes
 
-    # Plain FP64 path and agreement with it.
-    extra = {}
+    # Plain FP64 path (the reference's unpivoted-LU algorithm) over the same
+    # number of timed steps, and the agreement of the two paths.
+    extra = {"ms_per_step_median": statistics.median(times),
+             "e2e_ms_per_step_median": statistics.median(e2e_times)}
     if not args.no_fp64_compare:
         out_mixed = step(args.precision).cpu().numpy()
         f64_stats = {}
-        f64_times = timed(lambda: step("fp64", f64_stats), 1)
+        step("fp64")
+        f64_times = timed(lambda: step("fp64", f64_stats), args.steps)
         out64 = step("fp64").cpu().numpy()
-        f64_ms = f64_times[0]
+        f64_ms = sum(f64_times) / len(f64_times)
         if world > 1:
             t = torch.tensor([f64_ms], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             f64_ms = float(t.item())
         extra["fp64_value"] = m / (f64_ms * 1e-3)
+        extra["fp64_ms_per_step"] = f64_ms
+        extra["fp64_ms_per_step_median"] = statistics.median(f64_times)
         extra["mixed_over_fp64"] = extra["fp64_value"] and value / extra["fp64_value"]
+        extra["mixed_over_fp64_median"] = (statistics.median(f64_times) /
+                                           statistics.median(times))
         extra["rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(out_mixed - out64) / np.linalg.norm(out64))
         extra["fp64_ms_factor"] = f64_stats.get("ms_factor")
 
@@ -413,30 +610,60 @@ def main():
             batch[prec] = {"value": btot / (bms * 1e-3), "ms_per_call": bms}
         extra["many_uneven_256"] = batch
 
-    # Roofline of the dominant kernel, the step kernel of the large-patch
-    # Cholesky: one extra transfer after the timed region with CUDA events
-    # around each of its launches, on the stream it runs on.
-    peak = fp64_gemm_peak(torch, dev)
+    # Roofline of the dominant kernel: the int8 step kernel of the large-patch
+    # Cholesky (k_col_step_oz).  One extra transfer after the timed region,
+    # in the timed configuration (all slot groups on their streams), with CUDA
+    # events around every step launch on the stream it runs on; the span of
+    # each kind is the union of its launch intervals.
+    peaks = measured_peaks()
+    dgemm = fp64_gemm_peak(torch, dev)
     kst = {}
     plan = pacman.rbf.Plan(3, S, T, precision=args.precision, **kw)
     plan.execute(w["basis"], V, stats=kst, time_kernels=True)
     plan.close()
-    ms_upd = kst.get("ms_update", 0.0)
-    achieved = kst.get("update_flops", 0.0) / (ms_upd * 1e-3) / 1e12 if ms_upd else 0.0
-    nl = max(1, int(kst.get("update_launches", 0)))
-    roofline = {"bound": "fp64", "kernel": "k_col_step / k_col_step_oz (left-looking Cholesky "
-                                           "step: column update on the FP64 tensor cores, from "
-                                           "step 4 on the int8 tensor cores; trsm; next diagonal)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None,
-                "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU (FP64 has no "
-                               "faster path on B200; MEASURED_PEAKS.json holds no FP64 figure)",
-                "traffic": read_traffic(args.workload),
-                "flops_per_launch": kst.get("update_flops", 0.0) / nl,
-                "ms_per_launch": ms_upd / nl,
-                "launches_per_step": nl,
-                "ms_update_per_step": ms_upd,
-                "share_of_step": ms_upd / ms_per_step if ms_per_step else None}
+    tile_flops = 2.0 * 64 ** 3
+    ms_i8 = kst.get("ms_update_i8", 0.0)
+    prod_i8 = kst.get("update_flops_i8", 0.0) / tile_flops
+    ms_f64 = kst.get("ms_update_f64", 0.0)
+    # Algorithmic work of one int8 tile product: 28 int8 digit products of
+    # 64x64x64 (slice pairs a + b <= 8 of 7 slices) and the 7 int8 slices of
+    # one 64x64 L tile read from HBM (the shared tile row comes from L2).
+    i8_ops = prod_i8 * 28 * tile_flops
+    i8_bytes = prod_i8 * 7 * 64 * 64
+    int8_peak = 2.0 * peaks["bf16_tflops"]
+    nl = max(1, int(kst.get("update_launches_i8", 0)))
+    ach = i8_ops / (ms_i8 * 1e-3) / 1e12 if ms_i8 else 0.0
+    hbm_ach = i8_bytes / (ms_i8 * 1e-3) / 1e9 if ms_i8 else 0.0
+    traffic_per_product = read_profile_value("dram_bytes_per_tile_product[k_col_step_oz]")
+    roofline = {
+        "bound": "tensor",
+        "kernel": "k_col_step_oz (left-looking Cholesky step of the large patches: column "
+                  "update on the int8 tensor cores, tcgen05.mma kind::i8, 7-slice split-integer "
+                  "FP64 emulation; trsm; next diagonal tile)",
+        "achieved": ach, "peak": int8_peak, "unit": "TFLOP/s",
+        "frac": ach / int8_peak if int8_peak else None,
+        "peak_source": "int8 dense = 2 x bf16 dense, " + peaks["source"]
+                       + " (derived: int8 throughput itself is not measured)",
+        "traffic": (traffic_per_product * prod_i8 / nl) if traffic_per_product else None,
+        "algorithmic_bytes_per_launch": i8_bytes / nl,
+        "hbm": {"achieved_gbs": hbm_ach, "peak_gbs": peaks["hbm_gbs"],
+                "frac": hbm_ach / peaks["hbm_gbs"]},
+        "tile_products_per_launch": prod_i8 / nl,
+        "ms_per_launch": ms_i8 / nl,
+        "launches_per_step": nl,
+        "ms_span_per_step": ms_i8,
+        "share_of_step": ms_i8 / ms_per_step if ms_per_step else None,
+        "fp64_steps": {
+            "kernel": "k_col_step<1> (steps 0-3: column update on the FP64 tensor cores, "
+                      "mma.sync f64)",
+            "achieved": kst.get("update_flops_f64", 0.0) / (ms_f64 * 1e-3) / 1e12 if ms_f64 else 0,
+            "peak": dgemm, "unit": "TFLOP/s",
+            "peak_source": "measured live: cuBLAS DGEMM 8192^3 on this GPU",
+            "launches_per_step": int(kst.get("update_launches_f64", 0)),
+            "ms_span_per_step": ms_f64},
+    }
+    if roofline["fp64_steps"]["peak"]:
+        roofline["fp64_steps"]["frac"] = roofline["fp64_steps"]["achieved"] / dgemm
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -448,6 +675,7 @@ def main():
         "e2e": {"value": m / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(stats.get("kernel_launches", 0)) * args.steps,
+        "host_syncs_per_step": int(stats.get("host_syncs", 0)),
         "clocks": clk.summary(),
         "roofline": roofline,
         "stats": {k: stats.get(k) for k in ("radius", "num_patches", "sum_n", "sum_m", "max_n",
@@ -456,9 +684,12 @@ def main():
         **extra,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, desc, threads = cpu_baseline(w, args.cpu_seconds)
+        v, desc, threads, _, _ = cpu_baseline(w, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": desc}
+        v1, desc1, _, _, _ = cpu_baseline(w, args.cpu_seconds / 2, threads=1)
+        line["cpu_baseline_serial"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
+                                       "sample": desc1}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PACMAN_B200_ABI_VERSION 3
+#define PACMAN_B200_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define PACMAN_B200_API __attribute__((visibility("default")))
@@ -94,15 +94,28 @@ typedef struct pacman_b200_stats {
   int64_t kernel_launches;  /* this library's kernel launches in the call */
   double ms_factor;         /* device time of the dense factorisations */
   double factor_flops;      /* algorithmic FLOPs of those factorisations */
-  /* With PACMAN_B200_TIME_KERNELS: summed CUDA-event duration, algorithmic
-   * FLOPs (2 * 64^3 per tile product) and launch count of the trailing
-   * column update of the large-patch Cholesky (the dominant kernel). */
+  /* With PACMAN_B200_TIME_KERNELS: the step launches of the large-patch
+   * Cholesky (the dominant kernels), each bracketed by CUDA events on its
+   * own stream: the span of device time during which at least one of them
+   * runs (slot groups run concurrently on their streams, so this is the
+   * union of the launch intervals, not their sum), their algorithmic
+   * FP64-equivalent FLOPs (2 * 64^3 per tile product) and launch count. */
   double ms_update;
   double update_flops;
   int64_t update_launches;
   /* Patches solved from factorisations kept by an earlier execute
    * (PACMAN_B200_KEEP_FACTORS). */
   int64_t factors_reused;
+  /* The same three figures per kind of step launch: the column updates on
+   * the int8 tensor cores (k_col_step_oz) and those in FP64 (k_col_step). */
+  double ms_update_i8;
+  double update_flops_i8;
+  int64_t update_launches_i8;
+  double ms_update_f64;
+  double update_flops_f64;
+  int64_t update_launches_f64;
+  /* Host synchronisations (waits for the device) inside the call. */
+  int64_t host_syncs;
 } pacman_b200_stats;
 
 /* Fills the reference's defaults (50, 0.15, 0.1, FP64, current device). */
@@ -210,6 +223,17 @@ PACMAN_B200_API int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, i
 /* Per (patch, target) local interpolant values of the last execute, in the
  * order of the target membership lists, times n_fields. */
 PACMAN_B200_API int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local);
+
+/* Per-patch status words of the plan's last execute, K entries into host
+ * memory: which patches lost a polynomial axis, which were re-solved and
+ * why.  No counterpart in the reference, which has no per-patch checks
+ * after its LU (src/rbf_pum/solver/utils/serial_solve.hpp:76-84).  Bits: */
+#define PACMAN_B200_PATCH_DROPPED_AXIS 1 /* the linear polynomial lost an axis */
+#define PACMAN_B200_PATCH_NONFINITE 2    /* a non-finite local value */
+#define PACMAN_B200_PATCH_BREAKDOWN 4    /* non-positive Cholesky pivot (mixed) */
+#define PACMAN_B200_PATCH_TIMEOUT 8      /* a bounded tensor-core pipeline wait gave up */
+#define PACMAN_B200_PATCH_RESOLVED 16    /* re-solved by the FP64 LU after 2, 4 or 8 */
+PACMAN_B200_API int pacman_b200_plan_patch_status(const pacman_b200_plan *plan, int32_t *status);
 
 /*
  * Finite-element transfer of the reference's PACMAN::fe_interpolate

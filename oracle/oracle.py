@@ -52,9 +52,11 @@ def _load():
         lib.orc_tgt_csr.argtypes = [ctypes.c_void_p, _i64p, _i32p]
         lib.orc_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _f64p,
                                   ctypes.c_int, ctypes.c_int64, _f64p, _f64p, _i64p,
-                                  ctypes.c_int64, _i64p]
+                                  ctypes.c_int64, _i64p, _i32p]
         lib.orc_solve.restype = ctypes.c_int
         lib.orc_weight_sums.argtypes = [ctypes.c_void_p, _f64p]
+        lib.orc_poly_dropped.argtypes = [ctypes.c_void_p, _i32p]
+        lib.orc_poly_dropped.restype = ctypes.c_int
         lib.orc_wendland.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
         lib.orc_wendland.restype = ctypes.c_double
         lib.orc_set_threads.argtypes = [ctypes.c_int]
@@ -140,6 +142,14 @@ class OraclePlan:
         self._lib.orc_weight_sums(self._h, _ptr(out))
         return out
 
+    def poly_dropped(self) -> np.ndarray:
+        """Per patch: does its polynomial block drop an axis (bool, K)."""
+        out = np.zeros(max(self.num_patches, 1), dtype=np.int32)
+        rc = self._lib.orc_poly_dropped(self._h, _ptr(out, _i32p))
+        if rc != 0:
+            raise RuntimeError(f"oracle poly_dropped failed ({rc})")
+        return out[: self.num_patches].astype(bool)
+
     def solve(self, basis, values, support_radius=0.1, patch_list=None, want_local=False):
         """Returns (out[m, F] or out[m], local or None, stats dict)."""
         vals = np.ascontiguousarray(values, dtype=np.float64)
@@ -152,6 +162,7 @@ class OraclePlan:
         if want_local:
             local = np.zeros((max(self._lib.orc_tgt_nnz(self._h), 1), F), dtype=np.float64)
         stats = np.zeros(8, dtype=np.int64)
+        dropped = np.zeros(max(self.num_patches, 1), dtype=np.int32)
         pl = None
         npl = 0
         if patch_list is not None:
@@ -160,11 +171,12 @@ class OraclePlan:
         rc = self._lib.orc_solve(self._h, int(basis), float(support_radius), _ptr(vals2), F, F,
                                  _ptr(out), _ptr(local) if local is not None else None,
                                  _ptr(pl, _i64p) if pl is not None else None, npl,
-                                 _ptr(stats, _i64p))
+                                 _ptr(stats, _i64p), _ptr(dropped, _i32p))
         if rc != 0:
             raise RuntimeError(f"oracle solve failed ({rc}): {self._lib.orc_last_error().decode()}")
         st = dict(dropped_axis_patches=int(stats[0]), sum_n3=int(stats[1]), max_n=int(stats[2]),
-                  sum_n=int(stats[3]), sum_m=int(stats[4]))
+                  sum_n=int(stats[3]), sum_m=int(stats[4]),
+                  dropped=dropped[: self.num_patches].astype(bool))
         if local is not None:
             local = local[: self._lib.orc_tgt_nnz(self._h)]
         return (out[:, 0] if squeeze else out), local, st

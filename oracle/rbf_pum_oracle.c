@@ -660,6 +660,73 @@ static void fill_poly(double *P, int64_t rows, const double *pts, const int32_t 
 }
 
 /* One patch: solver.hpp:217-286 for F fields; writes local[m x F]. */
+/* SerialFillQ with the SVD condition loop (serial_ops.hpp:108-139): while
+ * sigma_max / max(sigma_min, eps) of Q = [1, x_active] exceeds 1e5, drop the
+ * active axis with the smallest coordinate range (SerialDeactivateOneAxis,
+ * serial_ops.hpp:28-57).  Q is n x 4 scratch; active[] and *pv are updated.
+ * Returns 1 if an axis was dropped. */
+static int poly_axes(const orc_plan *p, int64_t k, double *Q, int active[3], int *pv_io) {
+  const int dim = p->dim;
+  const int64_t n = p->soff[k + 1] - p->soff[k];
+  const int32_t *si = p->sidx + p->soff[k];
+  int pv = *pv_io, dropped = 0;
+  int act[3], nact;
+  for (;;) {
+    nact = 0;
+    for (int a = 0; a < dim; ++a) if (active[a]) act[nact++] = a;
+    if (pv <= 1) break;
+    fill_poly(Q, n, p->src, si, act, nact);
+    double sig[4];
+    singular_values(Q, n, pv, sig);
+    const double cond = sig[0] / fmax(sig[pv - 1], ORC_EPS);
+    if (!(cond > ORC_COND_MAX)) break;
+    double range[3];
+    for (int a = 0; a < dim; ++a) {
+      if (!active[a]) { range[a] = DBL_MAX; continue; }
+      double mn = p->src[3 * (int64_t)si[0] + a], mx = mn;
+      for (int64_t i = 1; i < n; ++i) {
+        const double v = p->src[3 * (int64_t)si[i] + a];
+        if (v < mn) mn = v;
+        if (mx < v) mx = v;
+      }
+      range[a] = fabs(mx - mn);
+    }
+    double mn = DBL_MAX;
+    int mi = 0;
+    for (int a = 0; a < dim; ++a) if (range[a] < mn) { mn = range[a]; mi = a; }
+    active[mi] = 0;
+    --pv;
+    dropped = 1;
+  }
+  *pv_io = pv;
+  return dropped;
+}
+
+int orc_poly_dropped(const orc_plan *p, int32_t *out) {
+  int err = 0;
+#pragma omp parallel
+  {
+    double *Q = NULL;
+    int64_t cap = 0;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t k = 0; k < p->K; ++k) {
+      const int64_t n = p->soff[k + 1] - p->soff[k];
+      if (n > cap) {
+        free(Q);
+        cap = n;
+        Q = (double *)malloc(sizeof(double) * (size_t)(4 * cap));
+        if (!Q) { err = 1; cap = 0; }
+      }
+      int active[3] = {1, 1, 1};
+      int pv = p->dim + 1;
+      out[k] = Q ? poly_axes(p, k, Q, active, &pv) : -1;
+    }
+    free(Q);
+  }
+  if (err) { set_err("poly_dropped: out of memory"); return -4; }
+  return 0;
+}
+
 static int solve_patch(const orc_plan *p, int64_t k, int basis, double rinv,
                        const double *vals, int F, int64_t ld, double *local,
                        work_t *w, int *dropped) {
@@ -682,39 +749,10 @@ static int solve_patch(const orc_plan *p, int64_t k, int basis, double rinv,
     for (int f = 0; f < F; ++f) B[(size_t)f * n + i] = vals[(int64_t)si[i] * ld + f];
   }
 
-  /* SerialFillQ with the SVD condition loop (serial_ops.hpp:108-139). */
   int active[3] = {1, 1, 1};
   int pv = dim + 1;
-  int act[3], nact;
-  for (;;) {
-    nact = 0;
-    for (int a = 0; a < dim; ++a) if (active[a]) act[nact++] = a;
-    if (pv <= 1) break;
-    fill_poly(Q, n, p->src, si, act, nact);
-    double sig[4];
-    singular_values(Q, n, pv, sig);
-    const double cond = sig[0] / fmax(sig[pv - 1], ORC_EPS);
-    if (!(cond > ORC_COND_MAX)) break;
-    /* SerialDeactivateOneAxis (serial_ops.hpp:28-57). */
-    double range[3];
-    for (int a = 0; a < dim; ++a) {
-      if (!active[a]) { range[a] = DBL_MAX; continue; }
-      double mn = p->src[3 * (int64_t)si[0] + a], mx = mn;
-      for (int64_t i = 1; i < n; ++i) {
-        const double v = p->src[3 * (int64_t)si[i] + a];
-        if (v < mn) mn = v;
-        if (mx < v) mx = v;
-      }
-      range[a] = fabs(mx - mn);
-    }
-    double mn = DBL_MAX;
-    int mi = 0;
-    for (int a = 0; a < dim; ++a) if (range[a] < mn) { mn = range[a]; mi = a; }
-    active[mi] = 0;
-    --pv;
-    *dropped = 1;
-  }
-  nact = 0;
+  if (poly_axes(p, k, Q, active, &pv)) *dropped = 1;
+  int act[3], nact = 0;
   for (int a = 0; a < dim; ++a) if (active[a]) act[nact++] = a;
 
   /* SerialSolveQR (serial_solve.hpp:46-67): Householder QR of Q, Q^T b,
@@ -892,7 +930,7 @@ static int64_t lower_bound_i32(const int32_t *a, int64_t n, int32_t v) {
 
 int orc_solve(const orc_plan *p, int basis, double support_radius, const double *vals,
               int F, int64_t ld, double *out, double *local_out,
-              const int64_t *plist, int64_t nplist, int64_t *stats) {
+              const int64_t *plist, int64_t nplist, int64_t *stats, int32_t *dropped_out) {
   if (basis < ORC_WENDLAND_C0 || basis > ORC_WENDLAND_C8) { set_err("unknown basis"); return -1; }
   if (F < 1 || F > 8) { set_err("nfields must be in [1, 8]"); return -1; }
   if (!(support_radius > 0.0)) { set_err("support radius must be > 0"); return -1; }
@@ -914,6 +952,7 @@ int orc_solve(const orc_plan *p, int basis, double support_radius, const double 
       if (solve_patch(p, k, basis, rinv, vals, F, ld, local + p->toff[k] * F, &w, &dropped)) err = 1;
       done[k] = 1;
       ndrop += dropped;
+      if (dropped_out) dropped_out[k] = dropped;
       const int64_t n = p->soff[k + 1] - p->soff[k];
       s3 += n * n * n;
       sn += n;

@@ -57,11 +57,18 @@ void orc_tgt_csr(const orc_plan *plan, int64_t *offsets, int32_t *indices);
  * patch_list (optional) restricts the solve to the listed patches (used to
  * time a bounded sample); out then only holds their contributions.
  * stats (optional, 8 entries): [0] patches whose polynomial basis lost an
- * axis, [1] sum n^3, [2] max n, [3] sum n, [4] sum m, [5..7] reserved. */
+ * axis, [1] sum n^3, [2] max n, [3] sum n, [4] sum m, [5..7] reserved.
+ * dropped (optional, K entries): 1 for each solved patch whose polynomial
+ * basis lost an axis, 0 for the other solved patches (others untouched). */
 int orc_solve(const orc_plan *plan, int basis, double support_radius,
               const double *vals, int nfields, int64_t ld_vals, double *out,
               double *local, const int64_t *patch_list, int64_t n_patch_list,
-              int64_t *stats);
+              int64_t *stats, int32_t *dropped);
+
+/* Per patch, 1 if the polynomial block of its solve drops an axis
+ * (serial_ops.hpp:108-139; the decision depends on the sources only), else
+ * 0: K entries. */
+int orc_poly_dropped(const orc_plan *plan, int32_t *out);
 
 /* Partition-of-unity weights of every target (solver.hpp:137-168):
  * per target t, the sum S_t of the un-normalised Wendland C2 weights of all

@@ -64,6 +64,13 @@ class Stats(ctypes.Structure):
         ("update_flops", ctypes.c_double),
         ("update_launches", ctypes.c_int64),
         ("factors_reused", ctypes.c_int64),
+        ("ms_update_i8", ctypes.c_double),
+        ("update_flops_i8", ctypes.c_double),
+        ("update_launches_i8", ctypes.c_int64),
+        ("ms_update_f64", ctypes.c_double),
+        ("update_flops_f64", ctypes.c_double),
+        ("update_launches_f64", ctypes.c_int64),
+        ("host_syncs", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -108,6 +115,7 @@ SIGNATURES = {
     "pacman_b200_plan_centers": (ctypes.c_int, [_VP, _VP]),
     "pacman_b200_plan_patch_lists": (ctypes.c_int, [_VP, ctypes.c_int32, _VP, _VP]),
     "pacman_b200_plan_local_values": (ctypes.c_int, [_VP, _VP]),
+    "pacman_b200_plan_patch_status": (ctypes.c_int, [_VP, _VP]),
     "pacman_b200_plan_shard": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "pacman_b200_fe_interpolate": (ctypes.c_int, [
         ctypes.c_int32, ctypes.c_int32, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_int64, _VP, _VP,

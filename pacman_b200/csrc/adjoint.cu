@@ -311,7 +311,7 @@ void adjoint(Plan &p, const double *gout, double *grad_values, double *grad_targ
   if (grad_values) PB_CUDA(cudaMemsetAsync(grad_values, 0, sizeof(double) * N * F, st));
   if (grad_targets) PB_CUDA(cudaMemsetAsync(grad_targets, 0, sizeof(double) * M * p.dim, st));
   if (p.K == 0 || M == 0 || N == 0) {
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
     return;
   }
   const double r = p.radius, rinv = 1.0 / r;
@@ -358,7 +358,7 @@ void adjoint(Plan &p, const double *gout, double *grad_values, double *grad_targ
     }
   }
   PB_CUDA(cudaGetLastError());
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
 }
 
 }  // namespace pacman_b200

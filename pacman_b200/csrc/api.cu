@@ -29,6 +29,11 @@ int64_t &launch_counter() {
   return c;
 }
 
+int64_t &host_sync_counter() {
+  static thread_local int64_t c = 0;
+  return c;
+}
+
 namespace {
 thread_local std::string g_last_error;
 }  // namespace
@@ -189,9 +194,10 @@ int create_plan(int32_t dim, const double *src, int64_t n, const double *tgt, in
       InBuf s, t;
       s.stage(src, size_t(n) * dim, p.device, p.stream);
       t.stage(tgt, size_t(m) * dim, p.device, p.stream);
-      const int64_t l0 = launch_counter();
+      const int64_t l0 = launch_counter(), h0 = host_sync_counter();
       build_geometry(p, s.ptr, t.ptr);
       p.launches_geometry = launch_counter() - l0;
+      p.syncs_geometry = host_sync_counter() - h0;
     }
   } catch (const Error &e) {
     delete h;
@@ -219,7 +225,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
     PB_CUDA(cudaEventCreate(&e1));
     PB_CUDA(cudaEventCreate(&e2));
     PB_CUDA(cudaEventRecord(e0, st));
-    const int64_t launches0 = launch_counter();
+    const int64_t launches0 = launch_counter(), syncs0 = host_sync_counter();
     p.saved_basis = -1;
     SolveReport rep;
     if (p.m > 0) {
@@ -251,7 +257,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       PB_CUDA(cudaEventRecord(e1, st));
     }
     PB_CUDA(cudaEventRecord(e2, st));
-    PB_CUDA(cudaEventSynchronize(e2));
+    PB_CUDA(host_sync_event(e2));
     PB_CUDA(cudaGetLastError());
     if (flags & PACMAN_B200_SAVE_FOR_ADJOINT) {
       p.saved_basis = basis;
@@ -278,11 +284,18 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       stats->ms_solve = ms_solve;
       stats->ms_total = ms_total;
       stats->kernel_launches = launch_counter() - launches0 + p.launches_geometry;
+      stats->host_syncs = host_sync_counter() - syncs0 + p.syncs_geometry;
       stats->ms_factor = rep.ms_factor;
       stats->factor_flops = rep.factor_flops;
       stats->ms_update = rep.ms_update;
       stats->update_flops = rep.update_flops;
       stats->update_launches = rep.update_launches;
+      stats->ms_update_i8 = rep.ms_kind[1];
+      stats->update_flops_i8 = rep.flops_kind[1];
+      stats->update_launches_i8 = rep.launches_kind[1];
+      stats->ms_update_f64 = rep.ms_kind[0];
+      stats->update_flops_f64 = rep.flops_kind[0];
+      stats->update_launches_f64 = rep.launches_kind[0];
       stats->factors_reused = rep.factors_reused;
     }
     cudaEventDestroy(e0);
@@ -543,7 +556,7 @@ void solve_group(const pacman_b200_problem *qs, const std::vector<int> &ids,
     PB_CUDA(cudaMemcpyAsync(q.target_values, h, sizeof(double) * size_t(p.m) * q.n_fields,
                             cudaMemcpyDeviceToHost, st));
   }
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   g.stream = st;  // merged buffers are freed stream-ordered on the batch stream
 }
 
@@ -573,7 +586,7 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
     PB_CUDA(cudaEventCreate(&e1));
     PB_CUDA(cudaEventCreate(&e2));
     PB_CUDA(cudaEventRecord(e0, st));
-    const int64_t launches0 = launch_counter();
+    const int64_t launches0 = launch_counter(), syncs0 = host_sync_counter();
     // Geometry per problem on a few host threads, each with its own stream:
     // the geometry phase waits on the device several times, and the threads
     // overlap those waits and the small launches of different problems.
@@ -618,7 +631,7 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
     SolveReport rep;
     for (const auto &ids : groups) solve_group(qs, ids, plans, o, st, ds.dev, rep);
     PB_CUDA(cudaEventRecord(e2, st));
-    PB_CUDA(cudaEventSynchronize(e2));
+    PB_CUDA(host_sync_event(e2));
     PB_CUDA(cudaGetLastError());
     if (stats) {
       float ms_solve = 0.f, ms_total = 0.f;
@@ -644,11 +657,19 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
       stats->ms_total = ms_total;
       stats->kernel_launches = launch_counter() - launches0;
       for (int32_t i = 0; i < count; ++i) stats->kernel_launches += plans[i].h->p.launches_geometry;
+      stats->host_syncs = host_sync_counter() - syncs0;
+      for (int32_t i = 0; i < count; ++i) stats->host_syncs += plans[i].h->p.syncs_geometry;
       stats->ms_factor = rep.ms_factor;
       stats->factor_flops = rep.factor_flops;
       stats->ms_update = rep.ms_update;
       stats->update_flops = rep.update_flops;
       stats->update_launches = rep.update_launches;
+      stats->ms_update_i8 = rep.ms_kind[1];
+      stats->update_flops_i8 = rep.flops_kind[1];
+      stats->update_launches_i8 = rep.launches_kind[1];
+      stats->ms_update_f64 = rep.ms_kind[0];
+      stats->update_flops_f64 = rep.flops_kind[0];
+      stats->update_launches_f64 = rep.launches_kind[0];
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -741,7 +762,7 @@ int pacman_b200_plan_adjoint(pacman_b200_plan *plan, const double *grad_out, dou
     adjoint(p, g.ptr, dv, dt);
     if (hv) PB_CUDA(cudaMemcpyAsync(grad_values, dv, sizeof(double) * p.n * F, cudaMemcpyDeviceToHost, st));
     if (ht) PB_CUDA(cudaMemcpyAsync(grad_targets, dt, sizeof(double) * p.m * p.dim, cudaMemcpyDeviceToHost, st));
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
   } catch (const Error &e) {
     return fail(e.code, e.msg);
   }
@@ -787,7 +808,7 @@ int pacman_b200_plan_centers(const pacman_b200_plan *plan, double *centers) {
     if (p.K)
       PB_CUDA(cudaMemcpyAsync(c.data(), p.centers.p, sizeof(double4) * p.K,
                               cudaMemcpyDeviceToHost, p.stream));
-    PB_CUDA(cudaStreamSynchronize(p.stream));
+    PB_CUDA(host_sync(p.stream));
     std::vector<double> h(size_t(p.K) * p.dim);
     for (int k = 0; k < p.K; ++k) {
       const double v[3] = {c[k].x, c[k].y, c[k].z};
@@ -820,7 +841,7 @@ int pacman_b200_plan_patch_lists(const pacman_b200_plan *plan, int32_t which, in
     } else {
       offsets[0] = 0;
     }
-    PB_CUDA(cudaStreamSynchronize(p.stream));
+    PB_CUDA(host_sync(p.stream));
   } catch (const Error &e) {
     return fail(e.code, e.msg);
   }
@@ -834,10 +855,19 @@ int pacman_b200_plan_local_values(const pacman_b200_plan *plan, double *local) {
   try {
     DeviceScope ds(p.device);
     PB_CUDA(cudaMemcpyAsync(local, p.local.p, p.local.bytes, cudaMemcpyDefault, p.stream));
-    PB_CUDA(cudaStreamSynchronize(p.stream));
+    PB_CUDA(host_sync(p.stream));
   } catch (const Error &e) {
     return fail(e.code, e.msg);
   }
+  return 0;
+}
+
+int pacman_b200_plan_patch_status(const pacman_b200_plan *plan, int32_t *status) {
+  if (!plan || !status) return fail(PACMAN_B200_ERR_INVALID, "null argument");
+  const Plan &p = plan->p;
+  if (p.K > 0 && p.patch_status.size() != size_t(p.K))
+    return fail(PACMAN_B200_ERR_INVALID, "plan has not been executed");
+  for (int k = 0; k < p.K; ++k) status[k] = p.patch_status[size_t(k)];
   return 0;
 }
 
@@ -897,7 +927,7 @@ int pacman_b200_fe_interpolate(int32_t dim, int32_t method, const double *src, i
       if (!out_dev)
         PB_CUDA(cudaMemcpyAsync(out, o_dev, sizeof(double) * size_t(m), cudaMemcpyDeviceToHost,
                                 st));
-      PB_CUDA(cudaStreamSynchronize(st));
+      PB_CUDA(host_sync(st));
     }
     if (own) {
       cudaStreamDestroy(own);
@@ -935,7 +965,7 @@ int pacman_b200_plan_owned_targets(const pacman_b200_plan *plan, int64_t *count,
     if (sharded) {
       PB_CUDA(cudaMemcpyAsync(owned, p.tlist.p, sizeof(int32_t) * size_t(*count),
                               cudaMemcpyDefault, p.stream));
-      PB_CUDA(cudaStreamSynchronize(p.stream));
+      PB_CUDA(host_sync(p.stream));
     } else {
       for (int64_t i = 0; i < *count; ++i) owned[i] = int32_t(i);
     }

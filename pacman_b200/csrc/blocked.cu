@@ -687,6 +687,14 @@ static void set_smem_attributes() {
 // next wave reuses it.
 void destroy_factor_cache(FactorCache *c) { delete c; }
 
+int pipeline_wait_limit() {
+  if (const char *e = std::getenv("PACMAN_B200_WAIT_LIMIT")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v >= 1) return int(std::min<long>(v, 1l << 30));
+  }
+  return 1 << 22;
+}
+
 void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
                const std::vector<int> &patches, double *local, int *status, SolveReport &rep,
                const BigExtra &extra, FactorCache *keep) {
@@ -721,6 +729,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   a.act_out = extra.act_out;
   a.h = extra.h;
   a.g_out = extra.g_out;
+  a.wait_limit = pipeline_wait_limit();
   const bool adjoint = extra.mode == kBigAdjoint;
   if (adjoint) lu = false;
   if (!lu) chol_set_smem_attributes();
@@ -753,7 +762,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
   while (pos < order.size()) {
     if (keep && pos > 0) {
       // Kept waves stay allocated: size the next one by what is left.
-      PB_CUDA(cudaStreamSynchronize(st));
+      PB_CUDA(host_sync(st));
       PB_CUDA(cudaMemGetInfo(&free_b, &total_b));
       budget = std::max<size_t>(size_t(1) << 28, size_t(double(free_b) * 0.6)) / 8;
     }
@@ -832,9 +841,20 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       a.zc = dzc.as<double>();
     }
     a.slices = nullptr;
+    a.dpart = nullptr;
+    a.dcount = nullptr;
+    DevMem ddiag;
     if (oz && tot_sl > 0) {
       dsl.alloc(size_t(tot_sl), st);
       a.slices = dsl.as<uint8_t>();
+      // The int8 steps' diagonal-tile hand-over: a TB x TB part and an
+      // arrival counter per slot (counters start at zero, the finishing CTA
+      // of each step puts its slot's back to zero).
+      const size_t part_bytes = sizeof(double) * TB * TB * size_t(ns);
+      ddiag.alloc(part_bytes + sizeof(int) * size_t(ns), st);
+      a.dpart = ddiag.as<double>();
+      a.dcount = reinterpret_cast<int *>(ddiag.as<char>() + part_bytes);
+      PB_CUDA(cudaMemsetAsync(a.dcount, 0, sizeof(int) * size_t(ns), st));
     }
     const size_t n_inv = lu ? size_t(2) * TB * TB * ns : size_t(tot_inv);
     const size_t n_beta = size_t(4) * kMaxF * ns;
@@ -868,7 +888,6 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       const char *genv = std::getenv("PACMAN_B200_GROUPS");
       int G = std::min<int>(AuxStreams::kN, std::max(1, ns / 8));
       if (genv) G = std::min<int>(AuxStreams::kN, std::max(1, std::atoi(genv)));
-      if (rep.time_kernels) G = 1;
       std::vector<std::vector<BigSlot>> gs(G);
       for (int q = 0; q < ns; ++q) gs[q % G].push_back(slots[q]);
       std::vector<CholPlan> gp(G);
@@ -981,6 +1000,7 @@ void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, in
   a.alpha_out = extra.alpha_out;
   a.beta_out = extra.beta_out;
   a.act_out = extra.act_out;
+  a.wait_limit = pipeline_wait_limit();
   DevMem dalpha;
   if (extra.alpha_out != nullptr) {
     a.alpha_c = extra.alpha_out;

@@ -167,7 +167,15 @@ struct BigArgs {
   uint8_t *slices;     // mixed forward: int8 slices of the L tiles, or null (FP64 updates)
   double oz_mul;       // 128 / sigma (sigma bounds |L|)
   double oz_sig2;      // sigma^2
+  int wait_limit;      // polls of a tensor-core pipeline wait before it gives up
+  double *dpart;       // mixed forward: per slot, the diagonal CTA's part of the next diagonal tile (TB x TB)
+  int *dcount;         // mixed forward: per slot, arrivals at the next diagonal tile (zero between steps)
 };
+
+// Polls of a tensor-core pipeline wait (mbarrier) before the step gives up
+// and marks its patch for the FP64 LU: 2^22, or PACMAN_B200_WAIT_LIMIT (a
+// test shortens it to exercise that path).
+int pipeline_wait_limit();
 
 // Left-looking Cholesky steps, backward sweep and local evaluation of one
 // wave of slots (cholesky.cu).  `pre` holds, per step, the prefix counts of
@@ -177,6 +185,7 @@ struct CholPlan {
   std::vector<int> cnt;      // active slots per step
   std::vector<int> off;      // per step: offset of its prefix arrays in pre
   std::vector<int> pre;      // per step: prefix of the CTA counts (cnt+1)
+  std::vector<int> ioff;     // per step: offset in pre of the item prefix counts (cnt+1)
 };
 CholPlan chol_prefix(const std::vector<BigSlot> &slots);
 void chol_set_smem_attributes();

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "blocked.cuh"
@@ -116,10 +117,10 @@ __device__ __forceinline__ void sync_all() { __syncthreads(); }
 // columns of the residual tile at rg (row stride rld), overwritten with y; X
 // goes to gi (row stride TB).  Xs (TB x LDS), cv, dis and ys are shared
 // scratch.  Returns true on a non-positive pivot.
-__device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, double *gi,
-                          double *Xs,
-                          double (*cv)[TB], double *dis, double (*ys)[kMaxF]) {
-  const int tid = threadIdx.x;
+template <class Sync>
+__device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F, double *gi,
+                            double *Xs, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
+                            int tid, Sync sync) {
   const int bi = tid >> 4, bs = tid & 15;
   bool bad = false;
   double v[4][4];
@@ -134,7 +135,7 @@ __device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, d
   }
   for (int e = tid; e < TB * kMaxF; e += 256) {
     const int r = e / kMaxF, f = e % kMaxF;
-    ys[r][f] = f < F ? rg[int64_t(r) * rld + f] : 0.0;
+    ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
   }
   for (int p = 0; p < TB; ++p) {
     double *c = cv[p & 1];
@@ -161,7 +162,7 @@ __device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, d
           c[4 * bi + r] = x;
         }
     }
-    __syncthreads();
+    sync();
     const double piv = c[p];
     bad |= !(piv > 0.0);
     const double inv = 1.0 / piv;
@@ -187,7 +188,7 @@ __device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, d
 #pragma unroll
     for (int r = 0; r < 4; ++r) dis[4 * bi + r] = 1.0 / sqrt(v[r][r]);
   }
-  __syncthreads();
+  sync();
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i = 4 * bi + r;
@@ -198,7 +199,7 @@ __device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, d
       Xs[i * LDS + sc] = sc < i ? v[r][b] * di : (sc == i ? di : 0.0);
     }
   }
-  __syncthreads();
+  sync();
   // y_j = X r_j (first F columns of the residual tile).
   double yv[2];
   int ny = 0;
@@ -216,6 +217,13 @@ __device__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F, d
         *reinterpret_cast<const double2 *>(Xs + r * LDS + 2 * c2);
   }
   return bad;
+}
+
+__device__ __forceinline__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F,
+                                          double *gi, double *Xs, double (*cv)[TB], double *dis,
+                                          double (*ys)[kMaxF]) {
+  return diag_tile_t(g, ld, rg, rld, F, gi, Xs, cv, dis, ys, int(threadIdx.x),
+                     [] { __syncthreads(); });
 }
 
 // The diagonal tile of step 0 of every slot.
@@ -340,12 +348,18 @@ constexpr int kOzSLOff = 40 * 1024;                   // phase 3: L[j+1, j] (TB 
 constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
 constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
+// Polls of the waits that drain a pipeline after it gave up: they wait for
+// copies and tensor-core operations already issued, which complete by
+// themselves, so they get a longer limit than the pipeline waits
+// (BigArgs::wait_limit) and are never shortened.
+constexpr int kOzDrainLimit = 1 << 24;
 
 static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
 static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzGenOff, "staging overlaps the tile");
 static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the tile");
 static_assert(kOzSLOff >= (TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps X");
-static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 8 <= 256, "barrier area");
+static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 16 <= 256, "barrier area");
+static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the diagonal tile");
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -358,17 +372,36 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-// Bounded wait for the phase with the given parity; false on time-out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
-  uint32_t done = 0;
-  for (int it = 0; it < kOzWaitLimit && !done; ++it)
-    asm volatile(
-        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        "selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(saddr(b)), "r"(parity)
-        : "memory");
+__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *b, uint32_t cnt) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(b)),
+               "r"(cnt)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
   return done != 0;
+}
+// Bounded wait for the phase with the given parity; false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int limit = kOzWaitLimit) {
+  bool done = false;
+  for (int it = 0; it < limit && !done; ++it) done = mbar_try(b, parity);
+  return done;
+}
+// Pipeline wait of the int8 K loop: bounded by `limit` polls, and given up
+// at once when the other side of the pipeline has aborted.
+__device__ __forceinline__ bool mbar_wait_pipe(uint64_t *b, uint32_t parity, int limit,
+                                               volatile int *abort_flag) {
+  for (int it = 0; it < limit; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if (*abort_flag) return false;
+  }
+  return false;
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *b) {
   asm volatile(
@@ -418,10 +451,18 @@ struct OzBars {
 // the first slice tile of their tile row (tiles of a row are consecutive in
 // p).  Thread 0 issues the bulk copies, thread 32 the MMAs; every thread
 // returns after the MMAs completed.  Threads 64.. run side(t, nt) meanwhile.
-// false if a wait timed out.
+//
+// Every pipeline wait is bounded by `limit` polls.  When one gives up, the
+// thread raises the CTA's abort flag and the other side stops at its next
+// wait; then the copies already issued (the latest use of each stage) and
+// the MMAs already issued (the final commit) are waited for with the longer
+// drain limit, so that nothing is still writing shared memory or TMEM when
+// the CTA goes on or exits.  Returns false, on every thread, if the loop was
+// aborted.
 template <class Side>
-__device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint8_t *rA0,
-                         const uint8_t *rA1, const uint8_t *rB, int nump, Side side) {
+__device__ bool oz_kloop(uint8_t *stages, OzBars *bar, volatile int *abort_flag, uint32_t tmem,
+                         const uint8_t *rA0, const uint8_t *rA1, const uint8_t *rB, int nump,
+                         int limit, Side side) {
   const int tid = threadIdx.x;
   // Earlier generic writes to the stage area before the async-proxy copies.
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -431,17 +472,21 @@ __device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint
       mbar_init(&bar->empty[i], 1);
     }
     mbar_init(&bar->done, 1);
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  bool ok = true;
   const int nh = 2 * nump;  // K = 32 halves of the column tiles
   if (tid == 0) {
     const uint32_t bytes = uint32_t((rA1 ? 2 : 1) * kOzTileBytes / 2 + kOzTileBytes / 2);
-    for (int hh = 0; hh < nh && ok; ++hh) {
+    int issued = 0;
+    for (int hh = 0; hh < nh; ++hh) {
       const int st = hh % kOzStages, u = hh / kOzStages;
-      if (hh >= kOzStages) ok = mbar_wait(&bar->empty[st], uint32_t((u - 1) & 1));
-      if (!ok) break;
+      if (hh >= kOzStages && !mbar_wait_pipe(&bar->empty[st], uint32_t((u - 1) & 1), limit,
+                                             abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
       uint8_t *sA = stages + st * kOzStage;
       uint8_t *sB = sA + kOzStageA;
       mbar_expect_tx(&bar->full[st], bytes);
@@ -453,12 +498,22 @@ __device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint
         if (a1) bulk_g2s(sA + (cs * 16 + 8) * 128, a1 + cs * 1024, 1024, &bar->full[st]);
       }
       bulk_g2s(sB, rB + toff, 2 * kOzS * 1024, &bar->full[st]);
+      issued = hh + 1;
+    }
+    // Drain: an earlier use of a stage was consumed before its stage was
+    // refilled, so only the latest use of each stage can still be in flight.
+    for (int st = 0; st < kOzStages && st < issued; ++st) {
+      const int last = st + kOzStages * ((issued - 1 - st) / kOzStages);
+      if (!mbar_wait(&bar->full[st], uint32_t((last / kOzStages) & 1), kOzDrainLimit))
+        *abort_flag = 1;
     }
   } else if (tid == 32) {
-    for (int hh = 0; hh < nh && ok; ++hh) {
+    for (int hh = 0; hh < nh; ++hh) {
       const int st = hh % kOzStages, u = hh / kOzStages;
-      ok = mbar_wait(&bar->full[st], uint32_t(u & 1));
-      if (!ok) break;
+      if (!mbar_wait_pipe(&bar->full[st], uint32_t(u & 1), limit, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
       tc_fence_after();
       const uint32_t sA = saddr(stages + st * kOzStage);
       const uint32_t sB = sA + kOzStageA;
@@ -476,14 +531,15 @@ __device__ bool oz_kloop(uint8_t *stages, OzBars *bar, uint32_t tmem, const uint
       }
       umma_commit(&bar->empty[st]);
     }
-    umma_commit(&bar->done);
+    umma_commit(&bar->done);  // arrives once every MMA issued above has completed
   } else if (tid >= 64) {
     side(tid - 64, int(blockDim.x) - 64);  // warps 2.. are free during the K loop
   }
   __syncthreads();
-  if (!mbar_wait(&bar->done, 0u)) ok = false;
+  if (!mbar_wait(&bar->done, 0u, kOzDrainLimit)) *abort_flag = 1;
   tc_fence_after();
-  return ok;
+  __syncthreads();
+  return *abort_flag == 0;
 }
 
 // Row r = 32 (warp % 4) + lane of the K loop's result, columns 32 h .. + 31
@@ -720,37 +776,104 @@ __global__ void __launch_bounds__(kColThreads, 2)
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
+// The next diagonal tile of a slot has two producers in the int8 step: the
+// diagonal CTA (D' = A[j+1, j+1] - the terms p < j) and row CTA 0 (L[j+1, j],
+// stored by its trsm).  Each writes its part to global memory and arrives on
+// the slot's counter; the second to arrive finishes the tile.  Nothing waits
+// on the other CTA: the first arrival just leaves, so the order in which the
+// CTAs are scheduled does not matter.  Returns true, on every thread, for the
+// second arrival, which also resets the counter for the next step's launch.
+__device__ __forceinline__ bool oz_diag_arrive(int *count, volatile int *flag) {
+  __threadfence();  // this thread's global writes, device-wide, before the arrival
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int old = atomicAdd(count, 1);
+    *flag = old;
+    if (old == 1) *count = 0;
+  }
+  __syncthreads();
+  const bool last = *flag == 1;
+  if (last) __threadfence();  // the partner's writes (fenced before its arrival) come first
+  return last;
+}
+
+// Finishes the diagonal tile j + 1 of a slot: Ds (shared, TB x LDS) holds
+// D' = A[j+1, j+1] - sum_{p<j} L[j+1, p] L[j+1, p]^T, or the CTA loads it
+// from the diagonal CTA's copy in a.dpart; then D = D' - L[j+1, j] L[j+1, j]^T
+// (FP64 tensor cores, L[j+1, j] read back from the workspace through L2),
+// and the inverse factor X_{j+1} and y_{j+1} = X_{j+1} r_{j+1} (diag_tile).
+// Data of the other CTA is read with L2 loads (ld.global.cg).
+__device__ void oz_finish_diag(const BigArgs &a, const BigSlot &sl, int j, uint8_t *smb,
+                               double *Ds, bool ds_from_global) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int ld = sl.ld;
+  double *W = a.W + sl.base;
+  double *rcol = W + int64_t(sl.T) * TB;
+  if (ds_from_global) {
+    const double *src = a.dpart + int64_t(sl.q) * TB * TB;
+    for (int e = tid; e < TB * TB; e += kColThreads) Ds[(e >> 6) * LDS + (e & 63)] = __ldcg(src + e);
+  }
+  double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
+  const double *lg = W + int64_t(j + 1) * TB * ld + int64_t(j) * TB;
+  for (int e = tid; e < TB * TB; e += kColThreads)
+    sL[(e >> 6) * LDS + (e & 63)] = __ldcg(lg + int64_t(e >> 6) * ld + (e & 63));
+  __syncthreads();
+  double acc[4][4][2];
+  if (wr < TB) {
+    acc_load(acc, Ds, LDS, wr, wc, lane);
+    mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
+  }
+  __syncthreads();
+  if (wr < TB) acc_store(acc, Ds, LDS, wr, wc, lane);
+  __syncthreads();
+  double *Xs = reinterpret_cast<double *>(smb);
+  double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
+  double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
+  double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
+  const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, a.F,
+                             a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
+  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+}
+
 // Step j of the factorisation with the column update on the int8 tensor cores
-// (same work split as k_col_step; one CTA per SM: the K loop holds 448 TMEM
-// columns).  Phase 2 also writes the int8 slices of the new L tiles.
+// (one CTA per SM: the K loop holds 448 TMEM columns).  Blocks [0, cnt) are
+// the diagonal CTAs of the active slots, [cnt, 2 cnt) their row CTAs 0, then
+// the other row CTAs (prefix counts in pre).
+//  * Row CTA l owns row tiles i0 = j + 1 + 2 l and i0 + 1: C = A[i, j] -
+//    sigma^2 sum_l 128^-l Z_l over p < j (int8 K loop; warps 2.. evaluate
+//    A[i, j] meanwhile), L[i, j] = C X_j^T and the forward substitution
+//    (step_trsm), then the int8 slices of L[i, j].
+//  * The diagonal CTA forms D' = A[j+1, j+1] - the p < j terms by its own
+//    int8 K loop, concurrently with the row CTAs, and stores it.
+//  * Whichever of the diagonal CTA and row CTA 0 arrives second finishes
+//    the tile (oz_finish_diag) for step j + 1.
 __global__ void __launch_bounds__(kColThreads, 1)
     k_col_step_oz(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
                   int j) {
   extern __shared__ __align__(1024) uint8_t smb[];
   double *sm = reinterpret_cast<double *>(smb);
-  OzBars *bars = reinterpret_cast<OzBars *>(smb + kOzBarOff);           // phase 1
-  OzBars *bars3 = bars + 1;                                               // phase 3
+  OzBars *bars = reinterpret_cast<OzBars *>(smb + kOzBarOff);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smb + kOzBarOff + 2 * sizeof(OzBars));
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(smb + kOzBarOff + 2 * sizeof(OzBars) + 8);
+  volatile int *arrive_flag = abort_flag + 1;
+  const int b = blockIdx.x;
+  const bool diag = b < cnt;
   int q, l;
-  if (int(blockIdx.x) < cnt) {
-    q = blockIdx.x;
+  if (diag) {
+    q = b;
+    l = -1;
+  } else if (b < 2 * cnt) {
+    q = b - cnt;
     l = 0;
   } else {
-    const int b = blockIdx.x - cnt;
-    q = find_slot(pre, cnt, b);
-    l = 1 + b - pre[q];
+    const int bb = b - 2 * cnt;
+    q = find_slot(pre, cnt, bb);
+    l = 1 + bb - pre[q];
   }
   const BigSlot sl = slots[q];
-  const int i0 = j + 1 + 2 * l;
-  const bool two = i0 + 1 < sl.T;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  const int ld = sl.ld, F = a.F;
-  double *W = a.W + sl.base;
-  double *rcol = W + int64_t(sl.T) * TB;
-  const int arows = two ? kColRows : TB;
-  const bool active = two || wr < TB;
   auto slice_row = [&](int i) {
     return a.slices + sl.sli + (int64_t(i) * (i - 1) / 2) * kOzTileBytes;
   };
@@ -766,55 +889,19 @@ __global__ void __launch_bounds__(kColThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
-
-  // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l in sGen (kColRows x LDS); A[i, j]
-  //    is evaluated by warps 2.. while the K loop runs.
   double *sGen = reinterpret_cast<double *>(smb + kOzGenOff);
   double *pts = reinterpret_cast<double *>(smb + kOzPtsOff);
-  if (j > 0) {
-    ok = oz_kloop(smb, bars, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr, slice_row(j), j,
-                  [&](int t0, int nt) {
-                    gen_tile(a, sl, i0, j, arows, sGen, pts, t0, nt,
-                             [&] { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); });
-                  });
-  } else {
-    gen_tile(a, sl, i0, j, arows, sGen, pts, tid, kColThreads, sync_all);
-  }
-  {
-    const int r = 32 * (warp & 3) + lane, h = warp >> 2;
-    double v[32];
-    if (j > 0) oz_levels(tmem, v);
-    if (j > 0) tc_fence_before();
-    __syncthreads();
-    if (j > 0 && r < arows) {
-      double *Cr = sGen + r * LDS + 32 * h;
-#pragma unroll
-      for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
-    }
-  }
-  // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
-  double acc[4][4][2];
-  step_trsm(a, sl, j, i0, arows, active, sm, sGen, sm, acc);
-  uint8_t *stg = smb + kOzStgOff;
-  if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
-  __syncthreads();
-  for (int tt = 0; tt < arows / TB; ++tt) {
-    int4 *dst = reinterpret_cast<int4 *>(slice_row(i0 + tt) + int64_t(j) * kOzTileBytes);
-    const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
-    for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
-  }
+  auto side_sync = [] (int nt) { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); };
 
-  if (l == 0) {
-    // 3. The diagonal tile of step j + 1: D = A[j+1, j+1] - sigma^2 sum_l
-    //    128^-l Z_l (p < j, int8) - L[j+1, j] L[j+1, j]^T (FP64), factored.
-    __syncthreads();  // the staging area is copied out
-    double *Ds = sGen;  // A[j+1, j+1], then D
-    if (j > 0 && ok) {
+  if (diag) {
+    // D' = A[j+1, j+1] - sigma^2 sum_l 128^-l Z_l (p < j) in sGen.
+    double *Ds = sGen;
+    if (j > 0) {
       const uint8_t *rd = slice_row(j + 1);
-      ok = oz_kloop(smb, bars3, tmem, rd, nullptr, rd, j, [&](int t0, int nt) {
-        gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, t0, nt,
-                 [&] { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); });
-      });
+      ok = oz_kloop(smb, bars, abort_flag, tmem, rd, nullptr, rd, j, a.wait_limit,
+                    [&](int t0, int nt) {
+                      gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, t0, nt, [&] { side_sync(nt); });
+                    });
     } else {
       gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, tid, kColThreads, sync_all);
     }
@@ -830,28 +917,446 @@ __global__ void __launch_bounds__(kColThreads, 1)
         for (int c = 0; c < 32; ++c) Dr[c] = __fma_rn(-a.oz_sig2, v[c], Dr[c]);
       }
     }
-    // L[j+1, j] (stored in phase 2) into shared memory for the FP64 term.
-    double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
-    async_tile(sL, W + int64_t(j + 1) * TB * ld + int64_t(j) * TB, ld, tid, kColThreads);
-    cp_async_commit();
-    cp_async_wait<0>();
     __syncthreads();
-    if (wr < TB) {
-      acc_load(acc, Ds, LDS, wr, wc, lane);
-      mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
+    double *dst = a.dpart + int64_t(sl.q) * TB * TB;
+    for (int e = tid; e < TB * TB; e += kColThreads) dst[e] = Ds[(e >> 6) * LDS + (e & 63)];
+    if (oz_diag_arrive(a.dcount + sl.q, arrive_flag)) oz_finish_diag(a, sl, j, smb, Ds, false);
+  } else {
+    const int i0 = j + 1 + 2 * l;
+    const bool two = i0 + 1 < sl.T;
+    const int arows = two ? kColRows : TB;
+    const bool active = two || wr < TB;
+    // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l in sGen (kColRows x LDS);
+    //    A[i, j] is evaluated by warps 2.. while the K loop runs.
+    if (j > 0) {
+      ok = oz_kloop(smb, bars, abort_flag, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr,
+                    slice_row(j), j, a.wait_limit, [&](int t0, int nt) {
+                      gen_tile(a, sl, i0, j, arows, sGen, pts, t0, nt, [&] { side_sync(nt); });
+                    });
+    } else {
+      gen_tile(a, sl, i0, j, arows, sGen, pts, tid, kColThreads, sync_all);
     }
+    {
+      const int r = 32 * (warp & 3) + lane, h = warp >> 2;
+      double v[32];
+      if (j > 0) oz_levels(tmem, v);
+      if (j > 0) tc_fence_before();
+      __syncthreads();
+      if (j > 0 && r < arows) {
+        double *Cr = sGen + r * LDS + 32 * h;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
+      }
+    }
+    // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
+    double acc[4][4][2];
+    step_trsm(a, sl, j, i0, arows, active, sm, sGen, sm, acc);
+    uint8_t *stg = smb + kOzStgOff;
+    if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
     __syncthreads();
-    if (wr < TB) acc_store(acc, Ds, LDS, wr, wc, lane);
-    __syncthreads();
-    double *Xs = sm;
-    double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
-    double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
-    double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
-    const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
-                               a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
-    if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+    for (int tt = 0; tt < arows / TB; ++tt) {
+      int4 *dst = reinterpret_cast<int4 *>(slice_row(i0 + tt) + int64_t(j) * kOzTileBytes);
+      const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
+      for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
+    }
+    // 3. Row CTA 0 stored L[j+1, j]: its half of the next diagonal tile.
+    if (l == 0 && oz_diag_arrive(a.dcount + sl.q, arrive_flag))
+      oz_finish_diag(a, sl, j, smb, sGen, true);
   }
   if (tid == 0 && !ok) atomicOr(&a.status[sl.k], 8);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(kOzTmemCols)
+                 : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Warp-specialised int8 step (k_col_step_ws)
+// ---------------------------------------------------------------------------
+//
+// The same step as k_col_step_oz, organised so that the int8 K loop of one
+// item overlaps the FP64 epilogue of the previous one on the same SM.  An
+// item is one 64-row tile: row tile i of column j (C = A[i, j] - sum_{p<j}
+// L[i, p] L[j, p]^T, then L[i, j] = C X_j^T, the forward substitution and
+// the int8 slices of L[i, j]), or the diagonal item of a slot (D' of tile
+// j + 1).  Each CTA takes a contiguous range of the step's items.
+//   warp 0 (one thread): bulk copies of the slice half-tiles (K = 32) of the
+//     item's row tile and of the column tile row through a kWsStages ring;
+//   warp 1 (one thread): the tcgen05 MMAs into one TMEM accumulator;
+//   warps 2..9: per item the Wendland tile (during the K loop), the TMEM
+//     drain (after which the MMA thread starts the next item), the level
+//     combination and the FP64 epilogue.
+// The MMA operand A holds two consecutive slices of the ONE row tile (rows
+// 0..63 slice a, 64..127 slice a + 1: the stored tile layout is already the
+// tensor core's, so a half-tile is one contiguous 14 KB copy), B the slices
+// of the column tile stacked along N.  With the accumulator of pair (a, a+1)
+// starting at TMEM column group a - 1, column group g (64 columns) holds
+// level g + 2 in lanes 0..63 and level g + 3 in lanes 64..127 whatever the
+// pair, so four pairs (1,2), (3,4), (5,6), (7,-) and six MMAs per K = 32
+// cover every slice pair with a + b <= 8 (products of level 9, in lanes
+// 64..127 of group 6, and of the missing slice 8 are not read).
+constexpr int kWsStages = 3;
+constexpr int kWsHalf = 2 * kOzS * 1024;                 // 14336: one K = 32 half of a slice tile
+constexpr int kWsStage = 2 * kWsHalf;                    // A half + B half
+constexpr int kWsThreads = 320;                          // 2 issue warps + 8 epilogue warps
+constexpr int kWsCOff = kWsStages * kWsStage;            // C / D (TB x LDS doubles)
+constexpr int kWsXOff = kWsCOff + TB * LDS * 8;          // X_j, or diag_tile scratch
+constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // L[j+1, j] (finisher)
+constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // points of the evaluated tile
+constexpr int kWsRedOff = kWsPtsOff + 3 * 2 * TB * 8;    // y_j, reductions, diag_tile vectors
+constexpr int kWsBarOff = kWsRedOff + 3 * TB * kMaxF * 8;
+constexpr size_t kWsSmem = size_t(kWsBarOff) + 256;
+static_assert(kWsSmem <= 232448, "shared memory of k_col_step_ws");
+static_assert(kOzTileBytes <= TB * LDS * 8, "slice staging does not fit the C buffer");
+static_assert((TB * kMaxF + 2 * TB + TB) * 8 <= 3 * TB * kMaxF * 8, "diag_tile vectors");
+
+struct WsBars {
+  uint64_t full[kWsStages], empty[kWsStages], acc_full, acc_empty, done;
+  int abort_flag, arrive_flag, ep_stop;
+  uint32_t tmem;
+};
+static_assert(sizeof(WsBars) <= 256, "barrier area");
+
+// The item `it` of step j: slot q (prefix counts ipre over the cnt active
+// slots), and r = it - ipre[q]: r == 0 the diagonal item, else row tile j + r.
+struct WsItem {
+  int q, r;
+};
+__device__ __forceinline__ WsItem ws_item(const int *ipre, int cnt, int it) {
+  const int q = find_slot(ipre, cnt, it);
+  return {q, it - ipre[q]};
+}
+
+// Six MMAs of one K = 32 half: pairs (1,2), (3,4), (5,6), (7,-) of the row
+// tile's slices against the column tile's slices 1..8-a stacked along N.
+__device__ __forceinline__ void ws_mma_half(uint32_t tmem, uint32_t sA, uint32_t sB, bool first) {
+  constexpr uint32_t kLbo = kOzS * 1024;  // between the two 16-byte K chunks of a half
+  const uint64_t b0 = umma_desc(sB, kLbo, 128), b4 = umma_desc(sB + 4 * 1024, kLbo, 128);
+  const uint32_t acc = first ? 0u : 1u;
+  uint64_t ad = umma_desc(sA, kLbo, 128);                 // pair (1, 2): groups 0..6
+  umma_i8(tmem, ad, b0, umma_idesc_i8(256), acc);
+  umma_i8(tmem + 256, ad, b4, umma_idesc_i8(192), acc);
+  ad = umma_desc(sA + 2 * 1024, kLbo, 128);               // pair (3, 4): groups 2..6
+  umma_i8(tmem + 128, ad, b0, umma_idesc_i8(256), 1u);
+  umma_i8(tmem + 384, ad, b4, umma_idesc_i8(64), 1u);
+  ad = umma_desc(sA + 4 * 1024, kLbo, 128);               // pair (5, 6): groups 4..6
+  umma_i8(tmem + 256, ad, b0, umma_idesc_i8(192), 1u);
+  ad = umma_desc(sA + 6 * 1024, kLbo, 128);               // pair (7, -): group 6
+  umma_i8(tmem + 384, ad, b0, umma_idesc_i8(64), 1u);
+}
+
+// Epilogue warp e (warp 2 + e) reads TMEM lanes 32 qd .. + 31 (qd = warp % 4)
+// and columns 32 h .. + 31 (h = e / 4) of every column group: v[c] = the
+// level sum of its half of row r (lanes 0..63: levels g + 2, rows r = lane;
+// lanes 64..127: levels g + 3, rows r = lane - 64).
+__device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double (&v)[32]) {
+  const uint32_t lane_base = uint32_t(32 * qd) << 16;
+  const int up = qd >= 2 ? 1 : 0;
+#pragma unroll
+  for (int c = 0; c < 32; ++c) v[c] = 0.0;
+#pragma unroll
+  for (int g = 0; g < kOzS; ++g) {
+    if (up && g == kOzS - 1) break;  // level 9
+    uint32_t z[32];
+    const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(z[0]), "=r"(z[1]), "=r"(z[2]), "=r"(z[3]), "=r"(z[4]), "=r"(z[5]), "=r"(z[6]),
+          "=r"(z[7]), "=r"(z[8]), "=r"(z[9]), "=r"(z[10]), "=r"(z[11]), "=r"(z[12]), "=r"(z[13]),
+          "=r"(z[14]), "=r"(z[15])
+        : "r"(addr));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(z[16]), "=r"(z[17]), "=r"(z[18]), "=r"(z[19]), "=r"(z[20]), "=r"(z[21]),
+          "=r"(z[22]), "=r"(z[23]), "=r"(z[24]), "=r"(z[25]), "=r"(z[26]), "=r"(z[27]),
+          "=r"(z[28]), "=r"(z[29]), "=r"(z[30]), "=r"(z[31])
+        : "r"(addr + 16));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    const double sc = ldexp(1.0, -7 * (g + 2 + up));
+#pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = __fma_rn(double(int32_t(z[c])), sc, v[c]);
+  }
+}
+
+__device__ __forceinline__ void ws_sync() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+
+// oz_diag_arrive for the 256 epilogue threads (etid 0 arrives).
+__device__ __forceinline__ bool ws_diag_arrive(int *count, volatile int *flag, int etid) {
+  __threadfence();
+  ws_sync();
+  if (etid == 0) {
+    const int old = atomicAdd(count, 1);
+    *flag = old;
+    if (old == 1) *count = 0;
+  }
+  ws_sync();
+  const bool last = *flag == 1;
+  if (last) __threadfence();
+  return last;
+}
+
+__global__ void __launch_bounds__(kWsThreads, 1)
+    k_col_step_ws(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ ipre,
+                  int cnt, int j) {
+  extern __shared__ __align__(1024) uint8_t smb[];
+  WsBars *bar = reinterpret_cast<WsBars *>(smb + kWsBarOff);
+  volatile int *abort_flag = &bar->abort_flag;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nitems = ipre[cnt];
+  const int it0 = int(int64_t(blockIdx.x) * nitems / gridDim.x);
+  const int it1 = int(int64_t(blockIdx.x + 1) * nitems / gridDim.x);
+  const int nh = 2 * j;  // K = 32 halves per item
+  auto slice_row = [&](const BigSlot &sl, int i) {
+    return a.slices + sl.sli + (int64_t(i) * (i - 1) / 2) * kOzTileBytes;
+  };
+  if (tid == 0) {
+    for (int i = 0; i < kWsStages; ++i) {
+      mbar_init(&bar->full[i], 1);
+      mbar_init(&bar->empty[i], 1);
+    }
+    mbar_init(&bar->acc_full, 1);
+    mbar_init(&bar->acc_empty, 8);
+    mbar_init(&bar->done, 1);
+    bar->abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     saddr(&bar->tmem)),
+                 "r"(kOzTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = bar->tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // Producer.
+      int hc = 0;
+      for (int it = it0; it < it1 && !*abort_flag; ++it) {
+        const WsItem w = ws_item(ipre, cnt, it);
+        const BigSlot sl = slots[w.q];
+        const uint8_t *ra = slice_row(sl, w.r == 0 ? j + 1 : j + w.r);
+        const uint8_t *rb = slice_row(sl, w.r == 0 ? j + 1 : j);
+        for (int hh = 0; hh < nh; ++hh, ++hc) {
+          const int st = hc % kWsStages, u = hc / kWsStages;
+          if (hc >= kWsStages &&
+              !mbar_wait_pipe(&bar->empty[st], uint32_t((u - 1) & 1), a.wait_limit, abort_flag)) {
+            *abort_flag = 1;
+            break;
+          }
+          uint8_t *sA = smb + st * kWsStage;
+          const int64_t off = int64_t(hh >> 1) * kOzTileBytes + (hh & 1) * kWsHalf;
+          mbar_expect_tx(&bar->full[st], uint32_t(kWsStage));
+          bulk_g2s(sA, ra + off, kWsHalf, &bar->full[st]);
+          bulk_g2s(sA + kWsHalf, rb + off, kWsHalf, &bar->full[st]);
+        }
+      }
+      // Drain: only the latest use of each stage can still be in flight.
+      const int issued = hc;
+      for (int st = 0; st < kWsStages && st < issued; ++st) {
+        const int last = st + kWsStages * ((issued - 1 - st) / kWsStages);
+        if (!mbar_wait(&bar->full[st], uint32_t((last / kWsStages) & 1), kOzDrainLimit))
+          *abort_flag = 1;
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issue.
+      int hc = 0, k = 0;
+      bool ok = true;
+      for (int it = it0; it < it1 && ok; ++it, ++k) {
+        // The accumulator is free once the epilogue drained the previous item.
+        if (k > 0 && !mbar_wait_pipe(&bar->acc_empty, uint32_t((k - 1) & 1), a.wait_limit,
+                                     abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int hh = 0; hh < nh; ++hh, ++hc) {
+          const int st = hc % kWsStages, u = hc / kWsStages;
+          if (!mbar_wait_pipe(&bar->full[st], uint32_t(u & 1), a.wait_limit, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sA = saddr(smb + st * kWsStage);
+          ws_mma_half(tmem, sA, sA + kWsHalf, hh == 0);
+          umma_commit(&bar->empty[st]);
+        }
+        if (!ok) break;
+        umma_commit(&bar->acc_full);
+      }
+      if (!ok) *abort_flag = 1;
+      umma_commit(&bar->done);  // arrives once every MMA issued above has completed
+    }
+  } else {
+    // Epilogue: 8 warps, etid 0..255.
+    const int etid = tid - 64, ew = warp - 2;
+    const int qd = warp & 3, h = ew >> 2;
+    const int wr = (ew >> 1) * 32, wc = (ew & 1) * 32;  // trsm blocks (ew < 4)
+    double *sC = reinterpret_cast<double *>(smb + kWsCOff);
+    double *sX = reinterpret_cast<double *>(smb + kWsXOff);
+    double *sL = reinterpret_cast<double *>(smb + kWsLOff);
+    double *pts = reinterpret_cast<double *>(smb + kWsPtsOff);
+    double *ysh = reinterpret_cast<double *>(smb + kWsRedOff);  // TB x kMaxF
+    double *red = ysh + TB * kMaxF;                              // 2 x TB x kMaxF
+    volatile int *arrive_flag = &bar->arrive_flag;
+    volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
+    if (etid == 0) *ep_stop = 0;
+    ws_sync();
+    int xq = -1;  // slot whose X_j is in sX
+    int k = 0;
+    for (int it = it0; it < it1; ++it, ++k) {
+      const WsItem w = ws_item(ipre, cnt, it);
+      const BigSlot sl = slots[w.q];
+      const int ld = sl.ld, F = a.F;
+      double *W = a.W + sl.base;
+      double *rcol = W + int64_t(sl.T) * TB;
+      const bool diag = w.r == 0;
+      const int i = diag ? j + 1 : j + w.r;
+      if (!diag && xq != w.q) {
+        const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
+        for (int idx = etid; idx < TB * TB / 2; idx += 256) {
+          const int r = idx >> 5, c2 = idx & 31;
+          cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
+        }
+        cp_async_commit();
+        xq = w.q;
+      }
+      // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run.
+      gen_tile(a, sl, i, diag ? j + 1 : j, TB, sC, pts, etid, 256, ws_sync);
+      ws_sync();
+      // Drain the accumulator, then hand it back to the MMA thread.
+      double v[32];
+      // Every epilogue thread waits; the decision to stop is made uniform
+      // through ep_stop (the global abort flag may change at any time).
+      if (!mbar_wait_pipe(&bar->acc_full, uint32_t(k & 1), a.wait_limit, abort_flag)) *ep_stop = 1;
+      ws_sync();
+      if (*ep_stop) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      ws_drain(tmem, qd, h, v);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cnt(&bar->acc_empty, 1);
+      // C = A - sigma^2 (lower-lane levels + upper-lane levels), in two turns.
+      if (qd < 2) {
+        double *Cr = sC + (32 * qd + lane) * LDS + 32 * h;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
+      }
+      ws_sync();
+      if (qd >= 2) {
+        double *Cr = sC + (32 * (qd - 2) + lane) * LDS + 32 * h;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
+      }
+      ws_sync();
+      bool finish = false;
+      if (diag) {
+        double *dst = a.dpart + int64_t(sl.q) * TB * TB;
+        for (int e = etid; e < TB * TB; e += 256) dst[e] = sC[(e >> 6) * LDS + (e & 63)];
+        finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
+      } else {
+        // L[i, j] = C X_j^T (four warps), stored; forward substitution.
+        cp_async_wait<0>();
+        ws_sync();
+        double acc[4][4][2];
+        acc_zero(acc);
+        if (ew < 4) {
+          mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
+          acc_store(acc, W + int64_t(i) * TB * ld + int64_t(j) * TB, ld, wr, wc, lane);
+        }
+        {
+          const double *yg = rcol + int64_t(j) * TB * ld;
+          for (int e = etid; e < TB * kMaxF; e += 256) {
+            const int r = e / kMaxF, f = e % kMaxF;
+            ysh[e] = f < F ? __ldcg(yg + int64_t(r) * ld + f) : 0.0;
+          }
+        }
+        ws_sync();  // sC consumed; ysh ready
+        if (ew < 4) {
+          const int g = lane >> 2, t = lane & 3;
+          for (int f = 0; f < F; ++f) {
+#pragma unroll
+            for (int ii = 0; ii < 4; ++ii) {
+              double sum = 0.0;
+#pragma unroll
+              for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+                for (int hb = 0; hb < 2; ++hb)
+                  sum = __fma_rn(acc[ii][jj][hb], ysh[(wc + 8 * jj + 2 * t + hb) * kMaxF + f], sum);
+              sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+              sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+              if (t == 0) red[((wc >> 5) * TB + wr + 8 * ii + g) * kMaxF + f] = sum;
+            }
+          }
+          // Slices of L[i, j] into the staging area (the C buffer).
+          oz_slice_acc(acc, a.oz_mul, reinterpret_cast<uint8_t *>(sC), wr, wc, lane);
+        }
+        ws_sync();
+        {
+          double *rg = rcol + int64_t(i) * TB * ld;
+          for (int e = etid; e < TB * F; e += 256) {
+            const int r = e / F, f = e % F;
+            rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(TB + r) * kMaxF + f];
+          }
+          int4 *dst = reinterpret_cast<int4 *>(slice_row(sl, i) + int64_t(j) * kOzTileBytes);
+          const int4 *src = reinterpret_cast<const int4 *>(sC);
+          for (int e = etid; e < kOzTileBytes / 16; e += 256) dst[e] = src[e];
+        }
+        if (i == j + 1) finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
+        else ws_sync();
+        if (finish) {
+          const double *src = a.dpart + int64_t(sl.q) * TB * TB;
+          for (int e = etid; e < TB * TB; e += 256) sC[(e >> 6) * LDS + (e & 63)] = __ldcg(src + e);
+        }
+      }
+      if (finish) {
+        // D = D' - L[j+1, j] L[j+1, j]^T, factored: X_{j+1}, y_{j+1}.
+        const double *lg = W + int64_t(j + 1) * TB * ld + int64_t(j) * TB;
+        for (int e = etid; e < TB * TB; e += 256)
+          sL[(e >> 6) * LDS + (e & 63)] = __ldcg(lg + int64_t(e >> 6) * ld + (e & 63));
+        ws_sync();
+        double acc[4][4][2];
+        if (ew < 4) {
+          acc_load(acc, sC, LDS, wr, wc, lane);
+          mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
+        }
+        ws_sync();
+        if (ew < 4) acc_store(acc, sC, LDS, wr, wc, lane);
+        ws_sync();
+        double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(ysh);
+        double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(ysh + TB * kMaxF);
+        double *dis = ysh + TB * kMaxF + 2 * TB;
+        const bool bad = diag_tile_t(sC, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
+                                     a.inv + sl.inv + int64_t(j + 1) * TB * TB, sX, cv, dis, ysd,
+                                     etid, ws_sync);
+        if (etid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+        xq = -1;  // sX was the factor's scratch
+      }
+      ws_sync();
+    }
+    cp_async_wait<0>();
+  }
+  __syncthreads();
+  if (!mbar_wait(&bar->done, 0u, kOzDrainLimit)) *abort_flag = 1;
+  tc_fence_after();
+  __syncthreads();
+  // After a time-out, the patches of every item of this CTA's range are
+  // marked for the FP64 LU (a slot whose diagonal hand-over this CTA did not
+  // complete is among them).
+  if (*abort_flag)
+    for (int it = it0 + tid; it < it1; it += kWsThreads)
+      atomicOr(&a.status[slots[ws_item(ipre, cnt, it).q].k], 8);
   tc_fence_before();
   __syncthreads();
   if (warp == 0)
@@ -887,31 +1392,11 @@ size_t chol_back_smem(int F) {
   return size_t(S) * kBkTile + size_t(8 * TB * F + TB * F) * 8 + 2 * S * 8 + 16;
 }
 
-__device__ __forceinline__ void mbar_arrive_cnt(uint64_t *b, uint32_t cnt) {
-  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(saddr(b)),
-               "r"(cnt)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      "selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(saddr(b)), "r"(parity)
-      : "memory");
-  return done != 0;
-}
 
 // Bounded wait for a phase that gives up early once the CTA has aborted.
 __device__ __forceinline__ bool mbar_wait_abort(uint64_t *b, uint32_t parity,
                                                 volatile int *abort_flag) {
-  for (int it = 0; it < kOzWaitLimit; ++it) {
-    if (mbar_try(b, parity)) return true;
-    if (*abort_flag) return false;
-  }
-  return false;
+  return mbar_wait_pipe(b, parity, kOzWaitLimit, abort_flag);
 }
 
 // One 64 x 64 FP64 tile (rows ld doubles apart) into a pipeline stage by the
@@ -1352,6 +1837,20 @@ CholPlan chol_prefix(const std::vector<BigSlot> &slots) {
     if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
   }
   cp.off[steps] = int(cp.pre.size());
+  // Items of the warp-specialised int8 step: T - j per slot (its diagonal
+  // item, then its row tiles j + 1 .. T - 1).
+  cp.ioff.resize(steps);
+  for (int j = 0; j < steps; ++j) {
+    const int c = cp.cnt[j];
+    cp.ioff[j] = int(cp.pre.size());
+    int64_t acc = 0;
+    cp.pre.push_back(0);
+    for (int q = 0; q < c; ++q) {
+      acc += slots[q].T - j;
+      cp.pre.push_back(int(acc));
+    }
+    if (acc > 0x7fffffffll) throw Error{PACMAN_B200_ERR_LIMIT, "too many tiles in one launch"};
+  }
   return cp;
 }
 
@@ -1364,6 +1863,8 @@ void chol_set_smem_attributes() {
                                int(kColSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_col_step_oz, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kOzSmem)));
+  PB_CUDA(cudaFuncSetAttribute(k_col_step_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kWsSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
   {
@@ -1390,16 +1891,15 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   k_diag_chol<<<cp.ns, 256, kDiagSmem, st>>>(a, ds, 0);
   note_launch();
   const int steps = int(cp.cnt.size());
-  std::vector<cudaEvent_t> ev;
-  if (rep.time_kernels) {
-    ev.resize(2 * size_t(steps));
-    for (auto &e : ev) PB_CUDA(cudaEventCreate(&e));
-  }
   int sms = 0;
   PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
-  // First step on the int8 tensor cores (PACMAN_B200_INT8_FROM overrides).
+  // First step on the int8 tensor cores (PACMAN_B200_INT8_FROM overrides),
+  // and the int8 step kernel: the warp-specialised one, or with
+  // PACMAN_B200_STEP=pair the one with two row tiles per CTA.
   const char *ofe = std::getenv("PACMAN_B200_INT8_FROM");
   const int oz_from = ofe ? std::max(1, std::atoi(ofe)) : 4;
+  const char *skind = std::getenv("PACMAN_B200_STEP");
+  const bool pair_kernel = skind && std::strcmp(skind, "pair") == 0;
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
@@ -1408,35 +1908,80 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       PB_CUDA(cudaEventRecord(tail_event, st));
       tail = true;
     }
-    if (rep.time_kernels) PB_CUDA(cudaEventRecord(ev[2 * j], st));
+    SolveReport::TimedLaunch tl{};
+    if (rep.time_kernels) {
+      PB_CUDA(cudaEventCreate(&tl.e0));
+      PB_CUDA(cudaEventCreate(&tl.e1));
+      PB_CUDA(cudaEventRecord(tl.e0, st));
+    }
     // With int8 slices: the FP64 kernel (two CTAs per SM) for the short K
     // loops of the first steps, writing the slices; the int8 kernel after.
+    const bool i8 = a.slices != nullptr && j >= oz_from;
     if (a.slices == nullptr)
       k_col_step<false><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
-    else if (j < oz_from)
+    else if (!i8)
       k_col_step<true><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
-    else
-      k_col_step_oz<<<n, kColThreads, kOzSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
+    else if (pair_kernel)  // plus one diagonal CTA per slot
+      k_col_step_oz<<<n + c, kColThreads, kOzSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
+    else {
+      const int items = cp.pre[cp.ioff[j] + c];
+      k_col_step_ws<<<std::min(items, sms), kWsThreads, kWsSmem, st>>>(a, ds, dpre + cp.ioff[j],
+                                                                       c, j);
+    }
     note_launch();
     if (rep.time_kernels) {
-      PB_CUDA(cudaEventRecord(ev[2 * j + 1], st));
+      PB_CUDA(cudaEventRecord(tl.e1, st));
       // Tile products: (T - j - 1) row tiles x (j + 1) (update + solve), and
       // j + 1 for the next diagonal tile.
+      tl.kind = i8 ? 1 : 0;
       for (int q = 0; q < c; ++q)
-        rep.update_flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j + 1);
-      ++rep.update_launches;
+        tl.flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j + 1);
+      rep.timed.push_back(tl);
     }
-  }
-  if (rep.time_kernels) {
-    PB_CUDA(cudaStreamSynchronize(st));
-    for (int j = 0; j < steps; ++j) {
-      float ms = 0.f;
-      PB_CUDA(cudaEventElapsedTime(&ms, ev[2 * j], ev[2 * j + 1]));
-      rep.ms_update += ms;
-    }
-    for (auto &e : ev) cudaEventDestroy(e);
   }
   if (!tail) PB_CUDA(cudaEventRecord(tail_event, st));
+}
+
+void finish_kernel_timing(SolveReport &rep, cudaEvent_t ref) {
+  if (rep.timed.empty()) return;
+  // Intervals [start, end) in ms after ref, per kind and for both kinds; the
+  // span is the length of their union (launches of different slot groups
+  // overlap in time on their own streams).
+  std::vector<std::pair<double, double>> iv[3];
+  for (const auto &t : rep.timed) {
+    float a0 = 0.f, a1 = 0.f;
+    PB_CUDA(cudaEventElapsedTime(&a0, ref, t.e0));
+    PB_CUDA(cudaEventElapsedTime(&a1, ref, t.e1));
+    iv[t.kind].push_back({a0, a1});
+    iv[2].push_back({a0, a1});
+    rep.flops_kind[t.kind] += t.flops;
+    rep.launches_kind[t.kind] += 1;
+    rep.update_flops += t.flops;
+    rep.update_launches += 1;
+    cudaEventDestroy(t.e0);
+    cudaEventDestroy(t.e1);
+  }
+  rep.timed.clear();
+  double span[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 3; ++k) {
+    std::sort(iv[k].begin(), iv[k].end());
+    double cs = 0.0, ce = -1.0;
+    bool open = false;
+    for (const auto &x : iv[k]) {
+      if (!open || x.first > ce) {
+        if (open) span[k] += ce - cs;
+        cs = x.first;
+        ce = x.second;
+        open = true;
+      } else if (x.second > ce) {
+        ce = x.second;
+      }
+    }
+    if (open) span[k] += ce - cs;
+  }
+  rep.ms_kind[0] += span[0];
+  rep.ms_kind[1] += span[1];
+  rep.ms_update += span[2];
 }
 
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,

@@ -571,7 +571,7 @@ void build_lists(Plan &p, const GridView &g, const double4 *pts, double radius, 
                           st));
   if (K > 0)
     PB_CUDA(cudaMemcpyAsync(sizes.data(), cnt.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   if (nnz > (int64_t(1) << 31) - 1)
     throw Error{PACMAN_B200_ERR_LIMIT, "more than 2^31 patch memberships"};
   unsorted.alloc(sizeof(int) * std::max<int64_t>(nnz, 1), st);
@@ -589,7 +589,7 @@ void build_lists(Plan &p, const GridView &g, const double4 *pts, double radius, 
     PB_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp2.p, tb2, unsorted.as<int>(), idx.as<int>(),
                                                nnz, K, off.as<int64_t>(),
                                                off.as<int64_t>() + 1, st));
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
   }
   PB_CUDA(cudaGetLastError());
 }
@@ -797,7 +797,7 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   PB_CUDA(cudaGetLastError());
   RadiusState rs;
   PB_CUDA(cudaMemcpyAsync(&rs, rsm.p, sizeof(rs), cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   for (int d = 0; d < 3; ++d) {
     p.lo[d] = rs.lo[d];
     p.hi[d] = rs.hi[d];
@@ -890,7 +890,7 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   int K = 0, stat = 0;
   PB_CUDA(cudaMemcpyAsync(&K, nsel.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   PB_CUDA(cudaMemcpyAsync(&stat, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   if (stat) throw Error{PACMAN_B200_ERR_LIMIT, "centre pruning did not settle"};
   p.K = K;
 
@@ -902,7 +902,7 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   // Grid of centres for the partition-of-unity weights.
   build_grid(p.cgrid, p.centers.as<double4>(), K, dim, p.lo, p.hi, r, st);
   PB_CUDA(cudaEventRecord(e1, st));
-  PB_CUDA(cudaEventSynchronize(e1));
+  PB_CUDA(host_sync_event(e1));
   float ms = 0.f;
   PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   p.ms_geometry = ms;
@@ -925,7 +925,7 @@ void pack_points(const double *in_dev, int dim, int64_t n, DevMem &out4, double 
   note_launch();
   unsigned long long h[6];
   PB_CUDA(cudaMemcpyAsync(h, bb.p, sizeof(h), cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   auto to_dbl = [](unsigned long long b) {
     b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
     double d;

@@ -95,7 +95,7 @@ void fe_nearest(int dim, const double *src_dev, int64_t n, const double *vals_de
                                        src4.as<double4>(), vals_dev, out_dev);
   note_launch();
   PB_CUDA(cudaGetLastError());
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
 }
 
 }  // namespace pacman_b200

@@ -18,6 +18,7 @@ enum PatchStatus : int {
   kStatusNonFinite = 2,   // a non-finite local value
   kStatusBreakdown = 4,   // non-positive Cholesky pivot
   kStatusTimeout = 8,     // a bounded tensor-core pipeline wait gave up
+  kStatusResolved = 16,   // re-solved by the FP64 LU after one of the above (host side)
 };
 
 struct PatchArgs {

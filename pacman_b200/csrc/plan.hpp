@@ -146,6 +146,7 @@ struct Plan {
   DevMem scratch;                   // solver workspace
   DevMem local;                     // per (patch, target) local values
   DevMem status;                    // per patch status words
+  std::vector<int> patch_status;    // status words of the last execute (host copy)
   double ms_geometry = 0.0;
   int64_t dropped_axis_patches = 0;
   // State saved by an execute for the adjoint (pacman_b200_plan_adjoint).
@@ -160,6 +161,7 @@ struct Plan {
   int64_t m_owned = -1;
   DevMem tlist;
   int64_t launches_geometry = 0;  // kernel launches of the geometry phase
+  int64_t syncs_geometry = 0;     // host waits of the geometry phase
   int64_t launches = 0;           // kernel launches of the current execute
   AuxStreams aux;
   std::unique_ptr<FactorCache, FactorCacheDeleter> fcache;  // kept factorisations, or null
@@ -194,6 +196,17 @@ class HostArena {
 // Launch counter of this library's own kernels on the calling thread.
 int64_t &launch_counter();
 inline void note_launch(int k = 1) { launch_counter() += k; }
+// Counter of the calling thread's host waits for the device, and the waits
+// themselves (every wait of a transfer goes through these).
+int64_t &host_sync_counter();
+inline cudaError_t host_sync(cudaStream_t s) {
+  ++host_sync_counter();
+  return cudaStreamSynchronize(s);
+}
+inline cudaError_t host_sync_event(cudaEvent_t e) {
+  ++host_sync_counter();
+  return cudaEventSynchronize(e);
+}
 
 // geometry.cu
 void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev);
@@ -221,8 +234,24 @@ struct SolveReport {
   cudaEvent_t tail_event = nullptr;
   double ms_update = 0.0, update_flops = 0.0;
   int64_t update_launches = 0;
+  // Per kind (0: FP64 steps k_col_step, 1: int8 steps k_col_step_oz): span
+  // of device time with at least one launch of the kind running, FLOPs and
+  // launch count (time_kernels only).
+  double ms_kind[2] = {0.0, 0.0}, flops_kind[2] = {0.0, 0.0};
+  int64_t launches_kind[2] = {0, 0};
+  // Events around each timed step launch, on the launching stream; resolved
+  // by finish_kernel_timing once the solve has completed.
+  struct TimedLaunch {
+    cudaEvent_t e0, e1;
+    int kind;
+    double flops;
+  };
+  std::vector<TimedLaunch> timed;
   int64_t factors_reused = 0;  // patches solved from kept factorisations
 };
+// Turns the recorded launch events into the spans of SolveReport (ref: an
+// event recorded on the solve's stream before any timed launch, complete).
+void finish_kernel_timing(SolveReport &rep, cudaEvent_t ref);
 void solve_patches(Plan &p, int basis, const double *vals_dev, int F, int precision,
                    double *local_dev, SolveReport &rep, bool save_state = false,
                    bool keep_factors = false);

@@ -192,7 +192,7 @@ void shard_plan(Plan &p, int rank, int world) {
   unsigned long long total = 0;
   PB_CUDA(cudaMemcpyAsync(&total, prefix.as<unsigned long long>() + (M - 1), sizeof(total),
                           cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   if (total == 0 || total > ~0ull / static_cast<unsigned long long>(world))
     throw Error{PACMAN_B200_ERR_LIMIT, "target costs out of range for the shard cut"};
   flag.alloc(M, st);
@@ -231,7 +231,7 @@ void shard_plan(Plan &p, int rank, int world) {
     int64_t nnz = 0;
     PB_CUDA(cudaMemcpyAsync(&nnz, noff.as<int64_t>() + K, sizeof(int64_t), cudaMemcpyDeviceToHost,
                             st));
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
     nidx.alloc(sizeof(int) * std::max<int64_t>(nnz, 1), st);
     ncount.alloc(sizeof(int) * K, st);
     k_list_fill<<<blocks(int64_t(K) * 32), 256, 0, st>>>(K, p.toff.as<int64_t>(), p.tidx.as<int>(),
@@ -241,7 +241,7 @@ void shard_plan(Plan &p, int rank, int world) {
     note_launch();
     PB_CUDA(cudaMemcpyAsync(p.m_host.data(), ncount.p, sizeof(int) * K, cudaMemcpyDeviceToHost,
                             st));
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
     std::swap(p.toff.p, noff.p);
     std::swap(p.toff.bytes, noff.bytes);
     std::swap(p.toff.s, noff.s);
@@ -250,7 +250,7 @@ void shard_plan(Plan &p, int rank, int world) {
     std::swap(p.tidx.s, nidx.s);
     p.tnnz = nnz;
   }
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   PB_CUDA(cudaGetLastError());
   p.m_owned = owned;
 }

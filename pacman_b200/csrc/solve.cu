@@ -562,10 +562,11 @@ static void solve_patches_impl(Plan &p, int basis, const double *vals_dev, int F
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
   PB_CUDA(cudaEventRecord(ev1, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   float ms = 0.f;
   PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   rep.ms_factor += ms;
+  finish_kernel_timing(rep, ev0);
   std::vector<int> redo_small, redo_big;
   std::vector<char> redo_mark(cached ? K : 0, 0);
   if (cached) {  // patches the factorising execute sent to the LU path
@@ -583,13 +584,16 @@ static void solve_patches_impl(Plan &p, int basis, const double *vals_dev, int F
     keep->redo_small = redo_small;
     keep->redo_big = redo_big;
   }
+  p.patch_status = stat;
+  for (int k : redo_small) p.patch_status[k] |= kStatusResolved;
+  for (int k : redo_big) p.patch_status[k] |= kStatusResolved;
   rep.patches_fp64 = int64_t(small.size() + big.size());
   if (!redo_small.empty() || !redo_big.empty()) {
     PB_CUDA(cudaEventRecord(ev0, st));
     run_list(p, a, kLU, redo_small, rep, st);
     solve_big(p, basis, vals_dev, F, true, redo_big, local_dev, p.status.as<int>(), rep, ex);
     PB_CUDA(cudaEventRecord(ev1, st));
-    PB_CUDA(cudaStreamSynchronize(st));
+    PB_CUDA(host_sync(st));
     PB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     rep.ms_factor += ms;
     rep.patches_fallback += int64_t(redo_small.size() + redo_big.size());
@@ -645,7 +649,7 @@ void solve_adjoint(Plan &p, int basis, int F, const double *h, double *g_out, So
   // The adjoint has no second path: a pipeline wait that gave up is an error.
   std::vector<int> stat(K);
   PB_CUDA(cudaMemcpyAsync(stat.data(), p.status.p, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
-  PB_CUDA(cudaStreamSynchronize(st));
+  PB_CUDA(host_sync(st));
   for (int k = 0; k < K; ++k)
     if (stat[k] & kStatusTimeout)
       throw Error{PACMAN_B200_ERR_CUDA, "adjoint: a pipeline wait timed out in patch " +

@@ -309,6 +309,16 @@ class Plan:
         _lib.raise_for(self._lib.pacman_b200_plan_local_values(self._h, out.ctypes.data))
         return out[: inf["tgt_nnz"]]
 
+    def patch_status(self) -> np.ndarray:
+        """Per-patch status words of the last execute (int32, K entries):
+        bit 1 polynomial axis dropped, 2 non-finite value, 4 non-positive
+        Cholesky pivot, 8 tensor-core pipeline time-out, 16 re-solved by the
+        FP64 LU."""
+        K = self.info()["num_patches"]
+        out = np.zeros(max(K, 1), dtype=np.int32)
+        _lib.raise_for(self._lib.pacman_b200_plan_patch_status(self._h, out.ctypes.data))
+        return out[:K]
+
     def execute(self, rbf_function, source_values, stats=None, save_for_adjoint=False,
                 time_kernels=False, keep_factors=False):
         """Transfer of source_values ((N,) or (N, F)); with save_for_adjoint the

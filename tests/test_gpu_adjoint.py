@@ -134,3 +134,115 @@ def test_autograd_function_matches_plan_adjoint():
     assert out.is_cuda and V.grad.is_cuda and T.grad.is_cuda
     assert rel_l2(V.grad.cpu().numpy(), gv) <= 1e-13
     assert rel_l2(T.grad.cpu().numpy(), gt) <= 1e-13
+
+
+# ---------------------------------------------------------------------------
+# Precision "mixed": the forward solves run the int8 tensor-core Cholesky and
+# save their coefficients; the adjoint's transpose solves stay FP64.
+# ---------------------------------------------------------------------------
+
+def _blobs_10k():
+    # Patches of up to ~1,700 sources: the large ones take the int8 steps.
+    w = W.make("grid_blobs_1m", scale=0.01)
+    return w["src"], w["tgt"], np.stack([w["values"][:, 0], np.sin(3 * w["src"][:, 1])], 1)
+
+
+def test_mixed_adjoint_agrees_with_fp64():
+    S, T, V = _blobs_10k()
+    G = np.random.default_rng(21).standard_normal((T.shape[0], V.shape[1]))
+    grads = {}
+    for precision in ("fp64", "mixed"):
+        plan = pacman.rbf.Plan(3, S, T, precision=precision)
+        plan.execute(0x12, V, save_for_adjoint=True)
+        grads[precision] = plan.adjoint(G)
+    assert rel_l2(grads["mixed"][0], grads["fp64"][0]) <= 1e-10
+    assert rel_l2(grads["mixed"][1], grads["fp64"][1]) <= 1e-10
+
+
+def test_mixed_target_gradient_central_differences():
+    S, T, V = _blobs_10k()
+    G = np.random.default_rng(22).standard_normal((T.shape[0], V.shape[1]))
+    plan = pacman.rbf.Plan(3, S, T, precision="mixed")
+    plan.execute(0x12, V, save_for_adjoint=True)
+    _, gt = plan.adjoint(G, values=False, targets=True)
+    base = plan.patch_lists("target")
+    rng = np.random.default_rng(23)
+    h, checked = 1e-6, 0
+    for _ in range(16):
+        D = rng.standard_normal(T.shape)
+        D /= np.linalg.norm(D)
+        obj, same = [], True
+        for sgn in (1.0, -1.0):
+            pl = pacman.rbf.Plan(3, S, T + sgn * h * D, precision="mixed")
+            obj.append(float(np.sum(pl.execute(0x12, V) * G)))
+            same &= all(np.array_equal(a, b) for a, b in zip(base, pl.patch_lists("target")))
+        if not same:
+            continue
+        fd = (obj[0] - obj[1]) / (2 * h)
+        an = float(np.sum(gt * D))
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+        checked += 1
+    assert checked >= 12
+
+
+# ---------------------------------------------------------------------------
+# The adjoint workload at its full size: 500,000 uniform sources -> 500,000
+# uniform targets, Wendland C4, 4 fields, upstream gradients N(0, 1).
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_uniform_500k_central_differences(precision):
+    w = W.make("uniform_500k")
+    S, T, V = w["src"], w["tgt"], w["values"]
+    G = np.random.default_rng(31).standard_normal((T.shape[0], V.shape[1]))
+    plan = pacman.rbf.Plan(3, S, T, precision=precision)
+    plan.execute(0x12, V, save_for_adjoint=True)
+    gv, gt = plan.adjoint(G)
+    base = plan.patch_lists("target")
+    rng = np.random.default_rng(32)
+    h = 1e-6
+    # Values: the transfer is linear in them, so central differences are
+    # exact up to rounding, 64 random directions.
+    for _ in range(64):
+        D = rng.standard_normal(V.shape)
+        fd = (np.sum(plan.execute(0x12, V + h * D) * G)
+              - np.sum(plan.execute(0x12, V - h * D) * G)) / (2 * h)
+        an = float(np.sum(gv * D))
+        assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
+    # Target coordinates: 64 random unit directions over all 1.5M coordinates
+    # (directions whose perturbation moves a target across a patch boundary
+    # are skipped: the transfer is not differentiable there).
+    checked = 0
+    for _ in range(64):
+        D = rng.standard_normal(T.shape)
+        D /= np.linalg.norm(D)
+        obj, same = [], True
+        for sgn in (1.0, -1.0):
+            pl = pacman.rbf.Plan(3, S, T + sgn * h * D, precision=precision)
+            obj.append(float(np.sum(pl.execute(0x12, V) * G)))
+            same &= all(np.array_equal(a, b) for a, b in zip(base, pl.patch_lists("target")))
+            pl.close()
+        if not same:
+            continue
+        fd = (obj[0] - obj[1]) / (2 * h)
+        an = float(np.sum(gt * D))
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+        checked += 1
+    assert checked >= 48
+
+
+def test_uniform_500k_subset_operator_transpose():
+    """The explicit FP64 operator of a 5,000-point subset of the adjoint
+    workload (its first 5,000 sources and targets), assembled column by
+    column from unit vectors, against the adjoint in both precisions."""
+    w = W.make("uniform_500k")
+    S, T = w["src"][:5000], w["tgt"][:5000]
+    plan = pacman.rbf.Plan(3, S, T)
+    M = _dense_operator(plan, S.shape[0], 0x12)
+    G = np.random.default_rng(33).standard_normal((T.shape[0], 4))
+    ref = M.T @ G
+    for precision, tol in (("fp64", 1e-11), ("mixed", 1e-10)):
+        p = pacman.rbf.Plan(3, S, T, precision=precision)
+        p.execute(0x12, w["values"][:5000], save_for_adjoint=True)
+        gv, _ = p.adjoint(G, values=True, targets=False)
+        assert rel_l2(gv, ref) <= tol, precision

@@ -1,0 +1,126 @@
+"""The headline workloads at full size against the oracle, patch by patch.
+
+The oracle cannot solve every patch of the 1M -> 1M transfer within a test
+(about nine CPU-minutes on 16 threads), but each patch's local values depend
+on that patch alone (src/rbf_pum/solver/solver.hpp:217-286).  So:
+* the geometry (patch radius, candidate count, centres, both membership CSRs)
+  is compared in full and must be bit-exact;
+* the polynomial block's axis-drop decision (serial_ops.hpp:108-139) is
+  compared for every patch;
+* a stratified sample of patches (by source count, with the 20 largest) is
+  solved by the oracle, and its per-(patch, target) local values are compared
+  with Plan.local_values(): rel-L2 per stratum <= 1e-12 for precision fp64
+  and <= 1e-10 for mixed, the transfer's bounds; the worst patch is named.
+
+Workloads: grid_blobs_1m (1M sources on a jittered grid plus Gaussian blobs,
+1M uniform targets, Wendland C4, one field) and shell_4m (4M sources on a
+perturbed sphere shell plus the enclosing cube, 2M targets, 8 fields) at
+Wendland C2, C4 and C6."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import pacman_b200 as pacman
+from pacman_b200 import workloads as W
+from tests.conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "mixed": 1e-10}
+EDGES = [0, 64, 128, 256, 512, 1024, 2048, 1 << 30]
+
+
+def _sample(n, m, per_stratum=24, largest=20, seed=0):
+    """Patch ids: the `largest` biggest patches plus up to `per_stratum`
+    random ones per size stratum, all with at least one target."""
+    rng = np.random.default_rng(seed)
+    has_t = m > 0
+    ids = set(int(k) for k in np.argsort(-n, kind="stable")[:largest] if has_t[k])
+    for lo, hi in zip(EDGES[:-1], EDGES[1:]):
+        cand = np.where((n > lo) & (n <= hi) & has_t)[0]
+        if len(cand):
+            ids.update(int(k) for k in rng.choice(cand, size=min(per_stratum, len(cand)),
+                                                  replace=False))
+    return np.array(sorted(ids), dtype=np.int64)
+
+
+def _geometry_and_axes(plan, ref):
+    info = plan.info()
+    assert info["radius"] == ref.radius
+    assert info["num_candidates"] == ref.num_candidates
+    assert info["num_patches"] == ref.num_patches
+    assert np.array_equal(plan.centers(), ref.centers())
+    csr = {}
+    for which, r in (("source", ref.src_csr()), ("target", ref.tgt_csr())):
+        off, idx = plan.patch_lists(which)
+        assert np.array_equal(off, r[0]), which
+        assert np.array_equal(idx, r[1]), which
+        csr[which] = off
+    return csr
+
+
+def _compare_locals(name, gpu_local, ref_local, toff, sample, n, tol):
+    """Per-stratum rel-L2 of the sampled patches' local values; asserts the
+    bound and returns a printable summary naming the worst patch."""
+    worst = (0.0, -1)
+    lines = []
+    for lo, hi in zip(EDGES[:-1], EDGES[1:]):
+        ks = [k for k in sample if lo < n[k] <= hi]
+        if not ks:
+            continue
+        rows = np.concatenate([np.arange(toff[k], toff[k + 1]) for k in ks])
+        err = rel_l2(gpu_local[rows], ref_local[rows])
+        for k in ks:
+            r = np.arange(toff[k], toff[k + 1])
+            e = rel_l2(gpu_local[r], ref_local[r])
+            if e > worst[0]:
+                worst = (e, k)
+        lines.append(f"n in ({lo},{min(hi, int(n.max()))}]: {len(ks)} patches rel-L2 {err:.2e}")
+        assert err <= tol, (name, lo, hi, err)
+    summary = (f"{name}: " + "; ".join(lines) +
+               f"; worst patch {worst[1]} (n={n[worst[1]]}) rel-L2 {worst[0]:.2e}")
+    print(summary)
+    return summary
+
+
+def _run(workload, basis, precisions=("fp64", "mixed")):
+    w = W.make(workload)
+    S, T = w["src"], w["tgt"]
+    V = w["values"][:, 0] if w["values"].shape[1] == 1 else w["values"]
+    npc = w["nodes_per_cluster"]
+    oracle.set_threads(os.cpu_count() or 1)
+    ref = oracle.build(3, S, T, npc)
+    soff, _ = ref.src_csr()
+    toff, _ = ref.tgt_csr()
+    n, m = np.diff(soff), np.diff(toff)
+    sample = _sample(n, m)
+    _, ref_local, _ = ref.solve(basis, V, patch_list=sample, want_local=True)
+    ref_local = ref_local.reshape(len(ref_local), -1)
+    dropped_ref = ref.poly_dropped()
+    for precision in precisions:
+        plan = pacman.rbf.Plan(3, S, T, nodes_per_cluster=npc, precision=precision)
+        _geometry_and_axes(plan, ref)
+        st = {}
+        plan.execute(basis, V, stats=st)
+        status = plan.patch_status()
+        live = m > 0
+        dropped_gpu = (status & 1).astype(bool)
+        differ = int(np.count_nonzero(dropped_gpu[live] != dropped_ref[live]))
+        print(f"{workload} {hex(basis)} {precision}: K={len(n)} max_n={n.max()} "
+              f"axis-drop decisions {int(dropped_ref[live].sum())} (oracle), "
+              f"{differ} differ; patches re-solved {int(np.count_nonzero(status & 16))}")
+        assert differ == 0
+        _compare_locals(f"{workload} {hex(basis)} {precision}", plan.local_values(), ref_local,
+                        toff, sample, n, TOL[precision])
+        plan.close()
+
+
+def test_grid_blobs_1m_per_patch_parity():
+    _run("grid_blobs_1m", W.WENDLANDC4)
+
+
+@pytest.mark.parametrize("basis", [W.WENDLANDC2, W.WENDLANDC4, W.WENDLANDC6])
+def test_shell_4m_per_patch_parity(basis):
+    _run("shell_4m", basis)
