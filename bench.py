@@ -58,6 +58,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--kernels-only", action="store_true",
                     help="run warmup + steps transfers and exit (for ncu launch lists)")
+    ap.add_argument("--with-adjoint", action="store_true",
+                    help="with --kernels-only: each step also runs the adjoint (values and "
+                         "target coordinates) of a saved execute")
+    ap.add_argument("--with-fe", action="store_true",
+                    help="with --kernels-only: each step also runs the NEAREST_NEAREST "
+                         "finite-element transfer of the same points")
     ap.add_argument("--configs", action="store_true",
                     help="one line per configuration of the baseline table (GPU in both "
                          "precisions, the CPU restatement in Serial and OpenMP, errors)")
@@ -507,8 +513,19 @@ def main():
     torch.cuda.synchronize()
     if args.kernels_only:
         st = {}
+        plan = None
+        if args.with_adjoint:
+            plan = pacman.rbf.Plan(3, S, T, precision=args.precision, **kw)
+            G = torch.ones_like(V)
         for _ in range(args.steps):
             step(args.precision, st)
+            if plan is not None:
+                plan.execute(w["basis"], V, save_for_adjoint=True)
+                plan.adjoint(G)
+            if args.with_fe:
+                pacman.fe.interpolate(3, pacman.execspaces.CUDA, 0xF0, S,
+                                      V if V.dim() == 1 else V[:, 0].contiguous(), None, None,
+                                      None, T)
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"kernels_only": True, "steps": args.steps, "stats": st}), flush=True)

@@ -83,3 +83,33 @@ def test_degenerate_planar_patches_drop_an_axis():
     out, _, st = plan.solve(0x11, f(S))
     assert st["dropped_axis_patches"] == plan.num_patches
     assert rel_l2(out, f(T)) < 1e-3
+
+
+@pytest.mark.parametrize("dim,N", [(1, 400), (2, 40)])
+def test_node_reproduction_1d_2d(dim, N):
+    # The 20^3 known answer of tests/test_cpp_rbf_interface.cpp:165-198 in one
+    # and two dimensions: a regular grid transferred onto itself reproduces
+    # the source values (rel-L2 < 1e-8, every basis).
+    g = np.arange(N) / (N - 1.0)
+    P = np.stack(np.meshgrid(*([g] * dim), indexing="ij"), axis=-1).reshape(-1, dim)
+    v = np.cos(3 * P[:, 0]) + (P[:, 1] ** 2 if dim > 1 else 0.0)
+    for basis in BASES:
+        out = oracle.interpolate(dim, basis, P, v, P, 30)
+        assert rel_l2(out, v) < 1e-8, basis
+
+
+def test_weights_sum_to_one_and_locals_interpolate_the_nodes():
+    # Every target inside the cover has normalised partition-of-unity weights
+    # summing to one (the un-normalised sums are positive), and every local
+    # interpolant reproduces the source values at its own nodes (targets equal
+    # to sources, so each patch's target list holds its interior nodes).
+    rng = np.random.default_rng(10)
+    S = rng.random((2500, 3))
+    v = W.franke_3d(S)
+    plan = oracle.build(3, S, S, 30)
+    assert (plan.weight_sums() > 0).all()
+    ones, _, _ = plan.solve(0x11, np.ones(len(S)))
+    assert np.max(np.abs(ones - 1.0)) < 1e-12
+    _, local, _ = plan.solve(0x11, v, want_local=True)
+    toff, tidx = plan.tgt_csr()
+    assert rel_l2(local[:, 0] if local.ndim == 2 else local, v[tidx]) < 1e-12
