@@ -73,7 +73,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
         objs = list(ex.map(lambda s: _compile(s, extra, verbose), srcs))
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
+        cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -280,7 +280,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       stats->patches_fp64 = rep.patches_fp64;
       stats->patches_fallback = rep.patches_fallback;
       stats->dropped_axis_patches = rep.dropped;
-      stats->ms_geometry = p.ms_geometry;
+      stats->ms_geometry = geometry_ms(p);
       stats->ms_solve = ms_solve;
       stats->ms_total = ms_total;
       stats->kernel_launches = launch_counter() - launches0 + p.launches_geometry;
@@ -639,14 +639,14 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
       cudaEventElapsedTime(&ms_total, e0, e2);
       double rmax = 0.0;
       for (int32_t i = 0; i < count; ++i) {
-        const Plan &p = plans[i].h->p;
+        Plan &p = plans[i].h->p;
         rmax = std::max(rmax, p.radius);
         stats->num_candidates += p.ncand;
         stats->num_patches += p.K;
         stats->sum_n += p.snnz;
         stats->sum_m += p.tnnz;
         for (int v : p.n_host) stats->max_n = std::max<int64_t>(stats->max_n, v);
-        stats->ms_geometry += p.ms_geometry;
+        stats->ms_geometry += geometry_ms(p);
       }
       stats->radius = rmax;
       stats->patches_fp32 = rep.patches_fp32;

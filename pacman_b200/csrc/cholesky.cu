@@ -1891,15 +1891,14 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   k_diag_chol<<<cp.ns, 256, kDiagSmem, st>>>(a, ds, 0);
   note_launch();
   const int steps = int(cp.cnt.size());
-  int sms = 0;
-  PB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
-  // First step on the int8 tensor cores (PACMAN_B200_INT8_FROM overrides),
-  // and the int8 step kernel: the warp-specialised one, or with
-  // PACMAN_B200_STEP=pair the one with two row tiles per CTA.
-  const char *ofe = std::getenv("PACMAN_B200_INT8_FROM");
-  const int oz_from = ofe ? std::max(1, std::atoi(ofe)) : 4;
+  const Tuning &tu = tuning_for_current_device();
+  const int sms = tu.sms;
+  // First step on the int8 tensor cores and the int8 step kernel (the
+  // warp-specialised one, or the one with two row tiles per CTA): tuned,
+  // PACMAN_B200_INT8_FROM and PACMAN_B200_STEP=pair|ws override.
+  const int oz_from = std::max(1, tuned_int("PACMAN_B200_INT8_FROM", tu.int8_from));
   const char *skind = std::getenv("PACMAN_B200_STEP");
-  const bool pair_kernel = skind && std::strcmp(skind, "pair") == 0;
+  const bool pair_kernel = skind ? std::strcmp(skind, "pair") == 0 : tu.pair_step;
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];

@@ -589,7 +589,7 @@ void build_lists(Plan &p, const GridView &g, const double4 *pts, double radius, 
     PB_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp2.p, tb2, unsorted.as<int>(), idx.as<int>(),
                                                nnz, K, off.as<int64_t>(),
                                                off.as<int64_t>() + 1, st));
-    PB_CUDA(host_sync(st));
+    // tmp2 and unsorted are released stream-ordered: no wait needed.
   }
   PB_CUDA(cudaGetLastError());
 }
@@ -902,12 +902,21 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   // Grid of centres for the partition-of-unity weights.
   build_grid(p.cgrid, p.centers.as<double4>(), K, dim, p.lo, p.hi, r, st);
   PB_CUDA(cudaEventRecord(e1, st));
-  PB_CUDA(host_sync_event(e1));
-  float ms = 0.f;
-  PB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  p.ms_geometry = ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  // No wait here: the time is read after the execute's own final wait.
+  p.geom_ev[0] = e0;
+  p.geom_ev[1] = e1;
+}
+
+double geometry_ms(Plan &p) {
+  if (p.geom_ev[0] && p.geom_ev[1] && cudaEventQuery(p.geom_ev[1]) == cudaSuccess) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.geom_ev[0], p.geom_ev[1]) == cudaSuccess) p.ms_geometry = ms;
+    cudaEventDestroy(p.geom_ev[0]);
+    cudaEventDestroy(p.geom_ev[1]);
+    p.geom_ev[0] = p.geom_ev[1] = nullptr;
+  }
+  cudaGetLastError();
+  return p.ms_geometry < 0.0 ? 0.0 : p.ms_geometry;
 }
 
 // Packed double4 copy of row-major points and their exact bounding box.

@@ -147,7 +147,15 @@ struct Plan {
   DevMem local;                     // per (patch, target) local values
   DevMem status;                    // per patch status words
   std::vector<int> patch_status;    // status words of the last execute (host copy)
-  double ms_geometry = 0.0;
+  double ms_geometry = -1.0;         // device time of the geometry (read lazily)
+  cudaEvent_t geom_ev[2] = {nullptr, nullptr};  // around the geometry, until read
+  Plan() = default;
+  Plan(const Plan &) = delete;
+  Plan &operator=(const Plan &) = delete;
+  ~Plan() {
+    for (cudaEvent_t e : geom_ev)
+      if (e) cudaEventDestroy(e);
+  }
   int64_t dropped_axis_patches = 0;
   // State saved by an execute for the adjoint (pacman_b200_plan_adjoint).
   int saved_basis = -1, saved_F = 0;
@@ -193,6 +201,21 @@ class HostArena {
   std::vector<char *> retired_;
 };
 
+// Launch parameters of the patch solvers for the current device: the tuned
+// file of its GPU model (tuning/<name>.conf beside the library) or the
+// built-in defaults (tuning.cpp).
+struct Tuning {
+  int big_n_chol = 64;  // patches above this size use the tiled Cholesky (mixed)
+  int int8_from = 4;    // first tile column updated on the int8 tensor cores
+  int groups = 0;       // slot groups of the tiled engine (0: min(4, slots / 8))
+  bool pair_step = false;  // int8 step with two row tiles per CTA instead of the warp-specialised one
+  int sms = 148;
+  std::string source = "built-in defaults";
+};
+const Tuning &tuning_for_current_device();
+// The environment variable if set, else the tuned value.
+int tuned_int(const char *env, int value);
+
 // Launch counter of this library's own kernels on the calling thread.
 int64_t &launch_counter();
 inline void note_launch(int k = 1) { launch_counter() += k; }
@@ -210,6 +233,9 @@ inline cudaError_t host_sync_event(cudaEvent_t e) {
 
 // geometry.cu
 void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev);
+// Device time of the plan's geometry phase: read from its events once the
+// stream has passed them (callers have synchronised it), then cached.
+double geometry_ms(Plan &p);
 void pu_gather(Plan &p, const double *local, int F, double *out_dev);
 // Packed double4 points with their exact bounding box, and the uniform cell
 // grid over them (geometry.cu; used by nearest.cu).

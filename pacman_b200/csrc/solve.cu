@@ -467,12 +467,14 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
 void solve_big_cached(Plan &p, FactorCache &c, int basis, const double *vals, int F,
                       double *local, int *status, SolveReport &rep, const BigExtra &extra);
 
-// Patches above this size use the blocked engine (blocked.cu): 64 for the
-// Cholesky path (the register kernels of small.cu take n <= 64), 128 for the
-// LU and adjoint paths.  PACMAN_B200_BIG_N overrides both.
+// Patches above this size use the blocked engine (blocked.cu): for the
+// Cholesky path the tuned value (64 by default; the register kernels of
+// small.cu take n <= 64), 128 for the LU and adjoint paths.
+// PACMAN_B200_BIG_N overrides both.
 static int big_threshold(int mode) {
   const char *e = std::getenv("PACMAN_B200_BIG_N");
-  return e ? std::max(1, std::atoi(e)) : (mode == kChol ? 64 : 128);
+  if (e) return std::max(1, std::atoi(e));
+  return mode == kChol ? std::min(64, std::max(1, tuning_for_current_device().big_n_chol)) : 128;
 }
 
 static void solve_patches_impl(Plan &p, int basis, const double *vals_dev, int F, int precision,

@@ -212,6 +212,12 @@ def test_uniform_500k_central_differences(precision):
     # Target coordinates: 64 random unit directions over all 1.5M coordinates
     # (directions whose perturbation moves a target across a patch boundary
     # are skipped: the transfer is not differentiable there).
+    # The objective sums 2M products out * G; each output carries rounding of
+    # order eps |out|, so two evaluations h apart differ by up to about
+    # eps * sum |out * G| beyond the true change: that, over 2h, is the
+    # central difference's own error at this size (~1e-4 here), added to the
+    # relative bound of the small cases.
+    noise = np.finfo(np.float64).eps * float(np.sum(np.abs(plan.execute(0x12, V) * G))) / (2 * h)
     checked = 0
     for _ in range(64):
         D = rng.standard_normal(T.shape)
@@ -226,7 +232,7 @@ def test_uniform_500k_central_differences(precision):
             continue
         fd = (obj[0] - obj[1]) / (2 * h)
         an = float(np.sum(gt * D))
-        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (fd, an)
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)) + noise, (fd, an, noise)
         checked += 1
     assert checked >= 48
 
