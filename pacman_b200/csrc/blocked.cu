@@ -283,13 +283,12 @@ __global__ void __launch_bounds__(256) k_big_poly(BigArgs a, const BigSlot *__re
   }
 }
 
-// Factors diagonal tile (s, s) of each listed slot and writes its inverses.
+// Factors diagonal tile (s, s) of each listed slot in place: unpivoted LU
+// (unit lower L below the diagonal, U on and above it) or Cholesky.
 template <bool LU>
 __global__ void __launch_bounds__(256) k_diag(BigArgs a, const BigSlot *__restrict__ slots, int s) {
   extern __shared__ double sm[];
   double *T = sm;                 // the tile
-  double *Li = T + TB * LDS;      // inverse of L
-  double *Ui = Li + TB * LDS;     // inverse of U (LU only)
   __shared__ double piv;
   __shared__ int bad;
   const int slot = blockIdx.x;
@@ -328,49 +327,12 @@ __global__ void __launch_bounds__(256) k_diag(BigArgs a, const BigSlot *__restri
       __syncthreads();
     }
   }
-  // Inverses row by row, all threads: X = L^{-1} from the top,
-  // X[p][c] = (delta_pc - sum_{c<=k<p} L[p][k] X[k][c]) / L[p][p], and for LU
-  // Y = U^{-1} from the bottom,
-  // Y[p][c] = (delta_pc - sum_{p<k<=c} U[p][k] Y[k][c]) / U[p][p];
-  // each column's dot product is split over 4 threads.
-  __shared__ double part[2][4][TB];
-  const int col = tid & 63, quarter = tid >> 6;
-  for (int i = 0; i < TB; ++i) {
-    const int pl = i, pu = TB - 1 - i;
-    double sl_ = 0.0, su_ = 0.0;
-    if (col < pl)
-      for (int k = col + quarter; k < pl; k += 4) sl_ = __fma_rn(T[pl * LDS + k], Li[k * LDS + col], sl_);
-    if (LU && col > pu)
-      for (int k = pu + 1 + quarter; k <= col; k += 4) su_ = __fma_rn(T[pu * LDS + k], Ui[k * LDS + col], su_);
-    part[0][quarter][col] = sl_;
-    part[1][quarter][col] = su_;
-    __syncthreads();
-    if (tid < TB) {
-      const double sumL = part[0][0][col] + part[0][1][col] + part[0][2][col] + part[0][3][col];
-      double x = 0.0;
-      if (col == pl) x = LU ? 1.0 : 1.0 / T[pl * LDS + pl];
-      else if (col < pl) x = LU ? -sumL : -sumL / T[pl * LDS + pl];
-      Li[pl * LDS + col] = x;
-    } else if (LU && tid < 2 * TB) {
-      const int c = tid - TB;
-      const double sumU = part[1][0][c] + part[1][1][c] + part[1][2][c] + part[1][3][c];
-      double y = 0.0;
-      if (c == pu) y = 1.0 / T[pu * LDS + pu];
-      else if (c > pu) y = -sumU / T[pu * LDS + pu];
-      Ui[pu * LDS + c] = y;
-    }
-    __syncthreads();
-  }
+  // The factors go back to the workspace, where the panel solves (k_trsm)
+  // and the backward sweep read them.
   for (int idx = tid; idx < TB * TB / 2; idx += blockDim.x) {
     const int r = idx >> 5, c2 = idx & 31;
     *reinterpret_cast<double2 *>(g + int64_t(r) * sl.ld + 2 * c2) =
         *reinterpret_cast<const double2 *>(T + r * LDS + 2 * c2);
-    double *gi = a.inv + int64_t(slot) * 2 * TB * TB;
-    *reinterpret_cast<double2 *>(gi + r * TB + 2 * c2) =
-        *reinterpret_cast<const double2 *>(Li + r * LDS + 2 * c2);
-    if (LU)
-      *reinterpret_cast<double2 *>(gi + TB * TB + r * TB + 2 * c2) =
-          *reinterpret_cast<const double2 *>(Ui + r * LDS + 2 * c2);
   }
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
@@ -384,13 +346,21 @@ __device__ __forceinline__ void load_inv(double *s, const double *g, int tid, in
 }
 
 // Panel tiles of step s: row panel X := L^{-1} X (ti == s), column panel
-// X := X U^{-1} (LU) or X := X L^{-T} (Cholesky).
+// X := X U^{-1} (LU) or X := X L^{-T} (Cholesky), by triangular solves with
+// the factors of the diagonal tile (s, s) as k_diag left them in the
+// workspace (unit lower L below the diagonal, U on and above it, or the
+// Cholesky factor below and on it): backward stable, unlike a product with
+// the explicit inverse, whose error grows with the condition number of the
+// diagonal tile.  Each warp solves 16 rows of X (column panel) or 16 columns
+// (row panel, as rows of X^T against L^T), in two passes of 8
+// (warp_row_solve).
 template <bool LU>
 __global__ void __launch_bounds__(128)
     k_trsm(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
            int s) {
   extern __shared__ double sm[];
-  double *sX = sm, *sI = sm + TB * LDS;
+  __shared__ double dinv[TB];
+  double *sX = sm, *sU = sm + TB * LDS;
   const int q = find_slot(pre, cnt, blockIdx.x);
   const BigSlot sl = slots[q];
   struct {
@@ -399,19 +369,48 @@ __global__ void __launch_bounds__(128)
   it.slot = q;
   decode_trsm(LU, sl, s, blockIdx.x - pre[q], it.ti, it.tj);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   double *X = a.W + sl.base + int64_t(it.ti) * TB * sl.ld + int64_t(it.tj) * TB;
-  const double *inv = a.inv + int64_t(it.slot) * 2 * TB * TB;
+  const double *D = a.W + sl.base + int64_t(s) * TB * sl.ld + int64_t(s) * TB;
   const bool left = it.ti == s;
   load_tile(sX, X, sl.ld, tid, blockDim.x);
-  load_inv(sI, (left || !LU) ? inv : inv + TB * TB, tid, blockDim.x);
+  // The upper triangular operand of x U = c: U itself (LU column panel), or
+  // the transpose of the lower factor (row panel: unit L; Cholesky: L).
+  for (int e = tid; e < TB * TB; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    const double v = D[int64_t(r) * sl.ld + c];
+    if (LU && !left) sU[r * LDS + c] = c >= r ? v : 0.0;
+    else if (LU) sU[c * LDS + r] = r > c ? v : (r == c ? 1.0 : 0.0);
+    else sU[c * LDS + r] = r >= c ? v : 0.0;
+  }
   __syncthreads();
-  double acc[4][4][2];
-  acc_zero(acc);
-  if (left) mma64<false, false>(sI, sX, acc, 1.0, wr, wc, lane);
-  else if (LU) mma64<false, false>(sX, sI, acc, 1.0, wr, wc, lane);
-  else mma64<false, true>(sX, sI, acc, 1.0, wr, wc, lane);
-  acc_store(acc, X, sl.ld, wr, wc, lane);
+  if (tid < TB) dinv[tid] = (LU && left) ? 1.0 : 1.0 / sU[tid * LDS + tid];
+  __syncthreads();
+  for (int pass = 0; pass < 2; ++pass) {
+    const int r0 = 16 * warp + 8 * pass;
+    double lo[8], hi[8];
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) {
+      lo[qq] = left ? sX[lane * LDS + r0 + qq] : sX[(r0 + qq) * LDS + lane];
+      hi[qq] = left ? sX[(lane + 32) * LDS + r0 + qq] : sX[(r0 + qq) * LDS + 32 + lane];
+    }
+    warp_row_solve<8>(lo, hi, sU, dinv, lane);
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) {
+      if (left) {
+        sX[lane * LDS + r0 + qq] = lo[qq];
+        sX[(lane + 32) * LDS + r0 + qq] = hi[qq];
+      } else {
+        sX[(r0 + qq) * LDS + lane] = lo[qq];
+        sX[(r0 + qq) * LDS + 32 + lane] = hi[qq];
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < TB * TB / 2; idx += blockDim.x) {
+    const int r = idx >> 5, c2 = idx & 31;
+    *reinterpret_cast<double2 *>(X + int64_t(r) * sl.ld + 2 * c2) =
+        *reinterpret_cast<const double2 *>(sX + r * LDS + 2 * c2);
+  }
 }
 
 template <bool LU>

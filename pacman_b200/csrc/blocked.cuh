@@ -120,6 +120,40 @@ __device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 }
 
+// Row solves x U = c for R rows of a 64-column tile by one warp: U upper
+// triangular (row-major, row stride LDS) in shared memory and dinv[c] =
+// 1 / U[c][c] (1 for a unit diagonal); on entry lo[q] / hi[q] hold columns
+// lane and lane + 32 of row q of c, on return those of x.  Right-looking
+// substitution: once x_c is known (broadcast from the lane holding column c),
+// every later column subtracts x_c U[c][c'].  This is a backward-stable
+// triangular solve (unlike a product with an explicitly inverted triangle,
+// whose error grows with the condition number of the triangle).
+template <int R>
+__device__ __forceinline__ void warp_row_solve(double (&lo)[R], double (&hi)[R],
+                                               const double *sU, const double *dinv, int lane) {
+#pragma unroll 1
+  for (int c = 0; c < 32; ++c) {
+    const double d = dinv[c];
+    const double ul = sU[c * LDS + lane], uh = sU[c * LDS + 32 + lane];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const double x = __shfl_sync(0xffffffffu, lo[q], c) * d;
+      lo[q] = lane == c ? x : (lane > c ? __fma_rn(-x, ul, lo[q]) : lo[q]);
+      hi[q] = __fma_rn(-x, uh, hi[q]);
+    }
+  }
+#pragma unroll 1
+  for (int c = 32; c < 64; ++c) {
+    const double d = dinv[c];
+    const double uh = sU[c * LDS + 32 + lane];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const double x = __shfl_sync(0xffffffffu, hi[q], c - 32) * d;
+      hi[q] = lane + 32 == c ? x : (lane + 32 > c ? __fma_rn(-x, uh, hi[q]) : hi[q]);
+    }
+  }
+}
+
 // Asynchronous 16-byte global -> shared copies (cp.async, sm_80+).
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -133,6 +167,17 @@ __device__ __forceinline__ void async_tile(double *s, const double *g, int ld, i
   for (int idx = tid; idx < TB * TB / 2; idx += nt) {
     const int r = idx >> 5, c2 = idx & 31;
     cp_async16(s + r * LDS + 2 * c2, g + int64_t(r) * ld + 2 * c2);
+  }
+}
+
+// Loads the diagonal tile's factor U = L_jj^T (row-major in the workspace's
+// diagonal tile position, written by diag_tile) into sU with cp.async; the
+// caller commits, waits, and then fills dinv[c] = 1 / U[c][c].
+__device__ __forceinline__ void load_factor_async(double *sU, const double *gu, int ld, int tid,
+                                                  int nt) {
+  for (int idx = tid; idx < TB * TB / 2; idx += nt) {
+    const int r = idx >> 5, c2 = idx & 31;
+    cp_async16(sU + r * LDS + 2 * c2, gu + int64_t(r) * ld + 2 * c2);
   }
 }
 

@@ -111,8 +111,12 @@ __device__ __forceinline__ void sync_all() { __syncthreads(); }
 // A[i][s] until pivot s and L^{-1}[i][s] afterwards.  Per pivot the owners
 // publish one vector (row p of L^{-1} left of the pivot, the pivot, column p
 // of A below it) and all threads update their slots: one barrier per pivot.
-// Only X = L_c^{-1} = D^{-1/2} L^{-1} is kept (the trsm, the forward and the
-// backward substitution use nothing else).  Non-positive pivots set status 4.
+// X = L_c^{-1} = D^{-1/2} L^{-1} is kept for the forward and backward
+// substitutions; with gu, the factor itself is written too, as U = L_c^T
+// (row p = column p of L_c, from the pivot column c / sqrt(pivot)), for the
+// triangular solves of the tiles below (a trsm by substitution: multiplying by
+// the explicit inverse loses accuracy on ill-conditioned tiles).
+// Non-positive pivots set status 4.
 // D: lower part at g (row stride ld, global or shared); r: the first F
 // columns of the residual tile at rg (row stride rld), overwritten with y; X
 // goes to gi (row stride TB).  Xs (TB x LDS), cv, dis and ys are shared
@@ -120,7 +124,7 @@ __device__ __forceinline__ void sync_all() { __syncthreads(); }
 template <class Sync>
 __device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F, double *gi,
                             double *Xs, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
-                            int tid, Sync sync) {
+                            int tid, Sync sync, double *gu = nullptr, int uld = 0) {
   const int bi = tid >> 4, bs = tid & 15;
   bool bad = false;
   double v[4][4];
@@ -166,6 +170,10 @@ __device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F,
     const double piv = c[p];
     bad |= !(piv > 0.0);
     const double inv = 1.0 / piv;
+    if (gu && tid < TB) {  // row p of U = L_c^T: column p of the Cholesky factor
+      const double sq = sqrt(piv);
+      gu[int64_t(p) * uld + tid] = tid > p ? c[tid] / sq : (tid == p ? sq : 0.0);
+    }
     double cs[4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) cs[b] = c[4 * bs + b];
@@ -221,9 +229,10 @@ __device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F,
 
 __device__ __forceinline__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F,
                                           double *gi, double *Xs, double (*cv)[TB], double *dis,
-                                          double (*ys)[kMaxF]) {
+                                          double (*ys)[kMaxF], double *gu = nullptr,
+                                          int uld = 0) {
   return diag_tile_t(g, ld, rg, rld, F, gi, Xs, cv, dis, ys, int(threadIdx.x),
-                     [] { __syncthreads(); });
+                     [] { __syncthreads(); }, gu, uld);
 }
 
 // The diagonal tile of step 0 of every slot.
@@ -241,76 +250,65 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
   __syncthreads();
   double *rg = a.W + sl.base + int64_t(j) * TB * ld + int64_t(sl.T) * TB;
   const bool bad =
-      diag_tile(gt, LDS, rg, ld, a.F, a.inv + sl.inv + int64_t(j) * TB * TB, sm, cv, dis, ys);
+      diag_tile(gt, LDS, rg, ld, a.F, a.inv + sl.inv + int64_t(j) * TB * TB, sm, cv, dis, ys,
+                a.W + sl.base + int64_t(j) * TB * ld + int64_t(j) * TB, ld);
   if (threadIdx.x == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
-// Phase 2 of a factorisation step.  sC holds C (the updated row tiles i0, and
-// i0 + 1 when arows = 2 TB; kColRows x LDS doubles).  L[i, j] = C X_j^T on the
-// FP64 tensor cores (X_j through sX, TB x LDS), stored in the workspace and
-// left in acc; then the forward substitution r_i -= L[i, j] y_j with scratch
-// at sm (TB kMaxF + 2 kColRows kMaxF doubles, after sX is consumed).  Ends
-// with a barrier.  256 threads.
-__device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, int arows, bool active,
-                          double *sm, double *sC, double *sX, double (&acc)[4][4][2]) {
+// Phase 2 of a factorisation step (256 threads, warp w: rows 16 w .. + 15,
+// in two passes of 8).  sC holds C (row tiles i0, and i0 + 1 when arows =
+// 2 TB; kColRows x LDS).  L[i, j] solves L[i, j] U_j = C with U_j = L_jj^T
+// (the factor of the diagonal tile, loaded into sU), row by row
+// (warp_row_solve); it is stored in the workspace and written back over C in
+// sC; then the forward substitution r_i -= L[i, j] y_j.  vec holds TB + TB
+// kMaxF doubles (1 / diag(U_j), y_j).  Ends with a barrier.
+__device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, int arows,
+                          double *sC, double *sU, double *vec) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int ld = sl.ld, F = a.F;
   double *W = a.W + sl.base;
   double *rcol = W + int64_t(sl.T) * TB;
-  double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
-  {
-    const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
-    for (int idx = tid; idx < TB * TB / 2; idx += kColThreads) {
-      const int r = idx >> 5, c2 = idx & 31;
-      cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
-    }
-    cp_async_commit();
-  }
-  cp_async_wait<0>();
-  __syncthreads();
-  acc_zero(acc);
-  if (active) {
-    mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
-    acc_store(acc, C, ld, wr, wc, lane);
-  }
-  __syncthreads();  // sC and sX are free
-  double *ysh = sm;               // TB x kMaxF
-  double *red = sm + TB * kMaxF;  // 2 x kColRows x kMaxF
+  double *dinv = vec, *ysh = vec + TB;
+  load_factor_async(sU, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, tid, kColThreads);
+  cp_async_commit();
   {
     const double *yg = rcol + int64_t(j) * TB * ld;
     for (int e = tid; e < TB * kMaxF; e += kColThreads) {
       const int r = e / kMaxF, f = e % kMaxF;
-      ysh[e] = f < F ? yg[int64_t(r) * ld + f] : 0.0;
+      ysh[e] = f < F ? __ldcg(yg + int64_t(r) * ld + f) : 0.0;
     }
   }
+  cp_async_wait<0>();
   __syncthreads();
-  for (int f = 0; f < F; ++f) {
-    double pr[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      double s = 0.0;
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-          s = __fma_rn(acc[i][jj][h], ysh[(wc + 8 * jj + 2 * t + h) * kMaxF + f], s);
-      s += __shfl_xor_sync(0xffffffffu, s, 1);
-      s += __shfl_xor_sync(0xffffffffu, s, 2);
-      pr[i] = s;
-    }
-    if (t == 0 && active) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) red[((wc >> 5) * kColRows + wr + 8 * i + g) * kMaxF + f] = pr[i];
-    }
-  }
+  if (tid < TB) dinv[tid] = 1.0 / sU[tid * LDS + tid];
   __syncthreads();
-  {
-    double *rg = rcol + int64_t(i0) * TB * ld;
-    for (int e = tid; e < arows * F; e += kColThreads) {
-      const int r = e / F, f = e % F;
-      rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(kColRows + r) * kMaxF + f];
+  double *C = W + int64_t(i0) * TB * ld + int64_t(j) * TB;
+  double *rg = rcol + int64_t(i0) * TB * ld;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int r0 = 16 * warp + 8 * pass;
+    if (r0 >= arows) break;
+    double lo[8], hi[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      lo[q] = sC[(r0 + q) * LDS + lane];
+      hi[q] = sC[(r0 + q) * LDS + 32 + lane];
+    }
+    warp_row_solve<8>(lo, hi, sU, dinv, lane);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      sC[(r0 + q) * LDS + lane] = lo[q];
+      sC[(r0 + q) * LDS + 32 + lane] = hi[q];
+      C[int64_t(r0 + q) * ld + lane] = lo[q];
+      C[int64_t(r0 + q) * ld + 32 + lane] = hi[q];
+    }
+    for (int f = 0; f < F; ++f) {
+      const double yl = ysh[lane * kMaxF + f], yh = ysh[(lane + 32) * kMaxF + f];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        double sum = __fma_rn(lo[q], yl, hi[q] * yh);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) rg[int64_t(r0 + q) * ld + f] -= sum;
+      }
     }
   }
   __syncthreads();
@@ -336,16 +334,6 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
 // core, copied to shared memory with bulk async copies.
 constexpr int kOzS = 7;
 constexpr int kOzTileBytes = 4 * kOzS * 8 * 128;      // 28672
-constexpr int kOzStages = 3;                          // pipeline depth, K = 32 per stage
-constexpr int kOzStageA = 2 * kOzS * 16 * 128;        // two row tiles: 28672
-constexpr int kOzStageB = 2 * kOzS * 8 * 128;         // one row tile: 14336
-constexpr int kOzStage = kOzStageA + kOzStageB;       // 43008
-constexpr int kOzGenOff = kOzStages * kOzStage;       // A[i, j] (then C), kColRows x LDS doubles
-constexpr int kOzPtsOff = kOzGenOff + kColRows * LDS * 8;  // points of the evaluated tile
-constexpr int kOzBarOff = kOzPtsOff + 3 * (kColRows + TB) * 8;  // barriers, TMEM address
-constexpr size_t kOzSmem = size_t(kOzBarOff) + 256;  // 2 x OzBars + TMEM address
-constexpr int kOzSLOff = 40 * 1024;                   // phase 3: L[j+1, j] (TB x LDS doubles)
-constexpr int kOzStgOff = 24 * 1024;                  // slice staging (2 tiles) in phase 2
 constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 // Polls of the waits that drain a pipeline after it gave up: they wait for
@@ -354,12 +342,6 @@ constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 // (BigArgs::wait_limit) and are never shortened.
 constexpr int kOzDrainLimit = 1 << 24;
 
-static_assert(kOzStgOff >= (TB * kMaxF + 2 * kColRows * kMaxF) * 8, "staging overlaps y/red");
-static_assert(kOzStgOff + 2 * kOzTileBytes <= kOzGenOff, "staging overlaps the tile");
-static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the tile");
-static_assert(kOzSLOff >= (TB * LDS + TB * kMaxF + 3 * TB) * 8, "L[j+1, j] overlaps X");
-static_assert(2 * sizeof(uint64_t) * (2 * kOzStages + 1) + 16 <= 256, "barrier area");
-static_assert(kOzSLOff + TB * LDS * 8 <= kOzGenOff, "L[j+1, j] overlaps the diagonal tile");
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -441,165 +423,40 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 }
 
-struct OzBars {
-  uint64_t full[kOzStages], empty[kOzStages], done;
-};
-
-// K loop over the p < nump column tiles of one step on the int8 tensor cores:
-// TMEM columns 64 (l - 2) .. + 63 receive level l = 2..kOzS+1 of
-// [rows of tile rA0 (and rA1)] x [rows of tile rB]^T.  rA0, rA1, rB point to
-// the first slice tile of their tile row (tiles of a row are consecutive in
-// p).  Thread 0 issues the bulk copies, thread 32 the MMAs; every thread
-// returns after the MMAs completed.  Threads 64.. run side(t, nt) meanwhile.
-//
-// Every pipeline wait is bounded by `limit` polls.  When one gives up, the
-// thread raises the CTA's abort flag and the other side stops at its next
-// wait; then the copies already issued (the latest use of each stage) and
-// the MMAs already issued (the final commit) are waited for with the longer
-// drain limit, so that nothing is still writing shared memory or TMEM when
-// the CTA goes on or exits.  Returns false, on every thread, if the loop was
-// aborted.
-template <class Side>
-__device__ bool oz_kloop(uint8_t *stages, OzBars *bar, volatile int *abort_flag, uint32_t tmem,
-                         const uint8_t *rA0, const uint8_t *rA1, const uint8_t *rB, int nump,
-                         int limit, Side side) {
-  const int tid = threadIdx.x;
-  // Earlier generic writes to the stage area before the async-proxy copies.
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  if (tid == 0) {
-    for (int i = 0; i < kOzStages; ++i) {
-      mbar_init(&bar->full[i], 1);
-      mbar_init(&bar->empty[i], 1);
+// The int8 digits of rows [0, nrows) of L tiles held in shared memory (row
+// stride LDS; rows 64.. belong to the second tile) straight into their slice
+// tiles in global memory (dst0: the tile of rows 0..63, dst1: rows 64..127).
+// A thread unit is (row, 16-column K chunk): it builds the 16 bytes of each of
+// the kOzS slices and stores each as one 16-byte word, consecutive units of a
+// warp writing consecutive words.  Digits: y = round(x 128^kOzS) as an
+// integer (x = L mul / 128 in [-1, 1]); balanced base-128 digits from the top,
+// d = round(y / 128^(kOzS-1-s)), y -= d 128^(kOzS-1-s).
+__device__ void slice_tile_smem(const double *sL, int nrows, double mul, uint8_t *dst0,
+                                uint8_t *dst1, int tid, int nt) {
+  for (int u = tid; u < nrows * 4; u += nt) {
+    const int r = (u & 63) + 64 * (u >> 8), c16 = (u >> 6) & 3;
+    uint32_t w[kOzS][4];
+#pragma unroll
+    for (int sl = 0; sl < kOzS; ++sl)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) w[sl][q] = 0u;
+#pragma unroll
+    for (int cc = 0; cc < 16; ++cc) {
+      const double xs = fmin(fmax(sL[r * LDS + 16 * c16 + cc] * mul, -127.49), 127.49);
+      long long y = __double2ll_rn(xs * 0x1p42);  // x * 128 * 128^(kOzS-1)
+#pragma unroll
+      for (int sl = 0; sl < kOzS; ++sl) {
+        const int sh = 7 * (kOzS - 1 - sl);
+        const long long d = sh ? ((y + (1ll << (sh - 1))) >> sh) : y;
+        y -= d << sh;
+        w[sl][cc >> 2] |= uint32_t(uint8_t(int8_t(d))) << (8 * (cc & 3));
+      }
     }
-    mbar_init(&bar->done, 1);
-    *abort_flag = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    uint8_t *dst = (r < 64 ? dst0 : dst1) + c16 * kOzS * 1024 + (r & 63) * 16;
+#pragma unroll
+    for (int sl = 0; sl < kOzS; ++sl)
+      *reinterpret_cast<uint4 *>(dst + sl * 1024) = make_uint4(w[sl][0], w[sl][1], w[sl][2], w[sl][3]);
   }
-  __syncthreads();
-  const int nh = 2 * nump;  // K = 32 halves of the column tiles
-  if (tid == 0) {
-    const uint32_t bytes = uint32_t((rA1 ? 2 : 1) * kOzTileBytes / 2 + kOzTileBytes / 2);
-    int issued = 0;
-    for (int hh = 0; hh < nh; ++hh) {
-      const int st = hh % kOzStages, u = hh / kOzStages;
-      if (hh >= kOzStages && !mbar_wait_pipe(&bar->empty[st], uint32_t((u - 1) & 1), limit,
-                                             abort_flag)) {
-        *abort_flag = 1;
-        break;
-      }
-      uint8_t *sA = stages + st * kOzStage;
-      uint8_t *sB = sA + kOzStageA;
-      mbar_expect_tx(&bar->full[st], bytes);
-      const int64_t toff = int64_t(hh >> 1) * kOzTileBytes + (hh & 1) * 2 * kOzS * 1024;
-      const uint8_t *a0 = rA0 + toff;
-      const uint8_t *a1 = rA1 ? rA1 + toff : nullptr;
-      for (int cs = 0; cs < 2 * kOzS; ++cs) {  // (K chunk, slice) pieces of 8 row groups
-        bulk_g2s(sA + cs * 16 * 128, a0 + cs * 1024, 1024, &bar->full[st]);
-        if (a1) bulk_g2s(sA + (cs * 16 + 8) * 128, a1 + cs * 1024, 1024, &bar->full[st]);
-      }
-      bulk_g2s(sB, rB + toff, 2 * kOzS * 1024, &bar->full[st]);
-      issued = hh + 1;
-    }
-    // Drain: an earlier use of a stage was consumed before its stage was
-    // refilled, so only the latest use of each stage can still be in flight.
-    for (int st = 0; st < kOzStages && st < issued; ++st) {
-      const int last = st + kOzStages * ((issued - 1 - st) / kOzStages);
-      if (!mbar_wait(&bar->full[st], uint32_t((last / kOzStages) & 1), kOzDrainLimit))
-        *abort_flag = 1;
-    }
-  } else if (tid == 32) {
-    for (int hh = 0; hh < nh; ++hh) {
-      const int st = hh % kOzStages, u = hh / kOzStages;
-      if (!mbar_wait_pipe(&bar->full[st], uint32_t(u & 1), limit, abort_flag)) {
-        *abort_flag = 1;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t sA = saddr(stages + st * kOzStage);
-      const uint32_t sB = sA + kOzStageA;
-#pragma unroll
-      for (int a = 1; a <= kOzS; ++a) {
-        const uint64_t ad = umma_desc(sA + ((a - 1) * 16) * 128, kOzS * 16 * 128, 128);
-        const int nb = kOzS + 1 - a;  // slices b = 1 .. nb -> levels a + 1 .. kOzS + 1
-        const uint32_t accf = (hh > 0 || a > 1) ? 1u : 0u;
-        const int n1 = nb < 4 ? nb : 4;
-        umma_i8(tmem + 64 * (a - 1), ad, umma_desc(sB, kOzS * 8 * 128, 128),
-                umma_idesc_i8(64 * n1), accf);
-        if (nb > 4)
-          umma_i8(tmem + 64 * (a - 1) + 256, ad, umma_desc(sB + 4 * 8 * 128, kOzS * 8 * 128, 128),
-                  umma_idesc_i8(64 * (nb - 4)), accf);
-      }
-      umma_commit(&bar->empty[st]);
-    }
-    umma_commit(&bar->done);  // arrives once every MMA issued above has completed
-  } else if (tid >= 64) {
-    side(tid - 64, int(blockDim.x) - 64);  // warps 2.. are free during the K loop
-  }
-  __syncthreads();
-  if (!mbar_wait(&bar->done, 0u, kOzDrainLimit)) *abort_flag = 1;
-  tc_fence_after();
-  __syncthreads();
-  return *abort_flag == 0;
-}
-
-// Row r = 32 (warp % 4) + lane of the K loop's result, columns 32 h .. + 31
-// (h = warp / 4): v[c] = sum_l 128^-l Z_l[r][32 h + c].
-__device__ __forceinline__ void oz_levels(uint32_t tmem, double (&v)[32]) {
-  const int warp = threadIdx.x >> 5;
-  const uint32_t lane_base = uint32_t(32 * (warp & 3)) << 16;
-  const int h = warp >> 2;
-#pragma unroll
-  for (int c = 0; c < 32; ++c) v[c] = 0.0;
-#pragma unroll
-  for (int lev = 2; lev <= kOzS + 1; ++lev) {
-    uint32_t z[32];
-    const uint32_t addr = tmem + lane_base + uint32_t(64 * (lev - 2) + 32 * h);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(z[0]), "=r"(z[1]), "=r"(z[2]), "=r"(z[3]), "=r"(z[4]), "=r"(z[5]), "=r"(z[6]),
-          "=r"(z[7]), "=r"(z[8]), "=r"(z[9]), "=r"(z[10]), "=r"(z[11]), "=r"(z[12]), "=r"(z[13]),
-          "=r"(z[14]), "=r"(z[15])
-        : "r"(addr));
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(z[16]), "=r"(z[17]), "=r"(z[18]), "=r"(z[19]), "=r"(z[20]), "=r"(z[21]),
-          "=r"(z[22]), "=r"(z[23]), "=r"(z[24]), "=r"(z[25]), "=r"(z[26]), "=r"(z[27]),
-          "=r"(z[28]), "=r"(z[29]), "=r"(z[30]), "=r"(z[31])
-        : "r"(addr + 16));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    const double sc = ldexp(1.0, -7 * lev);
-#pragma unroll
-    for (int c = 0; c < 32; ++c) v[c] = __fma_rn(double(int32_t(z[c])), sc, v[c]);
-  }
-}
-
-// The int8 digits of the FP64 tile values held in acc (rows wr.., columns
-// wc.. of a 128 x 64 pair) into the staging area stg (two slice tiles).
-__device__ __forceinline__ void oz_slice_acc(const double (&acc)[4][4][2], double mul, uint8_t *stg,
-                                             int wr, int wc, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = wr + 8 * i + g, c = wc + 8 * jj + 2 * t + h;
-        const int r64 = r & 63;
-        uint8_t *dst = stg + (r >> 6) * kOzTileBytes + (c >> 4) * kOzS * 1024 +
-                       (r64 >> 3) * 128 + (r64 & 7) * 16 + (c & 15);
-        // y = round(x 128^kOzS) as an integer; balanced base-128 digits from
-        // the top: d = round(y / 128^(kOzS-1-s)), y -= d 128^(kOzS-1-s).
-        const double xs = fmin(fmax(acc[i][jj][h] * mul, -127.49), 127.49);
-        long long y = __double2ll_rn(xs * 0x1p42);  // x * 128 * 128^(kOzS-1)
-#pragma unroll
-        for (int sl = 0; sl < kOzS; ++sl) {
-          const int sh = 7 * (kOzS - 1 - sl);
-          const long long d = sh ? ((y + (1ll << (sh - 1))) >> sh) : y;
-          y -= d << sh;
-          dst[sl * 1024] = uint8_t(int8_t(d));
-        }
-      }
 }
 
 // Step j of the factorisation, one launch over all slots with T > j + 1.
@@ -684,7 +541,7 @@ __global__ void __launch_bounds__(kColThreads, 2)
   cp_async_wait<0>();
   __syncthreads();
 
-  // 2. L[i, j] = C X_j^T through shared memory, then the forward substitution.
+  // 2. L[i, j] U_j = C through shared memory, then the forward substitution.
   if (active) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -693,34 +550,22 @@ __global__ void __launch_bounds__(kColThreads, 2)
         *reinterpret_cast<double2 *>(sm + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
             make_double2(-acc[i][jj][0], -acc[i][jj][1]);
   }
-  step_trsm(a, sl, j, i0, arows, active, sm, sm, sm + kColRows * LDS, acc);
+  __syncthreads();
+  step_trsm(a, sl, j, i0, arows, sm, sm + kColRows * LDS, sm + (kColRows + TB) * LDS);
   if (SLICE) {  // int8 slices of the new L tiles for the int8 steps that follow
-    uint8_t *stg = reinterpret_cast<uint8_t *>(sm) + kOzStgOff;
-    if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
-    __syncthreads();
-    const uint8_t *srow = a.slices + sl.sli;
-    for (int tt = 0; tt < arows / TB; ++tt) {
-      const int i = i0 + tt;
-      int4 *dst = reinterpret_cast<int4 *>(const_cast<uint8_t *>(srow) +
-                                           (int64_t(i) * (i - 1) / 2 + j) * kOzTileBytes);
-      const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
-      for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
-    }
+    uint8_t *srow = a.slices + sl.sli;
+    slice_tile_smem(sm, arows, a.oz_mul, srow + (int64_t(i0) * (i0 - 1) / 2 + j) * kOzTileBytes,
+                    srow + (int64_t(i0 + 1) * i0 / 2 + j) * kOzTileBytes, tid, kColThreads);
   }
   if (l != 0) return;
 
   // 3. The diagonal tile of step j + 1 (this CTA's first row tile).
   __syncthreads();
   constexpr int kDStage = TB * kKLD;
-  double *sL = sm + 2 * kDStage;  // L[j+1, j], TB x LDS
-  if (wr < TB) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-        *reinterpret_cast<double2 *>(sL + (wr + 8 * i + g) * LDS + wc + 8 * jj + 2 * t) =
-            make_double2(acc[i][jj][0], acc[i][jj][1]);
-  }
+  double *sL = sm + 2 * kDStage;  // L[j+1, j], TB x LDS (rows 0..63 of sC are below it)
+  static_assert(2 * kDStage >= TB * LDS, "L[j+1, j] overlaps its copy source");
+  for (int e = tid; e < TB * TB; e += kColThreads) sL[(e >> 6) * LDS + (e & 63)] = sm[(e >> 6) * LDS + (e & 63)];
+  __syncthreads();
   auto loadd = [&](int c, int stage) {
     double *sD = sm + stage * kDStage;
     const int col = c * kKC;
@@ -772,204 +617,9 @@ __global__ void __launch_bounds__(kColThreads, 2)
   double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
   double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
   const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
-                             a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
+                             a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd,
+                             W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld);
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
-}
-
-// The next diagonal tile of a slot has two producers in the int8 step: the
-// diagonal CTA (D' = A[j+1, j+1] - the terms p < j) and row CTA 0 (L[j+1, j],
-// stored by its trsm).  Each writes its part to global memory and arrives on
-// the slot's counter; the second to arrive finishes the tile.  Nothing waits
-// on the other CTA: the first arrival just leaves, so the order in which the
-// CTAs are scheduled does not matter.  Returns true, on every thread, for the
-// second arrival, which also resets the counter for the next step's launch.
-__device__ __forceinline__ bool oz_diag_arrive(int *count, volatile int *flag) {
-  __threadfence();  // this thread's global writes, device-wide, before the arrival
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int old = atomicAdd(count, 1);
-    *flag = old;
-    if (old == 1) *count = 0;
-  }
-  __syncthreads();
-  const bool last = *flag == 1;
-  if (last) __threadfence();  // the partner's writes (fenced before its arrival) come first
-  return last;
-}
-
-// Finishes the diagonal tile j + 1 of a slot: Ds (shared, TB x LDS) holds
-// D' = A[j+1, j+1] - sum_{p<j} L[j+1, p] L[j+1, p]^T, or the CTA loads it
-// from the diagonal CTA's copy in a.dpart; then D = D' - L[j+1, j] L[j+1, j]^T
-// (FP64 tensor cores, L[j+1, j] read back from the workspace through L2),
-// and the inverse factor X_{j+1} and y_{j+1} = X_{j+1} r_{j+1} (diag_tile).
-// Data of the other CTA is read with L2 loads (ld.global.cg).
-__device__ void oz_finish_diag(const BigArgs &a, const BigSlot &sl, int j, uint8_t *smb,
-                               double *Ds, bool ds_from_global) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  const int ld = sl.ld;
-  double *W = a.W + sl.base;
-  double *rcol = W + int64_t(sl.T) * TB;
-  if (ds_from_global) {
-    const double *src = a.dpart + int64_t(sl.q) * TB * TB;
-    for (int e = tid; e < TB * TB; e += kColThreads) Ds[(e >> 6) * LDS + (e & 63)] = __ldcg(src + e);
-  }
-  double *sL = reinterpret_cast<double *>(smb + kOzSLOff);
-  const double *lg = W + int64_t(j + 1) * TB * ld + int64_t(j) * TB;
-  for (int e = tid; e < TB * TB; e += kColThreads)
-    sL[(e >> 6) * LDS + (e & 63)] = __ldcg(lg + int64_t(e >> 6) * ld + (e & 63));
-  __syncthreads();
-  double acc[4][4][2];
-  if (wr < TB) {
-    acc_load(acc, Ds, LDS, wr, wc, lane);
-    mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
-  }
-  __syncthreads();
-  if (wr < TB) acc_store(acc, Ds, LDS, wr, wc, lane);
-  __syncthreads();
-  double *Xs = reinterpret_cast<double *>(smb);
-  double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(Xs + TB * LDS);
-  double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(Xs + TB * LDS + TB * kMaxF);
-  double *dis = Xs + TB * LDS + TB * kMaxF + 2 * TB;
-  const bool bad = diag_tile(Ds, LDS, rcol + int64_t(j + 1) * TB * ld, ld, a.F,
-                             a.inv + sl.inv + int64_t(j + 1) * TB * TB, Xs, cv, dis, ysd);
-  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
-}
-
-// Step j of the factorisation with the column update on the int8 tensor cores
-// (one CTA per SM: the K loop holds 448 TMEM columns).  Blocks [0, cnt) are
-// the diagonal CTAs of the active slots, [cnt, 2 cnt) their row CTAs 0, then
-// the other row CTAs (prefix counts in pre).
-//  * Row CTA l owns row tiles i0 = j + 1 + 2 l and i0 + 1: C = A[i, j] -
-//    sigma^2 sum_l 128^-l Z_l over p < j (int8 K loop; warps 2.. evaluate
-//    A[i, j] meanwhile), L[i, j] = C X_j^T and the forward substitution
-//    (step_trsm), then the int8 slices of L[i, j].
-//  * The diagonal CTA forms D' = A[j+1, j+1] - the p < j terms by its own
-//    int8 K loop, concurrently with the row CTAs, and stores it.
-//  * Whichever of the diagonal CTA and row CTA 0 arrives second finishes
-//    the tile (oz_finish_diag) for step j + 1.
-__global__ void __launch_bounds__(kColThreads, 1)
-    k_col_step_oz(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
-                  int j) {
-  extern __shared__ __align__(1024) uint8_t smb[];
-  double *sm = reinterpret_cast<double *>(smb);
-  OzBars *bars = reinterpret_cast<OzBars *>(smb + kOzBarOff);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smb + kOzBarOff + 2 * sizeof(OzBars));
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(smb + kOzBarOff + 2 * sizeof(OzBars) + 8);
-  volatile int *arrive_flag = abort_flag + 1;
-  const int b = blockIdx.x;
-  const bool diag = b < cnt;
-  int q, l;
-  if (diag) {
-    q = b;
-    l = -1;
-  } else if (b < 2 * cnt) {
-    q = b - cnt;
-    l = 0;
-  } else {
-    const int bb = b - 2 * cnt;
-    q = find_slot(pre, cnt, bb);
-    l = 1 + bb - pre[q];
-  }
-  const BigSlot sl = slots[q];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  auto slice_row = [&](int i) {
-    return a.slices + sl.sli + (int64_t(i) * (i - 1) / 2) * kOzTileBytes;
-  };
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     saddr(tmem_slot)),
-                 "r"(kOzTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  bool ok = true;
-  double *sGen = reinterpret_cast<double *>(smb + kOzGenOff);
-  double *pts = reinterpret_cast<double *>(smb + kOzPtsOff);
-  auto side_sync = [] (int nt) { asm volatile("bar.sync 1, %0;\n" ::"r"(nt) : "memory"); };
-
-  if (diag) {
-    // D' = A[j+1, j+1] - sigma^2 sum_l 128^-l Z_l (p < j) in sGen.
-    double *Ds = sGen;
-    if (j > 0) {
-      const uint8_t *rd = slice_row(j + 1);
-      ok = oz_kloop(smb, bars, abort_flag, tmem, rd, nullptr, rd, j, a.wait_limit,
-                    [&](int t0, int nt) {
-                      gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, t0, nt, [&] { side_sync(nt); });
-                    });
-    } else {
-      gen_tile(a, sl, j + 1, j + 1, TB, Ds, pts, tid, kColThreads, sync_all);
-    }
-    {
-      const int r = 32 * (warp & 3) + lane, h = warp >> 2;
-      double v[32];
-      if (j > 0) oz_levels(tmem, v);
-      if (j > 0) tc_fence_before();
-      __syncthreads();
-      if (j > 0 && r < TB) {
-        double *Dr = Ds + r * LDS + 32 * h;
-#pragma unroll
-        for (int c = 0; c < 32; ++c) Dr[c] = __fma_rn(-a.oz_sig2, v[c], Dr[c]);
-      }
-    }
-    __syncthreads();
-    double *dst = a.dpart + int64_t(sl.q) * TB * TB;
-    for (int e = tid; e < TB * TB; e += kColThreads) dst[e] = Ds[(e >> 6) * LDS + (e & 63)];
-    if (oz_diag_arrive(a.dcount + sl.q, arrive_flag)) oz_finish_diag(a, sl, j, smb, Ds, false);
-  } else {
-    const int i0 = j + 1 + 2 * l;
-    const bool two = i0 + 1 < sl.T;
-    const int arows = two ? kColRows : TB;
-    const bool active = two || wr < TB;
-    // 1. C = A[i, j] - sigma^2 sum_l 128^-l Z_l in sGen (kColRows x LDS);
-    //    A[i, j] is evaluated by warps 2.. while the K loop runs.
-    if (j > 0) {
-      ok = oz_kloop(smb, bars, abort_flag, tmem, slice_row(i0), two ? slice_row(i0 + 1) : nullptr,
-                    slice_row(j), j, a.wait_limit, [&](int t0, int nt) {
-                      gen_tile(a, sl, i0, j, arows, sGen, pts, t0, nt, [&] { side_sync(nt); });
-                    });
-    } else {
-      gen_tile(a, sl, i0, j, arows, sGen, pts, tid, kColThreads, sync_all);
-    }
-    {
-      const int r = 32 * (warp & 3) + lane, h = warp >> 2;
-      double v[32];
-      if (j > 0) oz_levels(tmem, v);
-      if (j > 0) tc_fence_before();
-      __syncthreads();
-      if (j > 0 && r < arows) {
-        double *Cr = sGen + r * LDS + 32 * h;
-#pragma unroll
-        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
-      }
-    }
-    // 2. L[i, j] = C X_j^T and the forward substitution; then the slices of L.
-    double acc[4][4][2];
-    step_trsm(a, sl, j, i0, arows, active, sm, sGen, sm, acc);
-    uint8_t *stg = smb + kOzStgOff;
-    if (active) oz_slice_acc(acc, a.oz_mul, stg, wr, wc, lane);
-    __syncthreads();
-    for (int tt = 0; tt < arows / TB; ++tt) {
-      int4 *dst = reinterpret_cast<int4 *>(slice_row(i0 + tt) + int64_t(j) * kOzTileBytes);
-      const int4 *src = reinterpret_cast<const int4 *>(stg + tt * kOzTileBytes);
-      for (int e = tid; e < kOzTileBytes / 16; e += kColThreads) dst[e] = src[e];
-    }
-    // 3. Row CTA 0 stored L[j+1, j]: its half of the next diagonal tile.
-    if (l == 0 && oz_diag_arrive(a.dcount + sl.q, arrive_flag))
-      oz_finish_diag(a, sl, j, smb, sGen, true);
-  }
-  if (tid == 0 && !ok) atomicOr(&a.status[sl.k], 8);
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(kOzTmemCols)
-                 : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -1205,12 +855,12 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     double *sL = reinterpret_cast<double *>(smb + kWsLOff);
     double *pts = reinterpret_cast<double *>(smb + kWsPtsOff);
     double *ysh = reinterpret_cast<double *>(smb + kWsRedOff);  // TB x kMaxF
-    double *red = ysh + TB * kMaxF;                              // 2 x TB x kMaxF
+    double *dinv = ysh + TB * kMaxF;                             // 1 / diag(U_j)
     volatile int *arrive_flag = &bar->arrive_flag;
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
     ws_sync();
-    int xq = -1;  // slot whose X_j is in sX
+    int xq = -1;  // slot whose U_j (factor of the diagonal tile, transposed) is in sX
     int k = 0;
     for (int it = it0; it < it1; ++it, ++k) {
       const WsItem w = ws_item(ipre, cnt, it);
@@ -1220,14 +870,12 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       double *rcol = W + int64_t(sl.T) * TB;
       const bool diag = w.r == 0;
       const int i = diag ? j + 1 : j + w.r;
+      bool fresh = false;
       if (!diag && xq != w.q) {
-        const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
-        for (int idx = etid; idx < TB * TB / 2; idx += 256) {
-          const int r = idx >> 5, c2 = idx & 31;
-          cp_async16(sX + r * LDS + 2 * c2, xg + r * TB + 2 * c2);
-        }
+        load_factor_async(sX, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, etid, 256);
         cp_async_commit();
         xq = w.q;
+        fresh = true;
       }
       // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run.
       gen_tile(a, sl, i, diag ? j + 1 : j, TB, sC, pts, etid, 256, ws_sync);
@@ -1266,15 +914,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         for (int e = etid; e < TB * TB; e += 256) dst[e] = sC[(e >> 6) * LDS + (e & 63)];
         finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
       } else {
-        // L[i, j] = C X_j^T (four warps), stored; forward substitution.
+        // L[i, j] U_j = C by row substitution (warp ew: rows 8 ew .. + 7),
+        // stored; forward substitution; int8 slices.
         cp_async_wait<0>();
         ws_sync();
-        double acc[4][4][2];
-        acc_zero(acc);
-        if (ew < 4) {
-          mma64<false, true>(sC, sX, acc, 1.0, wr, wc, lane);
-          acc_store(acc, W + int64_t(i) * TB * ld + int64_t(j) * TB, ld, wr, wc, lane);
-        }
+        if (fresh && etid < TB) dinv[etid] = 1.0 / sX[etid * LDS + etid];
         {
           const double *yg = rcol + int64_t(j) * TB * ld;
           for (int e = etid; e < TB * kMaxF; e += 256) {
@@ -1282,36 +926,39 @@ __global__ void __launch_bounds__(kWsThreads, 1)
             ysh[e] = f < F ? __ldcg(yg + int64_t(r) * ld + f) : 0.0;
           }
         }
-        ws_sync();  // sC consumed; ysh ready
-        if (ew < 4) {
-          const int g = lane >> 2, t = lane & 3;
+        ws_sync();
+        const int r0 = 8 * ew;
+        double lo[8], hi[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          lo[q] = sC[(r0 + q) * LDS + lane];
+          hi[q] = sC[(r0 + q) * LDS + 32 + lane];
+        }
+        warp_row_solve<8>(lo, hi, sX, dinv, lane);
+        {
+          double *Lg = W + int64_t(i) * TB * ld + int64_t(j) * TB;
+          double *rg = rcol + int64_t(i) * TB * ld;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            sC[(r0 + q) * LDS + lane] = lo[q];  // the warp's own rows: L over C
+            sC[(r0 + q) * LDS + 32 + lane] = hi[q];
+            Lg[int64_t(r0 + q) * ld + lane] = lo[q];
+            Lg[int64_t(r0 + q) * ld + 32 + lane] = hi[q];
+          }
           for (int f = 0; f < F; ++f) {
+            const double yl = ysh[lane * kMaxF + f], yh = ysh[(lane + 32) * kMaxF + f];
 #pragma unroll
-            for (int ii = 0; ii < 4; ++ii) {
-              double sum = 0.0;
-#pragma unroll
-              for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-                for (int hb = 0; hb < 2; ++hb)
-                  sum = __fma_rn(acc[ii][jj][hb], ysh[(wc + 8 * jj + 2 * t + hb) * kMaxF + f], sum);
-              sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-              sum += __shfl_xor_sync(0xffffffffu, sum, 2);
-              if (t == 0) red[((wc >> 5) * TB + wr + 8 * ii + g) * kMaxF + f] = sum;
+            for (int q = 0; q < 8; ++q) {
+              double sum = __fma_rn(lo[q], yl, hi[q] * yh);
+              for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+              if (lane == 0) rg[int64_t(r0 + q) * ld + f] -= sum;
             }
           }
-          // Slices of L[i, j] into the staging area (the C buffer).
-          oz_slice_acc(acc, a.oz_mul, reinterpret_cast<uint8_t *>(sC), wr, wc, lane);
         }
         ws_sync();
         {
-          double *rg = rcol + int64_t(i) * TB * ld;
-          for (int e = etid; e < TB * F; e += 256) {
-            const int r = e / F, f = e % F;
-            rg[int64_t(r) * ld + f] -= red[r * kMaxF + f] + red[(TB + r) * kMaxF + f];
-          }
-          int4 *dst = reinterpret_cast<int4 *>(slice_row(sl, i) + int64_t(j) * kOzTileBytes);
-          const int4 *src = reinterpret_cast<const int4 *>(sC);
-          for (int e = etid; e < kOzTileBytes / 16; e += 256) dst[e] = src[e];
+          uint8_t *dst = slice_row(sl, i) + int64_t(j) * kOzTileBytes;
+          slice_tile_smem(sC, TB, a.oz_mul, dst, dst, etid, 256);
         }
         if (i == j + 1) finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
         else ws_sync();
@@ -1339,7 +986,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         double *dis = ysh + TB * kMaxF + 2 * TB;
         const bool bad = diag_tile_t(sC, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
                                      a.inv + sl.inv + int64_t(j + 1) * TB * TB, sX, cv, dis, ysd,
-                                     etid, ws_sync);
+                                     etid, ws_sync,
+                                     W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld);
         if (etid == 0 && bad) atomicOr(&a.status[sl.k], 4);
         xq = -1;  // sX was the factor's scratch
       }
@@ -1861,8 +1509,6 @@ void chol_set_smem_attributes() {
                                int(kColSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_col_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kColSmem)));
-  PB_CUDA(cudaFuncSetAttribute(k_col_step_oz, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(kOzSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_col_step_ws, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kWsSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1893,12 +1539,8 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   const int steps = int(cp.cnt.size());
   const Tuning &tu = tuning_for_current_device();
   const int sms = tu.sms;
-  // First step on the int8 tensor cores and the int8 step kernel (the
-  // warp-specialised one, or the one with two row tiles per CTA): tuned,
-  // PACMAN_B200_INT8_FROM and PACMAN_B200_STEP=pair|ws override.
+  // First step on the int8 tensor cores: tuned, PACMAN_B200_INT8_FROM overrides.
   const int oz_from = std::max(1, tuned_int("PACMAN_B200_INT8_FROM", tu.int8_from));
-  const char *skind = std::getenv("PACMAN_B200_STEP");
-  const bool pair_kernel = skind ? std::strcmp(skind, "pair") == 0 : tu.pair_step;
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
@@ -1920,8 +1562,6 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       k_col_step<false><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
     else if (!i8)
       k_col_step<true><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
-    else if (pair_kernel)  // plus one diagonal CTA per slot
-      k_col_step_oz<<<n + c, kColThreads, kOzSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
     else {
       const int items = cp.pre[cp.ioff[j] + c];
       k_col_step_ws<<<std::min(items, sms), kWsThreads, kWsSmem, st>>>(a, ds, dpre + cp.ioff[j],

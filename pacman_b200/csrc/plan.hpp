@@ -208,7 +208,6 @@ struct Tuning {
   int big_n_chol = 64;  // patches above this size use the tiled Cholesky (mixed)
   int int8_from = 4;    // first tile column updated on the int8 tensor cores
   int groups = 0;       // slot groups of the tiled engine (0: min(4, slots / 8))
-  bool pair_step = false;  // int8 step with two row tiles per CTA instead of the warp-specialised one
   int sms = 148;
   std::string source = "built-in defaults";
 };

@@ -4,8 +4,6 @@ Times whole transfers (CUDA events, median after warm-up, inputs resident on
 the device) over these parameters, by coordinate descent from the built-in
 defaults:
 
-* ``PACMAN_B200_STEP``: the int8 step kernel, ``ws`` (warp-specialised, one
-  row tile per item) or ``pair`` (two row tiles per CTA);
 * ``PACMAN_B200_INT8_FROM``: the first tile column whose update runs on the
   int8 tensor cores (the columns before it use the FP64 tensor cores);
 * ``PACMAN_B200_GROUPS``: slot groups of the tiled engine, each stepping on
@@ -30,12 +28,11 @@ import statistics
 import sys
 
 SPACE = {
-    "PACMAN_B200_STEP": ["ws", "pair"],
     "PACMAN_B200_INT8_FROM": ["2", "3", "4", "5", "6"],
     "PACMAN_B200_GROUPS": ["1", "2", "3", "4"],
     "PACMAN_B200_BIG_N": ["32", "48", "64"],
 }
-DEFAULTS = {"PACMAN_B200_STEP": "ws", "PACMAN_B200_INT8_FROM": "4", "PACMAN_B200_GROUPS": "4",
+DEFAULTS = {"PACMAN_B200_INT8_FROM": "4", "PACMAN_B200_GROUPS": "4",
             "PACMAN_B200_BIG_N": "64"}
 
 
