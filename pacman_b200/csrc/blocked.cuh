@@ -121,13 +121,15 @@ __device__ __forceinline__ void acc_zero(double (&acc)[4][4][2]) {
 }
 
 // Row solves x U = c for R rows of a 64-column tile by one warp: U upper
-// triangular (row-major, row stride LDS) in shared memory and dinv[c] =
-// 1 / U[c][c] (1 for a unit diagonal); on entry lo[q] / hi[q] hold columns
-// lane and lane + 32 of row q of c, on return those of x.  Right-looking
-// substitution: once x_c is known (broadcast from the lane holding column c),
-// every later column subtracts x_c U[c][c'].  This is a backward-stable
-// triangular solve (unlike a product with an explicitly inverted triangle,
-// whose error grows with the condition number of the triangle).
+// triangular (row-major, row stride LDS, exact zeros below the diagonal) in
+// shared memory and dinv[c] = 1 / U[c][c] (1 for a unit diagonal); on entry
+// lo[q] / hi[q] hold columns lane and lane + 32 of row q of c, on return
+// those of x.  Right-looking substitution: once x_c is known (broadcast from
+// the lane holding column c), every column subtracts x_c U[c][c'] (a no-op
+// left of c, where U is zero) and the lane of column c keeps x_c.  This is a
+// backward-stable triangular solve (unlike a product with an explicitly
+// inverted triangle, whose error grows with the condition number of the
+// triangle).
 template <int R>
 __device__ __forceinline__ void warp_row_solve(double (&lo)[R], double (&hi)[R],
                                                const double *sU, const double *dinv, int lane) {
@@ -135,10 +137,11 @@ __device__ __forceinline__ void warp_row_solve(double (&lo)[R], double (&hi)[R],
   for (int c = 0; c < 32; ++c) {
     const double d = dinv[c];
     const double ul = sU[c * LDS + lane], uh = sU[c * LDS + 32 + lane];
+    const bool own = lane == c;
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const double x = __shfl_sync(0xffffffffu, lo[q], c) * d;
-      lo[q] = lane == c ? x : (lane > c ? __fma_rn(-x, ul, lo[q]) : lo[q]);
+      lo[q] = own ? x : __fma_rn(-x, ul, lo[q]);
       hi[q] = __fma_rn(-x, uh, hi[q]);
     }
   }
@@ -146,10 +149,11 @@ __device__ __forceinline__ void warp_row_solve(double (&lo)[R], double (&hi)[R],
   for (int c = 32; c < 64; ++c) {
     const double d = dinv[c];
     const double uh = sU[c * LDS + 32 + lane];
+    const bool own = lane + 32 == c;
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const double x = __shfl_sync(0xffffffffu, hi[q], c - 32) * d;
-      hi[q] = lane + 32 == c ? x : (lane + 32 > c ? __fma_rn(-x, uh, hi[q]) : hi[q]);
+      hi[q] = own ? x : __fma_rn(-x, uh, hi[q]);
     }
   }
 }

@@ -70,11 +70,13 @@ __device__ __forceinline__ void acc_neg(double (&acc)[4][4][2]) {
 template <class Sync>
 __device__ __forceinline__ void gen_tile(const BigArgs &a, const BigSlot &sl, int ti, int tj,
                                          int nrows, double *sT, double *pts, int t, int nt,
-                                         Sync sync) {
+                                         Sync sync, bool load_cols = true) {
   const int64_t s0 = a.soff[sl.k];
   double *rx = pts, *ry = rx + nrows, *rz = ry + nrows;
   double *cx = rz + nrows, *cy = cx + TB, *cz = cy + TB;
-  for (int e = t; e < nrows + TB; e += nt) {
+  // With load_cols false the column points are still in pts from a previous
+  // tile of the same slot and column tile.
+  for (int e = t; e < (load_cols ? nrows + TB : nrows); e += nt) {
     const int gi = e < nrows ? ti * TB + e : tj * TB + (e - nrows);
     double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
     if (gi < sl.n) p = a.src[a.sidx[s0 + gi]];
@@ -169,11 +171,10 @@ __device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F,
     sync();
     const double piv = c[p];
     bad |= !(piv > 0.0);
-    const double inv = 1.0 / piv;
-    if (gu && tid < TB) {  // row p of U = L_c^T: column p of the Cholesky factor
-      const double sq = sqrt(piv);
-      gu[int64_t(p) * uld + tid] = tid > p ? c[tid] / sq : (tid == p ? sq : 0.0);
-    }
+    const double inv = __drcp_rn(piv);
+    // Row p of U = L_c^T is column p of the Cholesky factor, c / sqrt(pivot):
+    // the unscaled column now, the scaling once the loop is over.
+    if (gu && tid < TB) gu[int64_t(p) * uld + tid] = tid >= p ? c[tid] : 0.0;
     double cs[4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) cs[b] = c[4 * bs + b];
@@ -197,6 +198,13 @@ __device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F,
     for (int r = 0; r < 4; ++r) dis[4 * bi + r] = 1.0 / sqrt(v[r][r]);
   }
   sync();
+  if (gu)  // U[p][i] = c_p[i] / sqrt(d_p) for i > p, sqrt(d_p) on the diagonal
+    for (int e = tid; e < TB * TB; e += 256) {
+      const int p = e >> 6, i = e & 63;
+      double *u = gu + int64_t(p) * uld + i;
+      if (i > p) *u = *u * dis[p];
+      else if (i == p) *u = 1.0 / dis[p];
+    }
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int i = 4 * bi + r;
@@ -698,35 +706,54 @@ __device__ __forceinline__ void ws_mma_half(uint32_t tmem, uint32_t sA, uint32_t
 }
 
 // Epilogue warp e (warp 2 + e) reads TMEM lanes 32 qd .. + 31 (qd = warp % 4)
-// and columns 32 h .. + 31 (h = e / 4) of every column group: v[c] = the
-// level sum of its half of row r (lanes 0..63: levels g + 2, rows r = lane;
-// lanes 64..127: levels g + 3, rows r = lane - 64).
-__device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double (&v)[32]) {
+// and columns 32 h .. + 31 (h = e / 4) of every column group: the level sum
+// of its half of row r (lanes 0..63: levels g + 2, rows r = lane; lanes
+// 64..127: levels g + 3, rows r = lane - 64).  The levels are merged in int64
+// first (|level| < 2^31, so three or four of them shifted by 7 bits each stay
+// below 2^53 and convert exactly), then two FP64 terms; 8 columns at a time,
+// one TMEM wait per 8 columns.  Lanes 0..63 subtract sig2 x their sum from
+// sC (which holds A); lanes 64..127 store theirs in sUp, which the caller
+// subtracts after a barrier.
+__device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *sC, double *sUp,
+                                         double sig2, int lane) {
   const uint32_t lane_base = uint32_t(32 * qd) << 16;
-  const int up = qd >= 2 ? 1 : 0;
+  const bool up = qd >= 2;
+  const int ng = up ? kOzS - 1 : kOzS;  // upper lanes: group 6 holds level 9, not read
 #pragma unroll
-  for (int c = 0; c < 32; ++c) v[c] = 0.0;
+  for (int cb = 0; cb < 4; ++cb) {
+    uint32_t z[kOzS][8];
 #pragma unroll
-  for (int g = 0; g < kOzS; ++g) {
-    if (up && g == kOzS - 1) break;  // level 9
-    uint32_t z[32];
-    const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h);
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(z[0]), "=r"(z[1]), "=r"(z[2]), "=r"(z[3]), "=r"(z[4]), "=r"(z[5]), "=r"(z[6]),
-          "=r"(z[7]), "=r"(z[8]), "=r"(z[9]), "=r"(z[10]), "=r"(z[11]), "=r"(z[12]), "=r"(z[13]),
-          "=r"(z[14]), "=r"(z[15])
-        : "r"(addr));
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(z[16]), "=r"(z[17]), "=r"(z[18]), "=r"(z[19]), "=r"(z[20]), "=r"(z[21]),
-          "=r"(z[22]), "=r"(z[23]), "=r"(z[24]), "=r"(z[25]), "=r"(z[26]), "=r"(z[27]),
-          "=r"(z[28]), "=r"(z[29]), "=r"(z[30]), "=r"(z[31])
-        : "r"(addr + 16));
+    for (int g = 0; g < kOzS; ++g) {
+      if (g >= ng) break;
+      const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h + 8 * cb);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+          : "=r"(z[g][0]), "=r"(z[g][1]), "=r"(z[g][2]), "=r"(z[g][3]), "=r"(z[g][4]),
+            "=r"(z[g][5]), "=r"(z[g][6]), "=r"(z[g][7])
+          : "r"(addr));
+    }
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    const double sc = ldexp(1.0, -7 * (g + 2 + up));
 #pragma unroll
-    for (int c = 0; c < 32; ++c) v[c] = __fma_rn(double(int32_t(z[c])), sc, v[c]);
+    for (int c = 0; c < 8; ++c) {
+      const long long z0 = int32_t(z[0][c]), z1 = int32_t(z[1][c]), z2 = int32_t(z[2][c]);
+      const long long z3 = int32_t(z[3][c]), z4 = int32_t(z[4][c]), z5 = int32_t(z[5][c]);
+      const long long hi = (z0 * 128 + z1) * 128 + z2;
+      double val;
+      if (!up) {
+        const long long lo = ((z3 * 128 + z4) * 128 + z5) * 128 + int32_t(z[6][c]);
+        val = __fma_rn(double(hi), 0x1p-28, double(lo) * 0x1p-56);  // levels 2..4, 5..8
+      } else {
+        const long long lo = (z3 * 128 + z4) * 128 + z5;
+        val = __fma_rn(double(hi), 0x1p-35, double(lo) * 0x1p-56);  // levels 3..5, 6..8
+      }
+      const int col = 32 * h + 8 * cb + c;
+      if (!up) {
+        double *cr = sC + (32 * qd + lane) * LDS + col;
+        *cr = __fma_rn(-sig2, val, *cr);
+      } else {
+        sUp[(32 * (qd - 2) + lane) * LDS + col] = val;
+      }
+    }
   }
 }
 
@@ -861,6 +888,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     if (etid == 0) *ep_stop = 0;
     ws_sync();
     int xq = -1;  // slot whose U_j (factor of the diagonal tile, transposed) is in sX
+    int pq = -1, ptj = -1;  // slot and column tile whose points are in pts
     int k = 0;
     for (int it = it0; it < it1; ++it, ++k) {
       const WsItem w = ws_item(ipre, cnt, it);
@@ -877,11 +905,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         xq = w.q;
         fresh = true;
       }
-      // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run.
-      gen_tile(a, sl, i, diag ? j + 1 : j, TB, sC, pts, etid, 256, ws_sync);
+      // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run; the
+      // column points stay in pts while the slot and column tile do.
+      const int tj = diag ? j + 1 : j;
+      gen_tile(a, sl, i, tj, TB, sC, pts, etid, 256, ws_sync, pq != w.q || ptj != tj);
+      pq = w.q;
+      ptj = tj;
       ws_sync();
       // Drain the accumulator, then hand it back to the MMA thread.
-      double v[32];
       // Every epilogue thread waits; the decision to stop is made uniform
       // through ep_stop (the global abort flag may change at any time).
       if (!mbar_wait_pipe(&bar->acc_full, uint32_t(k & 1), a.wait_limit, abort_flag)) *ep_stop = 1;
@@ -891,21 +922,16 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         break;
       }
       tc_fence_after();
-      ws_drain(tmem, qd, h, v);
+      // C = A - sigma^2 (lower-lane levels + upper-lane levels); the upper
+      // lanes' sums go through sL (free until the finisher).
+      ws_drain(tmem, qd, h, sC, sL, a.oz_sig2, lane);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cnt(&bar->acc_empty, 1);
-      // C = A - sigma^2 (lower-lane levels + upper-lane levels), in two turns.
-      if (qd < 2) {
-        double *Cr = sC + (32 * qd + lane) * LDS + 32 * h;
-#pragma unroll
-        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
-      }
       ws_sync();
-      if (qd >= 2) {
-        double *Cr = sC + (32 * (qd - 2) + lane) * LDS + 32 * h;
-#pragma unroll
-        for (int c = 0; c < 32; ++c) Cr[c] = __fma_rn(-a.oz_sig2, v[c], Cr[c]);
+      for (int e = etid; e < TB * TB; e += 256) {
+        const int r = e >> 6, c = e & 63;
+        sC[r * LDS + c] = __fma_rn(-a.oz_sig2, sL[r * LDS + c], sC[r * LDS + c]);
       }
       ws_sync();
       bool finish = false;
