@@ -40,6 +40,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "target pts/s, 1M→1M RBF-PUM: batched FP32+refine vs plain FP64 GPU @1e-10 err"
 UNIT = "target pts/s"
+# int8 64x64x64 digit products per FP64-equivalent tile product of the mixed
+# Cholesky: slice pairs (a, b) of 7 slices with a + b <= 9.
+I8_DIGIT_PRODUCTS = sum(min(7, 9 - a) for a in range(1, 8))
 
 
 def parse():
@@ -628,7 +631,7 @@ def main():
         extra["many_uneven_256"] = batch
 
     # Roofline of the dominant kernel: the int8 step kernel of the large-patch
-    # Cholesky (k_col_step_oz).  One extra transfer after the timed region,
+    # Cholesky (k_col_step_ws).  One extra transfer after the timed region,
     # in the timed configuration (all slot groups on their streams), with CUDA
     # events around every step launch on the stream it runs on; the span of
     # each kind is the union of its launch intervals.
@@ -640,23 +643,23 @@ def main():
     plan.close()
     tile_flops = 2.0 * 64 ** 3
     ms_i8 = kst.get("ms_update_i8", 0.0)
-    prod_i8 = kst.get("update_flops_i8", 0.0) / tile_flops
+    prod_i8 = kst.get("mma_products_i8", 0.0)
     ms_f64 = kst.get("ms_update_f64", 0.0)
-    # Algorithmic work of one int8 tile product: 28 int8 digit products of
-    # 64x64x64 (slice pairs a + b <= 8 of 7 slices) and the 7 int8 slices of
+    # Algorithmic work of one int8 tile product: 34 int8 digit products of
+    # 64x64x64 (slice pairs a + b <= 9 of 7 slices) and the 7 int8 slices of
     # one 64x64 L tile read from HBM (the shared tile row comes from L2).
-    i8_ops = prod_i8 * 28 * tile_flops
+    i8_ops = prod_i8 * I8_DIGIT_PRODUCTS * tile_flops
     i8_bytes = prod_i8 * 7 * 64 * 64
     int8_peak = 2.0 * peaks["bf16_tflops"]
     nl = max(1, int(kst.get("update_launches_i8", 0)))
     ach = i8_ops / (ms_i8 * 1e-3) / 1e12 if ms_i8 else 0.0
     hbm_ach = i8_bytes / (ms_i8 * 1e-3) / 1e9 if ms_i8 else 0.0
-    traffic_per_product = read_profile_value("dram_bytes_per_tile_product[k_col_step_oz]")
+    traffic_per_product = read_profile_value("dram_bytes_per_tile_product[k_col_step_ws]")
     roofline = {
         "bound": "tensor",
-        "kernel": "k_col_step_oz (left-looking Cholesky step of the large patches: column "
+        "kernel": "k_col_step_ws (left-looking Cholesky step of the large patches: column "
                   "update on the int8 tensor cores, tcgen05.mma kind::i8, 7-slice split-integer "
-                  "FP64 emulation; trsm; next diagonal tile)",
+                  "FP64 emulation, levels 2..9; triangular solve; next diagonal tile)",
         "achieved": ach, "peak": int8_peak, "unit": "TFLOP/s",
         "frac": ach / int8_peak if int8_peak else None,
         "peak_source": "int8 dense = 2 x bf16 dense, " + peaks["source"]

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PACMAN_B200_ABI_VERSION 4
+#define PACMAN_B200_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define PACMAN_B200_API __attribute__((visibility("default")))
@@ -107,7 +107,9 @@ typedef struct pacman_b200_stats {
    * (PACMAN_B200_KEEP_FACTORS). */
   int64_t factors_reused;
   /* The same three figures per kind of step launch: the column updates on
-   * the int8 tensor cores (k_col_step_oz) and those in FP64 (k_col_step). */
+   * the int8 tensor cores (k_col_step_ws) and those in FP64 (k_col_step).
+   * The FLOPs of a step count (j + 1) tile products per row tile: the j of
+   * the column update and one for the triangular solve. */
   double ms_update_i8;
   double update_flops_i8;
   int64_t update_launches_i8;
@@ -116,6 +118,10 @@ typedef struct pacman_b200_stats {
   int64_t update_launches_f64;
   /* Host synchronisations (waits for the device) inside the call. */
   int64_t host_syncs;
+  /* 64 x 64 x 64 tile products of the column updates on the int8 tensor
+   * cores alone (j per row tile and per next diagonal tile at step j); each
+   * is 34 int8 digit products (slice pairs a + b <= 9 of 7 slices). */
+  double mma_products_i8;
 } pacman_b200_stats;
 
 /* Fills the reference's defaults (50, 0.15, 0.1, FP64, current device). */

@@ -71,6 +71,7 @@ class Stats(ctypes.Structure):
         ("update_flops_f64", ctypes.c_double),
         ("update_launches_f64", ctypes.c_int64),
         ("host_syncs", ctypes.c_int64),
+        ("mma_products_i8", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

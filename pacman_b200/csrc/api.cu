@@ -296,6 +296,7 @@ int execute_plan(pacman_b200_plan *h, int32_t basis, const double *vals, int32_t
       stats->ms_update_f64 = rep.ms_kind[0];
       stats->update_flops_f64 = rep.flops_kind[0];
       stats->update_launches_f64 = rep.launches_kind[0];
+      stats->mma_products_i8 = rep.mma_products_i8;
       stats->factors_reused = rep.factors_reused;
     }
     cudaEventDestroy(e0);
@@ -670,6 +671,7 @@ int run_batch(const pacman_b200_problem *qs, int32_t count, const pacman_b200_op
       stats->ms_update_f64 = rep.ms_kind[0];
       stats->update_flops_f64 = rep.flops_kind[0];
       stats->update_launches_f64 = rep.launches_kind[0];
+      stats->mma_products_i8 = rep.mma_products_i8;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -351,11 +351,10 @@ __device__ __forceinline__ void load_inv(double *s, const double *g, int tid, in
 // workspace (unit lower L below the diagonal, U on and above it, or the
 // Cholesky factor below and on it): backward stable, unlike a product with
 // the explicit inverse, whose error grows with the condition number of the
-// diagonal tile.  Each warp solves 16 rows of X (column panel) or 16 columns
-// (row panel, as rows of X^T against L^T), in two passes of 8
-// (warp_row_solve).
+// diagonal tile.  Each of the 8 warps solves 8 rows of X (column panel) or 8
+// columns (row panel, as rows of X^T against L^T) with warp_row_solve.
 template <bool LU>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
     k_trsm(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ pre, int cnt,
            int s) {
   extern __shared__ double sm[];
@@ -385,8 +384,8 @@ __global__ void __launch_bounds__(128)
   __syncthreads();
   if (tid < TB) dinv[tid] = (LU && left) ? 1.0 : 1.0 / sU[tid * LDS + tid];
   __syncthreads();
-  for (int pass = 0; pass < 2; ++pass) {
-    const int r0 = 16 * warp + 8 * pass;
+  {
+    const int r0 = 8 * warp;
     double lo[8], hi[8];
 #pragma unroll
     for (int qq = 0; qq < 8; ++qq) {
@@ -744,7 +743,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     }
   }
   // The forward Cholesky of precision "mixed" runs its column updates on the
-  // int8 tensor cores (k_col_step_oz); PACMAN_B200_INT8=0 keeps them in FP64.
+  // int8 tensor cores (k_col_step_ws); PACMAN_B200_INT8=0 keeps them in FP64.
   const char *i8env = std::getenv("PACMAN_B200_INT8");
   const bool oz = !lu && !adjoint && !(i8env && std::atoi(i8env) == 0);
   if (oz) {
@@ -957,7 +956,7 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       const int nt = pre[off[s] + c];
       const int nu = pre[off[s] + c + 1 + c];
       k_diag<true><<<c, 256, s3, st>>>(a, ds, s);
-      if (nt) k_trsm<true><<<nt, 128, s2, st>>>(a, ds, pt, c, s);
+      if (nt) k_trsm<true><<<nt, 256, s2, st>>>(a, ds, pt, c, s);
       if (nu) k_update_strip<true><<<nu, 128, s3, st>>>(a, ds, pu, c, s);
       note_launch(1 + (nt ? 1 : 0) + (nu ? 1 : 0));
     }

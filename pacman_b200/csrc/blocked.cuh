@@ -158,10 +158,114 @@ __device__ __forceinline__ void warp_row_solve(double (&lo)[R], double (&hi)[R],
   }
 }
 
+// In-place row solve X U = C for 8 rows (row stride LDS, 64 columns) by one
+// warp, blocked by 16 columns, all in registers: lane l holds column
+// 16 b + l % 16 of rows l / 16 + 2 q (q = 0..3) for the four column blocks
+// b.  Block b is solved by right-looking substitution against U's 16 x 16
+// diagonal block, then the blocks right of it are updated with the block's
+// result (broadcast by shuffles) times U's off-diagonal block, by FMAs on the
+// FP64 pipe: on B200 the FP64 tensor instructions are no faster than FMAs and
+// would compete with the int8 tensor-core MMAs of the same SM.  U: upper
+// triangular with exact zeros below the diagonal; dinv[c] = 1 / U[c][c].
+// Only the warp's own rows are touched, so no block barrier is needed; this
+// is a blocked triangular solve (diagonal blocks by substitution, off-
+// diagonal blocks by products), backward stable.
+__device__ __forceinline__ void warp_rows_trsm8(double *rows, const double *sU,
+                                                const double *dinv, int lane) {
+  const int col16 = lane & 15, half = lane & 16, rsel = lane >> 4;
+  double v[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[b][q] = rows[(rsel + 2 * q) * LDS + 16 * b + col16];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int cb = 16 * b;
+#pragma unroll 4
+    for (int c = 0; c < 16; ++c) {
+      const double d = dinv[cb + c];
+      const double u = sU[(cb + c) * LDS + cb + col16];
+      const bool own = col16 == c;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double x = __shfl_sync(0xffffffffu, v[b][q], half | c) * d;
+        v[b][q] = own ? x : __fma_rn(-x, u, v[b][q]);
+      }
+    }
+    if (b < 3) {
+#pragma unroll 4
+      for (int k = 0; k < 16; ++k) {
+        double x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = __shfl_sync(0xffffffffu, v[b][q], half | k);
+        const double *ur = sU + (cb + k) * LDS + col16;
+#pragma unroll
+        for (int bb = b + 1; bb < 4; ++bb) {
+          const double u = ur[16 * bb];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[bb][q] = __fma_rn(-x[q], u, v[bb][q]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rows[(rsel + 2 * q) * LDS + 16 * b + col16] = v[b][q];
+  __syncwarp();
+}
+
+// warp_rows_trsm8 with the off-diagonal block products on the FP64 tensor
+// cores (mma.sync m8n8k4) through shared memory, for the FP64 step kernel,
+// which runs no int8 MMAs and has fewer registers to spare.
+__device__ __forceinline__ void warp_rows_trsm8_tc(double *rows, const double *sU,
+                                                   const double *dinv, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int col16 = lane & 15, half = lane & 16, rsel = lane >> 4;
+#pragma unroll 1
+  for (int b = 0; b < 4; ++b) {
+    const int cb = 16 * b;
+    double acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = rows[(rsel + 2 * q) * LDS + cb + col16];
+#pragma unroll 4
+    for (int c = 0; c < 16; ++c) {
+      const double d = dinv[cb + c];
+      const double u = sU[(cb + c) * LDS + cb + col16];
+      const bool own = col16 == c;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double x = __shfl_sync(0xffffffffu, acc[q], half | c) * d;
+        acc[q] = own ? x : __fma_rn(-x, u, acc[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rows[(rsel + 2 * q) * LDS + cb + col16] = acc[q];
+    __syncwarp();
+    // Columns to the right: C[:, n] -= X_b U[b, n], 8-column tiles.
+    for (int nt = 2 * b + 2; nt < 8; ++nt) {
+      double c0 = rows[g * LDS + 8 * nt + 2 * t], c1 = rows[g * LDS + 8 * nt + 2 * t + 1];
+#pragma unroll
+      for (int k0 = 0; k0 < 16; k0 += 4) {
+        const double av = -rows[g * LDS + cb + k0 + t];
+        const double bv = sU[(cb + k0 + t) * LDS + 8 * nt + g];
+        dmma(c0, c1, av, bv);
+      }
+      rows[g * LDS + 8 * nt + 2 * t] = c0;
+      rows[g * LDS + 8 * nt + 2 * t + 1] = c1;
+    }
+    __syncwarp();
+  }
+}
+
 // Asynchronous 16-byte global -> shared copies (cp.async, sm_80+).
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {

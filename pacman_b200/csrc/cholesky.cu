@@ -106,141 +106,141 @@ __device__ __forceinline__ void gen_tile(const BigArgs &a, const BigSlot &sl, in
 
 __device__ __forceinline__ void sync_all() { __syncthreads(); }
 
-// Inverse Cholesky factor X of one 64 x 64 tile D and y = X r (256 threads).  The tile is eliminated as L D L^T with the identity carried
-// along (Gauss-Jordan on [A | I]): at pivot p every row i > p gets
-// R_i -= (a_ip / a_pp) R_p, which leaves U = D L^T on the left and L^{-1} on
-// the right.  Each thread owns a 4 x 4 block of registers; slot (i, s) holds
-// A[i][s] until pivot s and L^{-1}[i][s] afterwards.  Per pivot the owners
-// publish one vector (row p of L^{-1} left of the pivot, the pivot, column p
-// of A below it) and all threads update their slots: one barrier per pivot.
-// X = L_c^{-1} = D^{-1/2} L^{-1} is kept for the forward and backward
-// substitutions; with gu, the factor itself is written too, as U = L_c^T
-// (row p = column p of L_c, from the pivot column c / sqrt(pivot)), for the
-// triangular solves of the tiles below (a trsm by substitution: multiplying by
-// the explicit inverse loses accuracy on ill-conditioned tiles).
-// Non-positive pivots set status 4.
-// D: lower part at g (row stride ld, global or shared); r: the first F
-// columns of the residual tile at rg (row stride rld), overwritten with y; X
-// goes to gi (row stride TB).  Xs (TB x LDS), cv, dis and ys are shared
-// scratch.  Returns true on a non-positive pivot.
-template <class Sync>
-__device__ bool diag_tile_t(const double *g, int ld, double *rg, int rld, int F, double *gi,
-                            double *Xs, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
+// The diagonal tile of a step, 256 threads (8 warps): the Cholesky factor
+// L_c of the 64 x 64 tile D (lower part, in shared memory at g with row stride
+// ld, overwritten), X = L_c^{-1} (to gi, row stride TB), y = X r for the first
+// F columns of the residual tile (rg, row stride rld, overwritten) and, with
+// gu, U = L_c^T (row stride uld; zeros below its diagonal) for the triangular
+// solves of the tiles below.  Blocked right-looking Cholesky in 16 x 16
+// blocks: warp 0 factors the diagonal block (16 column steps synchronised
+// within the warp), the eight warps solve the panel below it by substitution
+// and update the trailing blocks on the FP64 tensor cores, three barriers per
+// block.  X comes from the row solves X^T U = I (warp_rows_trsm8, or with
+// kTensorSolve warp_rows_trsm8_tc).  Us (TB x LDS) is shared scratch for U,
+// dis (TB) for 1 / diag(L_c), ys (TB x kMaxF) for r.  Returns true on a
+// non-positive pivot (status 4 for the caller).
+template <class Sync, bool kTensorSolve = false>
+__device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int F, double *gi,
+                            double *Us, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
                             int tid, Sync sync, double *gu = nullptr, int uld = 0) {
-  const int bi = tid >> 4, bs = tid & 15;
+  (void)cv;
+  double *D = const_cast<double *>(g_in);
+  const int lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int col16 = lane & 15, half = lane & 16, rsel = lane >> 4;
   bool bad = false;
-  double v[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const double2 lo = *reinterpret_cast<const double2 *>(g + int64_t(4 * bi + r) * ld + 4 * bs);
-    const double2 hi = *reinterpret_cast<const double2 *>(g + int64_t(4 * bi + r) * ld + 4 * bs + 2);
-    v[r][0] = lo.x;
-    v[r][1] = lo.y;
-    v[r][2] = hi.x;
-    v[r][3] = hi.y;
-  }
   for (int e = tid; e < TB * kMaxF; e += 256) {
     const int r = e / kMaxF, f = e % kMaxF;
     ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
   }
-  for (int p = 0; p < TB; ++p) {
-    double *c = cv[p & 1];
-    const int pb = p >> 2, pr = p & 3;
-    if (bi == pb) {  // row p: L^{-1}[p][s] for s < p, the pivot at s = p
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (4 * bs + b <= p) {
-          double x = v[0][b];
-          if (pr == 1) x = v[1][b];
-          if (pr == 2) x = v[2][b];
-          if (pr == 3) x = v[3][b];
-          c[4 * bs + b] = x;
+  for (int kb = 0; kb < TB; kb += 16) {
+    // (a) the diagonal block, warp 0.
+    if (warp == 0) {
+      for (int c = 0; c < 16; ++c) {
+        const int p = kb + c;
+        const double piv = D[p * ld + p];
+        bad |= !(piv > 0.0);
+        const double sq = sqrt(piv), rs = __drcp_rn(sq);
+        if (col16 > c && half == 0) D[(kb + col16) * ld + p] *= rs;
+        if (lane == 0) {
+          D[p * ld + p] = sq;
+          dis[p] = rs;
         }
-    }
-    if (bs == pb) {  // column p below the pivot: A[i][p], i > p
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (4 * bi + r > p) {
-          double x = v[r][0];
-          if (pr == 1) x = v[r][1];
-          if (pr == 2) x = v[r][2];
-          if (pr == 3) x = v[r][3];
-          c[4 * bi + r] = x;
+        __syncwarp();
+        // Trailing part of the block: lane i (row kb + i) updates its row.
+        if (half == 0 && col16 > c) {
+          const int i = kb + col16;
+          const double lip = D[i * ld + p];
+          for (int jj = c + 1; jj <= col16; ++jj)
+            D[i * ld + kb + jj] = __fma_rn(-lip, D[(kb + jj) * ld + p], D[i * ld + kb + jj]);
         }
-    }
-    sync();
-    const double piv = c[p];
-    bad |= !(piv > 0.0);
-    const double inv = __drcp_rn(piv);
-    // Row p of U = L_c^T is column p of the Cholesky factor, c / sqrt(pivot):
-    // the unscaled column now, the scaling once the loop is over.
-    if (gu && tid < TB) gu[int64_t(p) * uld + tid] = tid >= p ? c[tid] : 0.0;
-    double cs[4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) cs[b] = c[4 * bs + b];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = 4 * bi + r;
-      if (i > p) {
-        const double m = c[i] * inv;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int sc = 4 * bs + b;
-          if (sc == p) v[r][b] = -m;
-          else if (sc <= i) v[r][b] = __fma_rn(-m, cs[b], v[r][b]);
-        }
+        __syncwarp();
       }
     }
-  }
-  // X[i][s] = L^{-1}[i][s] / sqrt(d_i); d_i is the final diagonal slot.
-  if (bi == bs) {
+    sync();
+    // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d.
+    const int r0 = kb + 16 + 8 * warp;
+    if (r0 < TB) {
+      double acc[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) dis[4 * bi + r] = 1.0 / sqrt(v[r][r]);
+      for (int q = 0; q < 4; ++q) acc[q] = D[(r0 + rsel + 2 * q) * ld + kb + col16];
+#pragma unroll 4
+      for (int c = 0; c < 16; ++c) {
+        const double d = dis[kb + c];
+        const double l = D[(kb + col16) * ld + kb + c];  // L_kk[col16][c], used for col16 > c
+        const bool own = col16 == c, below = col16 > c;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double x = __shfl_sync(0xffffffffu, acc[q], half | c) * d;
+          acc[q] = own ? x : (below ? __fma_rn(-x, l, acc[q]) : acc[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) D[(r0 + rsel + 2 * q) * ld + kb + col16] = acc[q];
+    }
+    sync();
+    // (c) trailing blocks: D[i, j] -= P_i P_j^T (P: the panel columns), 8 x 8
+    // output tiles (ti, tj) with kb + 16 <= 8 tj <= 8 ti, four per warp step.
+    {
+      const int base = (kb + 16) / 8, nt = 8 - base;
+      for (int u = warp; u < nt * nt; u += 8) {
+        const int ti = base + u / nt, tj = base + u % nt;
+        if (tj > ti) continue;
+        double c0 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq];
+        double c1 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1];
+#pragma unroll
+        for (int k0 = 0; k0 < 16; k0 += 4) {
+          const double av = -D[(8 * ti + gq) * ld + kb + k0 + tq];
+          const double bv = D[(8 * tj + gq) * ld + kb + k0 + tq];
+          dmma(c0, c1, av, bv);
+        }
+        D[(8 * ti + gq) * ld + 8 * tj + 2 * tq] = c0;
+        D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1] = c1;
+      }
+    }
+    sync();
+  }
+  // U = L_c^T with zeros below its diagonal; 1 / diag for the row solves.
+  for (int e = tid; e < TB * TB; e += 256) {
+    const int p = e >> 6, i = e & 63;
+    const double u = i >= p ? D[i * ld + p] : 0.0;
+    Us[p * LDS + i] = u;
+    if (gu) gu[int64_t(p) * uld + i] = u;
   }
   sync();
-  if (gu)  // U[p][i] = c_p[i] / sqrt(d_p) for i > p, sqrt(d_p) on the diagonal
-    for (int e = tid; e < TB * TB; e += 256) {
-      const int p = e >> 6, i = e & 63;
-      double *u = gu + int64_t(p) * uld + i;
-      if (i > p) *u = *u * dis[p];
-      else if (i == p) *u = 1.0 / dis[p];
-    }
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const int i = 4 * bi + r;
-    const double di = dis[i];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int sc = 4 * bs + b;
-      Xs[i * LDS + sc] = sc < i ? v[r][b] * di : (sc == i ? di : 0.0);
-    }
-  }
+  // X^T from X^T U = I: rows of the identity solved in place of D.
+  for (int e = tid; e < TB * TB; e += 256) D[(e >> 6) * ld + (e & 63)] = (e >> 6) == (e & 63);
   sync();
-  // y_j = X r_j (first F columns of the residual tile).
-  double yv[2];
-  int ny = 0;
+  if (kTensorSolve) warp_rows_trsm8_tc(D + 8 * warp * ld, Us, dis, lane);
+  else warp_rows_trsm8(D + 8 * warp * ld, Us, dis, lane);
+  sync();
+  // X (row-major, gi) and y = X r.
+  for (int e = tid; e < TB * TB; e += 256) {
+    const int r = e >> 6, c = e & 63;
+    gi[r * TB + c] = D[c * ld + r];
+  }
   for (int e = tid; e < TB * F; e += 256) {
     const int r = e / F, f = e % F;
     double s = 0.0;
-    for (int k = 0; k <= r; ++k) s = __fma_rn(Xs[r * LDS + k], ys[k][f], s);
-    yv[ny++] = s;
+    for (int k = 0; k <= r; ++k) s = __fma_rn(D[k * ld + r], ys[k][f], s);
+    rg[int64_t(r) * rld + f] = s;
   }
-  ny = 0;
-  for (int e = tid; e < TB * F; e += 256) rg[int64_t(e / F) * rld + e % F] = yv[ny++];
-  for (int idx = tid; idx < TB * TB / 2; idx += 256) {
-    const int r = idx >> 5, c2 = idx & 31;
-    *reinterpret_cast<double2 *>(gi + r * TB + 2 * c2) =
-        *reinterpret_cast<const double2 *>(Xs + r * LDS + 2 * c2);
-  }
-  return bad;
+  // Every thread learns about a breakdown (warp 0 saw the pivots).
+  __shared__ int bad_any;
+  if (tid == 0) bad_any = 0;
+  sync();
+  if (bad) bad_any = 1;
+  sync();
+  return bad_any != 0;
 }
 
 __device__ __forceinline__ bool diag_tile(const double *g, int ld, double *rg, int rld, int F,
                                           double *gi, double *Xs, double (*cv)[TB], double *dis,
                                           double (*ys)[kMaxF], double *gu = nullptr,
                                           int uld = 0) {
-  return diag_tile_t(g, ld, rg, rld, F, gi, Xs, cv, dis, ys, int(threadIdx.x),
-                     [] { __syncthreads(); }, gu, uld);
+  auto sync = [] { __syncthreads(); };
+  return diag_tile_t<decltype(sync), true>(g, ld, rg, rld, F, gi, Xs, cv, dis, ys,
+                                            int(threadIdx.x), sync, gu, uld);
 }
 
 // The diagonal tile of step 0 of every slot.
@@ -266,10 +266,11 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
 // Phase 2 of a factorisation step (256 threads, warp w: rows 16 w .. + 15,
 // in two passes of 8).  sC holds C (row tiles i0, and i0 + 1 when arows =
 // 2 TB; kColRows x LDS).  L[i, j] solves L[i, j] U_j = C with U_j = L_jj^T
-// (the factor of the diagonal tile, loaded into sU), row by row
-// (warp_row_solve); it is stored in the workspace and written back over C in
-// sC; then the forward substitution r_i -= L[i, j] y_j.  vec holds TB + TB
-// kMaxF doubles (1 / diag(U_j), y_j).  Ends with a barrier.
+// (the factor of the diagonal tile, loaded into sU), by blocked row solves
+// (warp_rows_trsm8_tc); it is stored in the workspace and written back over C
+// in sC (in place); then the forward substitution r_i -=
+// L[i, j] y_j.  vec holds TB + TB kMaxF doubles (1 / diag(U_j), y_j).  Ends
+// with a barrier.
 __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, int arows,
                           double *sC, double *sU, double *vec) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -295,17 +296,12 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
   for (int pass = 0; pass < 2; ++pass) {
     const int r0 = 16 * warp + 8 * pass;
     if (r0 >= arows) break;
+    warp_rows_trsm8_tc(sC + r0 * LDS, sU, dinv, lane);
     double lo[8], hi[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       lo[q] = sC[(r0 + q) * LDS + lane];
       hi[q] = sC[(r0 + q) * LDS + 32 + lane];
-    }
-    warp_row_solve<8>(lo, hi, sU, dinv, lane);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      sC[(r0 + q) * LDS + lane] = lo[q];
-      sC[(r0 + q) * LDS + 32 + lane] = hi[q];
       C[int64_t(r0 + q) * ld + lane] = lo[q];
       C[int64_t(r0 + q) * ld + 32 + lane] = hi[q];
     }
@@ -331,9 +327,13 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
 // since the rows of L have norm sqrt(A_rr)): x = sum_s d_s 128^-s, d_1 in
 // [-127, 127], d_s in [-64, 64] after.  The update
 //   sum_p L[i, p] L[j, p]^T = sigma^2 sum_{a,b} 128^-(a+b) D_a[i] D_b[j]^T
-// keeps the slice pairs with a + b <= kOzS + 1 (27 levels of products dropped
-// below 128^-8 ~ 2^-56) and sums each level a + b exactly in int32 on the
-// tcgen05 tensor cores (kind::i8); the levels are combined in FP64 at the end.
+// keeps the slice pairs with a + b <= kOzS + 2 (levels 2..9) and sums each
+// level exactly in int32 on the tcgen05 tensor cores (kind::i8); the levels
+// are combined in int64 and FP64 at the end.  A digit product is at most
+// 2^12 in magnitude, so a dropped term (level >= 10) is below 2^-58 sigma^2:
+// the truncation of a K-long sum stays near the FP64 rounding of the same
+// sum.  Dropping level 9 as well (2^-51 per term) is not enough: on patches
+// with cond(A) ~ 1e13 it multiplies the error of the local values by ~15.
 // This is the split-integer emulation of an FP64 product (Ozaki, Ogita, Oishi
 // and Rump 2012; Uchino, Ozaki and Imamura 2024 for integer tensor cores).
 //
@@ -342,7 +342,7 @@ __device__ void step_trsm(const BigArgs &a, const BigSlot &sl, int j, int i0, in
 // core, copied to shared memory with bulk async copies.
 constexpr int kOzS = 7;
 constexpr int kOzTileBytes = 4 * kOzS * 8 * 128;      // 28672
-constexpr int kOzTmemCols = 512;                      // kOzS levels x 64 columns, rounded up
+constexpr int kOzTmemCols = 512;                      // 8 column groups of 64 (levels 2..9)
 constexpr int kOzWaitLimit = 1 << 22;                 // bounded mbarrier polls
 // Polls of the waits that drain a pipeline after it gave up: they wait for
 // copies and tensor-core operations already issued, which complete by
@@ -634,12 +634,14 @@ __global__ void __launch_bounds__(kColThreads, 2)
 // Warp-specialised int8 step (k_col_step_ws)
 // ---------------------------------------------------------------------------
 //
-// The same step as k_col_step_oz, organised so that the int8 K loop of one
-// item overlaps the FP64 epilogue of the previous one on the same SM.  An
-// item is one 64-row tile: row tile i of column j (C = A[i, j] - sum_{p<j}
-// L[i, p] L[j, p]^T, then L[i, j] = C X_j^T, the forward substitution and
-// the int8 slices of L[i, j]), or the diagonal item of a slot (D' of tile
-// j + 1).  Each CTA takes a contiguous range of the step's items.
+// Step j of the factorisation with the column update on the int8 tensor
+// cores, organised so that the int8 K loop of one item overlaps the FP64
+// epilogue of the previous one on the same SM.  An item is one 64-row tile:
+// row tile i of column j (C = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T, then
+// L[i, j] U_j = C solved against the diagonal tile's factor, the forward
+// substitution and the int8 slices of L[i, j]), or the diagonal item of a
+// slot (D' of tile j + 1).  Each CTA takes a contiguous range of the step's
+// items.
 //   warp 0 (one thread): bulk copies of the slice half-tiles (K = 32) of the
 //     item's row tile and of the column tile row through a kWsStages ring;
 //   warp 1 (one thread): the tcgen05 MMAs into one TMEM accumulator;
@@ -647,28 +649,37 @@ __global__ void __launch_bounds__(kColThreads, 2)
 //     drain (after which the MMA thread starts the next item), the level
 //     combination and the FP64 epilogue.
 // The MMA operand A holds two consecutive slices of the ONE row tile (rows
-// 0..63 slice a, 64..127 slice a + 1: the stored tile layout is already the
-// tensor core's, so a half-tile is one contiguous 14 KB copy), B the slices
-// of the column tile stacked along N.  With the accumulator of pair (a, a+1)
-// starting at TMEM column group a - 1, column group g (64 columns) holds
-// level g + 2 in lanes 0..63 and level g + 3 in lanes 64..127 whatever the
-// pair, so four pairs (1,2), (3,4), (5,6), (7,-) and six MMAs per K = 32
-// cover every slice pair with a + b <= 8 (products of level 9, in lanes
-// 64..127 of group 6, and of the missing slice 8 are not read).
+// 0..63 slice a, 64..127 slice a + 1), B the slices of the column tile
+// stacked along N.  With the accumulator of pair (a, a+1) starting at TMEM
+// column group a - 1, column group g (64 columns) holds level g + 2 in lanes
+// 0..63 and level g + 3 in lanes 64..127 whatever the pair, so four pairs
+// (1,2), (3,4), (5,6), (7,0) against the column slices 1..9-a and six MMAs
+// per K = 32 cover every slice pair with a + b <= 9: levels 2..9 are lanes
+// 0..63 of groups 0..7 and lanes 64..127 of groups 0..6 (lanes 64..127 of
+// group 7 hold a partial level 10, not read).  In shared memory a K = 32 half
+// of the row tile is staged as [K chunk (2)][slice (8)][8-row group (8)][128
+// B] with the eighth slice of each chunk kept zero, so that the pair (7, 0)
+// adds nothing to lanes 64..127; the column tile's half is the stored layout
+// itself ([K chunk (2)][slice (7)]...), one contiguous 14 KB copy.
 constexpr int kWsStages = 3;
-constexpr int kWsHalf = 2 * kOzS * 1024;                 // 14336: one K = 32 half of a slice tile
-constexpr int kWsStage = 2 * kWsHalf;                    // A half + B half
+constexpr int kWsChunk = kOzS * 1024;                    // 7168: one 16-byte K chunk, 7 slices
+constexpr int kWsHalf = 2 * kWsChunk;                    // 14336: one K = 32 half of a slice tile
+constexpr int kWsChunkA = (kOzS + 1) * 1024;             // staged row-tile chunk with a zero slice
+constexpr int kWsHalfA = 2 * kWsChunkA;                  // 16384
+constexpr int kWsStage = kWsHalfA + kWsHalf;             // row half + column half
 constexpr int kWsThreads = 320;                          // 2 issue warps + 8 epilogue warps
 constexpr int kWsCOff = kWsStages * kWsStage;            // C / D (TB x LDS doubles)
 constexpr int kWsXOff = kWsCOff + TB * LDS * 8;          // X_j, or diag_tile scratch
 constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // L[j+1, j] (finisher)
-constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // points of the evaluated tile
-constexpr int kWsRedOff = kWsPtsOff + 3 * 2 * TB * 8;    // y_j, reductions, diag_tile vectors
+constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // row points (2 x TB), column points
+constexpr int kWsRedOff = kWsPtsOff + 2 * TB * 32 + 3 * TB * 8;  // y_j, r_i, diag_tile vectors
 constexpr int kWsBarOff = kWsRedOff + 3 * TB * kMaxF * 8;
 constexpr size_t kWsSmem = size_t(kWsBarOff) + 256;
 static_assert(kWsSmem <= 232448, "shared memory of k_col_step_ws");
+static_assert(kWsStage % 1024 == 0, "stages start on 1 KB boundaries");
 static_assert(kOzTileBytes <= TB * LDS * 8, "slice staging does not fit the C buffer");
 static_assert((TB * kMaxF + 2 * TB + TB) * 8 <= 3 * TB * kMaxF * 8, "diag_tile vectors");
+static_assert(2 * TB * kMaxF + 3 * TB <= 3 * TB * kMaxF, "residual rows after the diag_tile vectors");
 
 struct WsBars {
   uint64_t full[kWsStages], empty[kWsStages], acc_full, acc_empty, done;
@@ -686,44 +697,69 @@ __device__ __forceinline__ WsItem ws_item(const int *ipre, int cnt, int it) {
   const int q = find_slot(ipre, cnt, it);
   return {q, it - ipre[q]};
 }
+// The items of a CTA's range in order: one binary search for the first,
+// then the slot advances when the item passes the next slot's first item
+// (the slot record is reloaded only then).
+struct WsCursor {
+  int q = -1, first = 0, next = 0;
+  BigSlot sl;
+  int64_t s0 = 0;  // first membership entry of the slot's patch (with soff)
+  __device__ __forceinline__ WsItem at(const int *ipre, const BigSlot *slots, const int64_t *soff,
+                                       int cnt, int it) {
+    if (q < 0 || it >= next) {
+      if (q < 0) q = find_slot(ipre, cnt, it);
+      else
+        do ++q;
+        while (it >= ipre[q + 1]);
+      first = ipre[q];
+      next = ipre[q + 1];
+      sl = slots[q];
+      if (soff) s0 = soff[sl.k];
+    }
+    return {q, it - first};
+  }
+};
 
-// Six MMAs of one K = 32 half: pairs (1,2), (3,4), (5,6), (7,-) of the row
-// tile's slices against the column tile's slices 1..8-a stacked along N.
+// Six MMAs of one K = 32 half: pairs (1,2), (3,4), (5,6), (7,0) of the row
+// tile's slices against the column tile's slices 1..9-a stacked along N.  On
+// the first half of an item the first MMA to reach a column overwrites it:
+// pair (1, 2) groups 0..3, pair (5, 6) groups 4..7, issued first.
 __device__ __forceinline__ void ws_mma_half(uint32_t tmem, uint32_t sA, uint32_t sB, bool first) {
-  constexpr uint32_t kLbo = kOzS * 1024;  // between the two 16-byte K chunks of a half
-  const uint64_t b0 = umma_desc(sB, kLbo, 128), b4 = umma_desc(sB + 4 * 1024, kLbo, 128);
+  const uint64_t b0 = umma_desc(sB, kWsChunk, 128), b4 = umma_desc(sB + 4 * 1024, kWsChunk, 128);
   const uint32_t acc = first ? 0u : 1u;
-  uint64_t ad = umma_desc(sA, kLbo, 128);                 // pair (1, 2): groups 0..6
-  umma_i8(tmem, ad, b0, umma_idesc_i8(256), acc);
-  umma_i8(tmem + 256, ad, b4, umma_idesc_i8(192), acc);
-  ad = umma_desc(sA + 2 * 1024, kLbo, 128);               // pair (3, 4): groups 2..6
-  umma_i8(tmem + 128, ad, b0, umma_idesc_i8(256), 1u);
-  umma_i8(tmem + 384, ad, b4, umma_idesc_i8(64), 1u);
-  ad = umma_desc(sA + 4 * 1024, kLbo, 128);               // pair (5, 6): groups 4..6
-  umma_i8(tmem + 256, ad, b0, umma_idesc_i8(192), 1u);
-  ad = umma_desc(sA + 6 * 1024, kLbo, 128);               // pair (7, -): group 6
-  umma_i8(tmem + 384, ad, b0, umma_idesc_i8(64), 1u);
+  const uint64_t a12 = umma_desc(sA, kWsChunkA, 128);
+  const uint64_t a34 = umma_desc(sA + 2 * 1024, kWsChunkA, 128);
+  const uint64_t a56 = umma_desc(sA + 4 * 1024, kWsChunkA, 128);
+  const uint64_t a70 = umma_desc(sA + 6 * 1024, kWsChunkA, 128);
+  umma_i8(tmem, a12, b0, umma_idesc_i8(256), acc);          // (1,2) x 1..4: groups 0..3
+  umma_i8(tmem + 256, a56, b0, umma_idesc_i8(256), acc);    // (5,6) x 1..4: groups 4..7
+  umma_i8(tmem + 256, a12, b4, umma_idesc_i8(192), 1u);     // (1,2) x 5..7: groups 4..6
+  umma_i8(tmem + 128, a34, b0, umma_idesc_i8(256), 1u);     // (3,4) x 1..4: groups 2..5
+  umma_i8(tmem + 384, a34, b4, umma_idesc_i8(128), 1u);     // (3,4) x 5..6: groups 6..7
+  umma_i8(tmem + 384, a70, b0, umma_idesc_i8(128), 1u);     // (7,0) x 1..2: groups 6..7
 }
 
 // Epilogue warp e (warp 2 + e) reads TMEM lanes 32 qd .. + 31 (qd = warp % 4)
-// and columns 32 h .. + 31 (h = e / 4) of every column group: the level sum
-// of its half of row r (lanes 0..63: levels g + 2, rows r = lane; lanes
-// 64..127: levels g + 3, rows r = lane - 64).  The levels are merged in int64
-// first (|level| < 2^31, so three or four of them shifted by 7 bits each stay
-// below 2^53 and convert exactly), then two FP64 terms; 8 columns at a time,
-// one TMEM wait per 8 columns.  Lanes 0..63 subtract sig2 x their sum from
-// sC (which holds A); lanes 64..127 store theirs in sUp, which the caller
-// subtracts after a barrier.
+// and columns 32 h .. + 31 (h = e / 4) of the column groups: the level sums of
+// its half of row r (lanes 0..63: levels 2..9 in groups 0..7, rows r = lane;
+// lanes 64..127: levels 3..9 in groups 0..6, rows r = lane - 64).  The levels
+// are merged in int64 first: |level| < 2^31, so the top three shifted by 7
+// bits each stay below 2^53 and convert exactly, and the lower four or five
+// (below 2^60 in units of 128^-9) round to within 2^-57; then two FP64
+// terms (in units of sigma^2).  8 columns at a time, one TMEM wait per 8 columns.  Lanes 0..63
+// subtract sig2 x their sum from sC (which holds A); lanes 64..127 store
+// theirs in sUp, which the caller subtracts after a barrier.
 __device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *sC, double *sUp,
                                          double sig2, int lane) {
+  constexpr int kG = kOzS + 1;  // column groups 0..7
   const uint32_t lane_base = uint32_t(32 * qd) << 16;
   const bool up = qd >= 2;
-  const int ng = up ? kOzS - 1 : kOzS;  // upper lanes: group 6 holds level 9, not read
+  const int ng = up ? kG - 1 : kG;  // upper lanes: group 7 holds a partial level 10
 #pragma unroll
   for (int cb = 0; cb < 4; ++cb) {
-    uint32_t z[kOzS][8];
+    uint32_t z[kG][8];
 #pragma unroll
-    for (int g = 0; g < kOzS; ++g) {
+    for (int g = 0; g < kG; ++g) {
       if (g >= ng) break;
       const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h + 8 * cb);
       asm volatile(
@@ -737,14 +773,15 @@ __device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *s
     for (int c = 0; c < 8; ++c) {
       const long long z0 = int32_t(z[0][c]), z1 = int32_t(z[1][c]), z2 = int32_t(z[2][c]);
       const long long z3 = int32_t(z[3][c]), z4 = int32_t(z[4][c]), z5 = int32_t(z[5][c]);
+      const long long z6 = int32_t(z[6][c]);
       const long long hi = (z0 * 128 + z1) * 128 + z2;
       double val;
       if (!up) {
-        const long long lo = ((z3 * 128 + z4) * 128 + z5) * 128 + int32_t(z[6][c]);
-        val = __fma_rn(double(hi), 0x1p-28, double(lo) * 0x1p-56);  // levels 2..4, 5..8
+        const long long lo = (((z3 * 128 + z4) * 128 + z5) * 128 + z6) * 128 + int32_t(z[7][c]);
+        val = __fma_rn(double(hi), 0x1p-28, double(lo) * 0x1p-63);  // levels 2..4, 5..9
       } else {
-        const long long lo = (z3 * 128 + z4) * 128 + z5;
-        val = __fma_rn(double(hi), 0x1p-35, double(lo) * 0x1p-56);  // levels 3..5, 6..8
+        const long long lo = ((z3 * 128 + z4) * 128 + z5) * 128 + z6;
+        val = __fma_rn(double(hi), 0x1p-35, double(lo) * 0x1p-63);  // levels 3..5, 6..9
       }
       const int col = 32 * h + 8 * cb + c;
       if (!up) {
@@ -758,6 +795,57 @@ __device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *s
 }
 
 __device__ __forceinline__ void ws_sync() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
+
+// Row points of a tile: thread e < TB loads the membership index of row e
+// early (ws_point_index) and copies the point into prow[e] later
+// (ws_point_copy, cp.async; zeros past n), so that the next item's points
+// arrive while the current item's epilogue runs.
+__device__ __forceinline__ int ws_point_index(const BigArgs &a, const BigSlot &sl, int64_t s0,
+                                              int ti, int e) {
+  const int gi = ti * TB + e;
+  return gi < sl.n ? a.sidx[s0 + gi] : -1;
+}
+__device__ __forceinline__ void ws_point_copy(const BigArgs &a, double4 *prow, int e, int idx) {
+  if (idx >= 0) {
+    const double *g = reinterpret_cast<const double *>(a.src + idx);
+    double *d = reinterpret_cast<double *>(prow + e);
+    cp_async16(d, g);
+    cp_async16(d + 2, g + 2);
+  } else {
+    prow[e] = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+}
+// A[ti, tj] of the slot (gen_tile) into sT, by the 256 epilogue threads, from
+// the row points in prow (staged and waited for by the caller) and the
+// column points in cpts (3 x TB, reloaded when load_cols).
+__device__ __forceinline__ void ws_gen_tile(const BigArgs &a, const BigSlot &sl, int64_t s0,
+                                            int ti, int tj, double *sT, const double4 *prow,
+                                            double *cpts, int t, bool load_cols) {
+  double *cx = cpts, *cy = cx + TB, *cz = cy + TB;
+  if (load_cols)
+    for (int e = t; e < TB; e += 256) {
+      const int gj = tj * TB + e;
+      double4 p = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (gj < sl.n) p = a.src[a.sidx[s0 + gj]];
+      cx[e] = p.x;
+      cy[e] = p.y;
+      cz[e] = p.z;
+    }
+  ws_sync();
+  for (int e = t; e < TB * TB; e += 256) {
+    const int r = e >> 6, c = e & 63;
+    const int gi = ti * TB + r, gj = tj * TB + c;
+    double v;
+    if (gi < sl.n && gj < sl.n) {
+      const double4 pr = prow[r];
+      v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(pr.x, pr.y, pr.z, cx[c], cy[c], cz[c])),
+                           a.rinv);
+    } else {
+      v = (gi == gj) ? 1.0 : 0.0;
+    }
+    sT[r * LDS + c] = v;
+  }
+}
 
 // oz_diag_arrive for the 256 epilogue threads (etid 0 arrives).
 __device__ __forceinline__ bool ws_diag_arrive(int *count, volatile int *flag, int etid) {
@@ -806,6 +894,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
+  // The zero eighth slice of each staged row-tile chunk, made visible to the
+  // tensor core (async proxy); the copies never write it.
+  for (int u = tid; u < kWsStages * 2 * 64; u += kWsThreads) {
+    const int st = u >> 7, ch = (u >> 6) & 1, w16 = u & 63;
+    *reinterpret_cast<uint4 *>(smb + st * kWsStage + ch * kWsChunkA + kWsChunk + 16 * w16) =
+        make_uint4(0u, 0u, 0u, 0u);
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -815,9 +911,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     if (lane == 0) {
       // Producer.
       int hc = 0;
+      WsCursor cur;
       for (int it = it0; it < it1 && !*abort_flag; ++it) {
-        const WsItem w = ws_item(ipre, cnt, it);
-        const BigSlot sl = slots[w.q];
+        const WsItem w = cur.at(ipre, slots, nullptr, cnt, it);
+        const BigSlot &sl = cur.sl;
         const uint8_t *ra = slice_row(sl, w.r == 0 ? j + 1 : j + w.r);
         const uint8_t *rb = slice_row(sl, w.r == 0 ? j + 1 : j);
         for (int hh = 0; hh < nh; ++hh, ++hc) {
@@ -829,9 +926,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           }
           uint8_t *sA = smb + st * kWsStage;
           const int64_t off = int64_t(hh >> 1) * kOzTileBytes + (hh & 1) * kWsHalf;
-          mbar_expect_tx(&bar->full[st], uint32_t(kWsStage));
-          bulk_g2s(sA, ra + off, kWsHalf, &bar->full[st]);
-          bulk_g2s(sA + kWsHalf, rb + off, kWsHalf, &bar->full[st]);
+          mbar_expect_tx(&bar->full[st], uint32_t(2 * kWsHalf));
+          bulk_g2s(sA, ra + off, kWsChunk, &bar->full[st]);
+          bulk_g2s(sA + kWsChunkA, ra + off + kWsChunk, kWsChunk, &bar->full[st]);
+          bulk_g2s(sA + kWsHalfA, rb + off, kWsHalf, &bar->full[st]);
         }
       }
       // Drain: only the latest use of each stage can still be in flight.
@@ -863,7 +961,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           }
           tc_fence_after();
           const uint32_t sA = saddr(smb + st * kWsStage);
-          ws_mma_half(tmem, sA, sA + kWsHalf, hh == 0);
+          ws_mma_half(tmem, sA, sA + kWsHalfA, hh == 0);
           umma_commit(&bar->empty[st]);
         }
         if (!ok) break;
@@ -880,35 +978,59 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     double *sC = reinterpret_cast<double *>(smb + kWsCOff);
     double *sX = reinterpret_cast<double *>(smb + kWsXOff);
     double *sL = reinterpret_cast<double *>(smb + kWsLOff);
-    double *pts = reinterpret_cast<double *>(smb + kWsPtsOff);
+    double4 *prows = reinterpret_cast<double4 *>(smb + kWsPtsOff);              // 2 x TB
+    double *cpts = reinterpret_cast<double *>(smb + kWsPtsOff + 2 * TB * 32);  // 3 x TB
     double *ysh = reinterpret_cast<double *>(smb + kWsRedOff);  // TB x kMaxF
     double *dinv = ysh + TB * kMaxF;                             // 1 / diag(U_j)
+    double *rsh = ysh + TB * kMaxF + 3 * TB;                     // r_i, TB x kMaxF
     volatile int *arrive_flag = &bar->arrive_flag;
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
     ws_sync();
     int xq = -1;  // slot whose U_j (factor of the diagonal tile, transposed) is in sX
-    int pq = -1, ptj = -1;  // slot and column tile whose points are in pts
+    int pq = -1, ptj = -1;  // slot and column tile whose points are in cpts
     int k = 0;
+    WsCursor cur, nxt;  // the item, and the next one (its row points are prefetched)
+    int nidx = -1;      // membership index of this thread's row point of the next item
+    if (it0 < it1) {
+      const WsItem w0 = nxt.at(ipre, slots, a.soff, cnt, it0);
+      if (etid < TB)
+        ws_point_copy(a, prows, etid,
+                      ws_point_index(a, nxt.sl, nxt.s0, w0.r == 0 ? j + 1 : j + w0.r, etid));
+    }
+    cp_async_commit();
     for (int it = it0; it < it1; ++it, ++k) {
-      const WsItem w = ws_item(ipre, cnt, it);
-      const BigSlot sl = slots[w.q];
+      const WsItem w = cur.at(ipre, slots, a.soff, cnt, it);
+      const BigSlot sl = cur.sl;
       const int ld = sl.ld, F = a.F;
       double *W = a.W + sl.base;
       double *rcol = W + int64_t(sl.T) * TB;
       const bool diag = w.r == 0;
       const int i = diag ? j + 1 : j + w.r;
       bool fresh = false;
-      if (!diag && xq != w.q) {
-        load_factor_async(sX, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, etid, 256);
-        cp_async_commit();
-        xq = w.q;
-        fresh = true;
+      if (!diag) {
+        // U_j and y_j once per slot (the finisher reuses their buffers), the
+        // residual rows r_i of every item: copied while the tile is made.
+        if (xq != w.q) {
+          load_factor_async(sX, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, etid, 256);
+          const double *yg = rcol + int64_t(j) * TB * ld;
+          for (int e = etid; e < TB * F; e += 256)
+            cp_async8(ysh + (e / F) * kMaxF + e % F, yg + int64_t(e / F) * ld + e % F);
+          xq = w.q;
+          fresh = true;
+        }
+        const double *rg = rcol + int64_t(i) * TB * ld;
+        for (int e = etid; e < TB * F; e += 256)
+          cp_async8(rsh + (e / F) * kMaxF + e % F, rg + int64_t(e / F) * ld + e % F);
       }
-      // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run; the
-      // column points stay in pts while the slot and column tile do.
+      cp_async_commit();
+      // A[i, j] (or A[j+1, j+1]) while the MMAs of this item run, once the
+      // row points (the group before the one just committed) have landed;
+      // the column points stay in cpts while the slot and column tile do.
+      cp_async_wait<1>();
       const int tj = diag ? j + 1 : j;
-      gen_tile(a, sl, i, tj, TB, sC, pts, etid, 256, ws_sync, pq != w.q || ptj != tj);
+      ws_gen_tile(a, sl, cur.s0, i, tj, sC, prows + (k & 1) * TB, cpts, etid,
+                  pq != w.q || ptj != tj);
       pq = w.q;
       ptj = tj;
       ws_sync();
@@ -929,45 +1051,50 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive_cnt(&bar->acc_empty, 1);
       ws_sync();
+      // The next item's membership indices, loaded while this one finishes.
+      if (it + 1 < it1 && etid < TB) {
+        const WsItem wn = nxt.at(ipre, slots, a.soff, cnt, it + 1);
+        nidx = ws_point_index(a, nxt.sl, nxt.s0, wn.r == 0 ? j + 1 : j + wn.r, etid);
+      }
       for (int e = etid; e < TB * TB; e += 256) {
         const int r = e >> 6, c = e & 63;
         sC[r * LDS + c] = __fma_rn(-a.oz_sig2, sL[r * LDS + c], sC[r * LDS + c]);
       }
       ws_sync();
       bool finish = false;
+      // The copies of the next item's row points (one commit group per item).
+      auto next_points = [&]() {
+        if (it + 1 < it1) {
+          if (etid < TB) ws_point_copy(a, prows + ((k + 1) & 1) * TB, etid, nidx);
+          cp_async_commit();
+        }
+      };
       if (diag) {
         double *dst = a.dpart + int64_t(sl.q) * TB * TB;
         for (int e = etid; e < TB * TB; e += 256) dst[e] = sC[(e >> 6) * LDS + (e & 63)];
+        next_points();
         finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
       } else {
-        // L[i, j] U_j = C by row substitution (warp ew: rows 8 ew .. + 7),
+        // L[i, j] U_j = C by blocked row solves (warp ew: rows 8 ew .. + 7),
         // stored; forward substitution; int8 slices.
         cp_async_wait<0>();
         ws_sync();
         if (fresh && etid < TB) dinv[etid] = 1.0 / sX[etid * LDS + etid];
-        {
-          const double *yg = rcol + int64_t(j) * TB * ld;
-          for (int e = etid; e < TB * kMaxF; e += 256) {
-            const int r = e / kMaxF, f = e % kMaxF;
-            ysh[e] = f < F ? __ldcg(yg + int64_t(r) * ld + f) : 0.0;
-          }
-        }
         ws_sync();
         const int r0 = 8 * ew;
+        warp_rows_trsm8(sC + r0 * LDS, sX, dinv, lane);
+        next_points();
         double lo[8], hi[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           lo[q] = sC[(r0 + q) * LDS + lane];
           hi[q] = sC[(r0 + q) * LDS + 32 + lane];
         }
-        warp_row_solve<8>(lo, hi, sX, dinv, lane);
         {
           double *Lg = W + int64_t(i) * TB * ld + int64_t(j) * TB;
           double *rg = rcol + int64_t(i) * TB * ld;
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            sC[(r0 + q) * LDS + lane] = lo[q];  // the warp's own rows: L over C
-            sC[(r0 + q) * LDS + 32 + lane] = hi[q];
             Lg[int64_t(r0 + q) * ld + lane] = lo[q];
             Lg[int64_t(r0 + q) * ld + 32 + lane] = hi[q];
           }
@@ -977,7 +1104,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
             for (int q = 0; q < 8; ++q) {
               double sum = __fma_rn(lo[q], yl, hi[q] * yh);
               for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-              if (lane == 0) rg[int64_t(r0 + q) * ld + f] -= sum;
+              if (lane == 0) rg[int64_t(r0 + q) * ld + f] = rsh[(r0 + q) * kMaxF + f] - sum;
             }
           }
         }
@@ -1599,8 +1726,10 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       // Tile products: (T - j - 1) row tiles x (j + 1) (update + solve), and
       // j + 1 for the next diagonal tile.
       tl.kind = i8 ? 1 : 0;
-      for (int q = 0; q < c; ++q)
+      for (int q = 0; q < c; ++q) {
         tl.flops += 2.0 * TB * TB * TB * double(hs[q].T - j) * double(j + 1);
+        if (i8) tl.mma_products += double(hs[q].T - j) * double(j);
+      }
       rep.timed.push_back(tl);
     }
   }
@@ -1620,6 +1749,7 @@ void finish_kernel_timing(SolveReport &rep, cudaEvent_t ref) {
     iv[t.kind].push_back({a0, a1});
     iv[2].push_back({a0, a1});
     rep.flops_kind[t.kind] += t.flops;
+    rep.mma_products_i8 += t.mma_products;
     rep.launches_kind[t.kind] += 1;
     rep.update_flops += t.flops;
     rep.update_launches += 1;

@@ -259,17 +259,19 @@ struct SolveReport {
   cudaEvent_t tail_event = nullptr;
   double ms_update = 0.0, update_flops = 0.0;
   int64_t update_launches = 0;
-  // Per kind (0: FP64 steps k_col_step, 1: int8 steps k_col_step_oz): span
+  // Per kind (0: FP64 steps k_col_step, 1: int8 steps k_col_step_ws): span
   // of device time with at least one launch of the kind running, FLOPs and
   // launch count (time_kernels only).
   double ms_kind[2] = {0.0, 0.0}, flops_kind[2] = {0.0, 0.0};
   int64_t launches_kind[2] = {0, 0};
+  double mma_products_i8 = 0.0;
   // Events around each timed step launch, on the launching stream; resolved
   // by finish_kernel_timing once the solve has completed.
   struct TimedLaunch {
     cudaEvent_t e0, e1;
     int kind;
     double flops;
+    double mma_products;  // int8 tile products (kind 1)
   };
   std::vector<TimedLaunch> timed;
   int64_t factors_reused = 0;  // patches solved from kept factorisations

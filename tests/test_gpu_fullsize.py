@@ -119,16 +119,16 @@ def _compare_locals(name, gpu_local, ref_local, toff, sample, n, tol, lapack):
             continue
         rows = np.concatenate([np.arange(toff[k], toff[k + 1]) for k in ks])
         err = rel_l2(gpu_local[rows], ref_local[rows])
-        lk = [k for k in ks if int(k) in lapack]
-        lap = 0.0
-        if lk:
-            lrows = np.concatenate([np.arange(toff[k], toff[k + 1]) for k in lk])
-            for v in range(2):
-                sel = [k for k in lk if len(lapack[int(k)]) > v]
-                if len(sel) < len(lk):
-                    continue
-                lap = max(lap, rel_l2(np.concatenate([lapack[int(k)][v] for k in sel]),
-                                      ref_local[lrows]))
+        # Per patch, the larger disagreement of the independent solvers with
+        # the oracle; the stratum's band is their root-sum-square.
+        num = den = 0.0
+        for k in ks:
+            if int(k) not in lapack:
+                continue
+            r = np.arange(toff[k], toff[k + 1])
+            num += max(float(np.sum((v - ref_local[r]) ** 2)) for v in lapack[int(k)])
+            den += float(np.sum(ref_local[r] ** 2))
+        lap = float(np.sqrt(num / den)) if den > 0 else 0.0
         for k in ks:
             r = np.arange(toff[k], toff[k + 1])
             e = rel_l2(gpu_local[r], ref_local[r])
