@@ -292,10 +292,10 @@ PACMAN_B200_API int pacman_b200_plan_owned_targets(const pacman_b200_plan *plan,
  * 16 KiB file-scope __device__ array, present on every GPU that loads this
  * library until the process exits.  Every call resolves that array's address
  * (cudaGetSymbolAddress) in the context current on the calling thread, so a
- * cudaDeviceReset or a context the caller made current is followed; the
- * first call on a device also loads this library's kernels there, so make the
- * first call before any stream capture.  Calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller.
+ * cudaDeviceReset or a context the caller made current is followed.  The
+ * call synchronises the stream to read the radius back, so it cannot be
+ * captured into a CUDA graph.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.
  * source_points: device memory of the current device, row-major [n x dim];
  * limits: dim <= 3 (the array holds at most 7 samples), 1 <= n <= 2^31 - 1.
  * stream: cudaStream_t (NULL = default stream); the call returns after

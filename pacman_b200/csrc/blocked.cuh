@@ -215,6 +215,67 @@ __device__ __forceinline__ void warp_rows_trsm8(double *rows, const double *sU,
   __syncwarp();
 }
 
+// warp_rows_trsm8 with each 16-column block solved by a product with the
+// inverse of U's 16 x 16 diagonal block instead of by substitution, all
+// products on the FP64 tensor cores (mma.sync m8n8k4: the warp's 8 rows are
+// the instruction's M): X_b = R_b Ui_b, then R_c -= X_b U_bc for the blocks
+// c right of b.  Ui_b = U_bb^-1 is stored as sUi[b][k][c] = U_bb^-1[k][c]
+// (the diagonal blocks of X_j = L_jj^-1 read as X_j[16 b + c][16 b + k]).
+// The blocks of U_jj are at most as ill-conditioned as U_jj (cond(U_bb) <=
+// cond(U_jj)), and the blocked solve stays backward stable blockwise.  No
+// shuffles (a 64-bit shuffle costs two of the SM's one-per-clock shuffle
+// slots): operands come from shared memory.  The right-hand side is C = rows
+// - sig2 up (one rounding), formed first.
+__device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *sU,
+                                                   const double *sUi, int lane,
+                                                   const double *up, double sig2) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int e = lane; e < 8 * TB; e += 32) {
+    const int o = (e >> 6) * LDS + (e & 63);
+    rows[o] = __fma_rn(-sig2, up[o], rows[o]);
+  }
+  __syncwarp();
+#pragma unroll 1
+  for (int b = 0; b < 4; ++b) {
+    const int cb = 16 * b;
+    // X_b = R_b Ui_b, two 8-column halves.
+    double x[2][2];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+      for (int k0 = 0; k0 < 16; k0 += 4) {
+        const double av = rows[g * LDS + cb + k0 + t];
+        const double bv = sUi[b * 256 + (k0 + t) * 16 + 8 * nt + g];
+        dmma(c0, c1, av, bv);
+      }
+      x[nt][0] = c0;
+      x[nt][1] = c1;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      rows[g * LDS + cb + 8 * nt + 2 * t] = x[nt][0];
+      rows[g * LDS + cb + 8 * nt + 2 * t + 1] = x[nt][1];
+    }
+    __syncwarp();
+    // Columns to the right: R[:, n] -= X_b U[b, n], 8-column tiles.
+    for (int nt = 2 * b + 2; nt < 8; ++nt) {
+      double c0 = rows[g * LDS + 8 * nt + 2 * t], c1 = rows[g * LDS + 8 * nt + 2 * t + 1];
+#pragma unroll
+      for (int k0 = 0; k0 < 16; k0 += 4) {
+        const double av = -rows[g * LDS + cb + k0 + t];
+        const double bv = sU[(cb + k0 + t) * LDS + 8 * nt + g];
+        dmma(c0, c1, av, bv);
+      }
+      rows[g * LDS + 8 * nt + 2 * t] = c0;
+      rows[g * LDS + 8 * nt + 2 * t + 1] = c1;
+    }
+    __syncwarp();
+  }
+}
+
 // warp_rows_trsm8 with the off-diagonal block products on the FP64 tensor
 // cores (mma.sync m8n8k4) through shared memory, for the FP64 step kernel,
 // which runs no int8 MMAs and has fewer registers to spare.

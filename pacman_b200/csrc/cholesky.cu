@@ -106,6 +106,46 @@ __device__ __forceinline__ void gen_tile(const BigArgs &a, const BigSlot &sl, in
 
 __device__ __forceinline__ void sync_all() { __syncthreads(); }
 
+// Cholesky of the 16 x 16 block D[kb.., kb..] (lower part, row stride ld,
+// overwritten by L) by one warp in registers: lane i + 16 h holds columns
+// 8 h .. 8 h + 7 of row kb + i; column c's entries reach the other lanes by
+// shuffles.  The same operations as a column-by-column right-looking
+// Cholesky of the block: L_cc = sqrt(d_cc), L_ic = d_ic (1 / L_cc), d_ij -=
+// L_ic L_jc; dis[kb + c] = 1 / L_cc.  Returns true on a pivot that is not
+// > 0.
+__device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis, int lane) {
+  const int i = lane & 15, h = lane >> 4;
+  bool bad = false;
+  double a[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) a[t] = 8 * h + t <= i ? D[(kb + i) * ld + kb + 8 * h + t] : 0.0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int hc = c >> 3, tc = c & 7;
+    const double piv = __shfl_sync(0xffffffffu, a[tc], c + 16 * hc);
+    bad |= !(piv > 0.0);
+    const double sq = sqrt(piv), rs = __drcp_rn(sq);
+    if (h == hc) {
+      if (i == c) a[tc] = sq;
+      else if (i > c) a[tc] *= rs;
+    }
+    if (lane == 0) dis[kb + c] = rs;
+    const double oth = __shfl_xor_sync(0xffffffffu, a[tc], 16);
+    const double lic = h == hc ? a[tc] : oth;  // L[i][c]
+#pragma unroll
+    for (int jj = 0; jj < 16; ++jj) {
+      if (jj <= c) continue;
+      const double ljc = __shfl_sync(0xffffffffu, a[tc], jj + 16 * hc);  // L[jj][c]
+      if (h == (jj >> 3) && i >= jj) a[jj & 7] = __fma_rn(-lic, ljc, a[jj & 7]);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (8 * h + t <= i) D[(kb + i) * ld + kb + 8 * h + t] = a[t];
+  __syncwarp();
+  return bad;
+}
+
 // The diagonal tile of a step, 256 threads (8 warps): the Cholesky factor
 // L_c of the 64 x 64 tile D (lower part, in shared memory at g with row stride
 // ld, overwritten), X = L_c^{-1} (to gi, row stride TB), y = X r for the first
@@ -134,29 +174,8 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
   }
   for (int kb = 0; kb < TB; kb += 16) {
-    // (a) the diagonal block, warp 0.
-    if (warp == 0) {
-      for (int c = 0; c < 16; ++c) {
-        const int p = kb + c;
-        const double piv = D[p * ld + p];
-        bad |= !(piv > 0.0);
-        const double sq = sqrt(piv), rs = __drcp_rn(sq);
-        if (col16 > c && half == 0) D[(kb + col16) * ld + p] *= rs;
-        if (lane == 0) {
-          D[p * ld + p] = sq;
-          dis[p] = rs;
-        }
-        __syncwarp();
-        // Trailing part of the block: lane i (row kb + i) updates its row.
-        if (half == 0 && col16 > c) {
-          const int i = kb + col16;
-          const double lip = D[i * ld + p];
-          for (int jj = c + 1; jj <= col16; ++jj)
-            D[i * ld + kb + jj] = __fma_rn(-lip, D[(kb + jj) * ld + p], D[i * ld + kb + jj]);
-        }
-        __syncwarp();
-      }
-    }
+    // (a) the diagonal block, warp 0 (warp_chol16).
+    if (warp == 0) bad |= warp_chol16(D, ld, kb, dis, lane);
     sync();
     // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d.
     const int r0 = kb + 16 + 8 * warp;
@@ -673,7 +692,8 @@ constexpr int kWsXOff = kWsCOff + TB * LDS * 8;          // X_j, or diag_tile sc
 constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // L[j+1, j] (finisher)
 constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // row points (2 x TB), column points
 constexpr int kWsRedOff = kWsPtsOff + 2 * TB * 32 + 3 * TB * 8;  // y_j, r_i, diag_tile vectors
-constexpr int kWsBarOff = kWsRedOff + 3 * TB * kMaxF * 8;
+constexpr int kWsUiOff = kWsRedOff + 3 * TB * kMaxF * 8;  // U_j's diagonal block inverses
+constexpr int kWsBarOff = kWsUiOff + 4 * 16 * 16 * 8;
 constexpr size_t kWsSmem = size_t(kWsBarOff) + 256;
 static_assert(kWsSmem <= 232448, "shared memory of k_col_step_ws");
 static_assert(kWsStage % 1024 == 0, "stages start on 1 KB boundaries");
@@ -832,14 +852,18 @@ __device__ __forceinline__ void ws_gen_tile(const BigArgs &a, const BigSlot &sl,
       cz[e] = p.z;
     }
   ws_sync();
-  for (int e = t; e < TB * TB; e += 256) {
-    const int r = e >> 6, c = e & 63;
-    const int gi = ti * TB + r, gj = tj * TB + c;
+  // Thread t: column c = t % 64 of rows t / 64 + 4 m, m = 0..15 (unrolled by
+  // four for independent evaluations in flight).
+  const int c = t & 63, gj = tj * TB + c;
+  const double px = cx[c], py = cy[c], pz = cz[c];
+#pragma unroll 4
+  for (int m = 0; m < TB * TB / 256; ++m) {
+    const int r = (t >> 6) + 4 * m;
+    const int gi = ti * TB + r;
     double v;
     if (gi < sl.n && gj < sl.n) {
       const double4 pr = prow[r];
-      v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(pr.x, pr.y, pr.z, cx[c], cy[c], cz[c])),
-                           a.rinv);
+      v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(pr.x, pr.y, pr.z, px, py, pz)), a.rinv);
     } else {
       v = (gi == gj) ? 1.0 : 0.0;
     }
@@ -981,8 +1005,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     double4 *prows = reinterpret_cast<double4 *>(smb + kWsPtsOff);              // 2 x TB
     double *cpts = reinterpret_cast<double *>(smb + kWsPtsOff + 2 * TB * 32);  // 3 x TB
     double *ysh = reinterpret_cast<double *>(smb + kWsRedOff);  // TB x kMaxF
-    double *dinv = ysh + TB * kMaxF;                             // 1 / diag(U_j)
     double *rsh = ysh + TB * kMaxF + 3 * TB;                     // r_i, TB x kMaxF
+    double *sUi = reinterpret_cast<double *>(smb + kWsUiOff);   // [b][k][c] = U_bb^-1[k][c]
     volatile int *arrive_flag = &bar->arrive_flag;
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
@@ -1007,17 +1031,21 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       double *rcol = W + int64_t(sl.T) * TB;
       const bool diag = w.r == 0;
       const int i = diag ? j + 1 : j + w.r;
-      bool fresh = false;
       if (!diag) {
         // U_j and y_j once per slot (the finisher reuses their buffers), the
         // residual rows r_i of every item: copied while the tile is made.
         if (xq != w.q) {
           load_factor_async(sX, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, etid, 256);
+          // U_bb^-1 = (X_j's diagonal block b)^T, X_j = L_jj^-1 row-major.
+          const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
+          for (int e = etid; e < 4 * 256; e += 256) {
+            const int b = e >> 8, k = (e >> 4) & 15, c = e & 15;
+            cp_async8(sUi + e, xg + (16 * b + c) * TB + 16 * b + k);
+          }
           const double *yg = rcol + int64_t(j) * TB * ld;
           for (int e = etid; e < TB * F; e += 256)
             cp_async8(ysh + (e / F) * kMaxF + e % F, yg + int64_t(e / F) * ld + e % F);
           xq = w.q;
-          fresh = true;
         }
         const double *rg = rcol + int64_t(i) * TB * ld;
         for (int e = etid; e < TB * F; e += 256)
@@ -1044,8 +1072,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         break;
       }
       tc_fence_after();
-      // C = A - sigma^2 (lower-lane levels + upper-lane levels); the upper
-      // lanes' sums go through sL (free until the finisher).
+      // C = A - sigma^2 (lower-lane levels + upper-lane levels): sC gets A
+      // minus the lower lanes' sums, sL (free until the finisher) the upper
+      // lanes' sums.
       ws_drain(tmem, qd, h, sC, sL, a.oz_sig2, lane);
       tc_fence_before();
       __syncwarp();
@@ -1056,11 +1085,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         const WsItem wn = nxt.at(ipre, slots, a.soff, cnt, it + 1);
         nidx = ws_point_index(a, nxt.sl, nxt.s0, wn.r == 0 ? j + 1 : j + wn.r, etid);
       }
-      for (int e = etid; e < TB * TB; e += 256) {
-        const int r = e >> 6, c = e & 63;
-        sC[r * LDS + c] = __fma_rn(-a.oz_sig2, sL[r * LDS + c], sC[r * LDS + c]);
-      }
-      ws_sync();
+      // C = sC - sigma^2 sL is formed where it is read: by the diagonal
+      // item's copy, or by the triangular solve's loads.
       bool finish = false;
       // The copies of the next item's row points (one commit group per item).
       auto next_points = [&]() {
@@ -1070,8 +1096,15 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         }
       };
       if (diag) {
+        // D' into sC (this CTA may finish the tile) and to dpart (for the
+        // other producer, if it arrives last).
         double *dst = a.dpart + int64_t(sl.q) * TB * TB;
-        for (int e = etid; e < TB * TB; e += 256) dst[e] = sC[(e >> 6) * LDS + (e & 63)];
+        for (int e = etid; e < TB * TB; e += 256) {
+          const int o = (e >> 6) * LDS + (e & 63);
+          const double d = __fma_rn(-a.oz_sig2, sL[o], sC[o]);
+          sC[o] = d;
+          dst[e] = d;
+        }
         next_points();
         finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
       } else {
@@ -1079,10 +1112,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         // stored; forward substitution; int8 slices.
         cp_async_wait<0>();
         ws_sync();
-        if (fresh && etid < TB) dinv[etid] = 1.0 / sX[etid * LDS + etid];
         ws_sync();
         const int r0 = 8 * ew;
-        warp_rows_trsm8(sC + r0 * LDS, sX, dinv, lane);
+        warp_rows_trsm8_bi(sC + r0 * LDS, sX, sUi, lane, sL + r0 * LDS, a.oz_sig2);
         next_points();
         double lo[8], hi[8];
 #pragma unroll
