@@ -882,8 +882,8 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
       // Interleaved groups of slots, each stepping in lockstep on its own
       // stream: the short diagonal and trsm launches and the tails of one
       // group's column updates overlap the other groups' work.
-      // The tuned group count (PACMAN_B200_GROUPS, 1..4, overrides it).
-      int G = std::min<int>(AuxStreams::kN, std::max(1, ns / 8));
+      // The tuned group count (PACMAN_B200_GROUPS, 1..8, overrides it).
+      int G = std::min<int>(AuxStreams::kDefaultGroups, std::max(1, ns / 8));
       const int gt = tuned_int("PACMAN_B200_GROUPS", tuning_for_current_device().groups);
       if (gt > 0) G = std::min<int>(AuxStreams::kN, std::min(gt, ns));
       std::vector<std::vector<BigSlot>> gs(G);

@@ -14,6 +14,7 @@ namespace pacman_b200 {
 
 constexpr int TB = 64;   // tile size
 constexpr int LDS = 68;  // shared-memory row stride (doubles): conflict-free fragments
+constexpr int kUiLd = 20;  // row stride (doubles) of the 16 x 16 block inverses in shared memory
 
 struct BigSlot {
   int64_t base;  // offset (doubles) of the augmented matrix in the workspace
@@ -219,23 +220,27 @@ __device__ __forceinline__ void warp_rows_trsm8(double *rows, const double *sU,
 // inverse of U's 16 x 16 diagonal block instead of by substitution, all
 // products on the FP64 tensor cores (mma.sync m8n8k4: the warp's 8 rows are
 // the instruction's M): X_b = R_b Ui_b, then R_c -= X_b U_bc for the blocks
-// c right of b.  Ui_b = U_bb^-1 is stored as sUi[b][k][c] = U_bb^-1[k][c]
-// (the diagonal blocks of X_j = L_jj^-1 read as X_j[16 b + c][16 b + k]).
+// c right of b.  Ui_b = U_bb^-1 is stored as sUi[(16 b + k) kUiLd + c] =
+// U_bb^-1[k][c] (the diagonal blocks of X_j = L_jj^-1 read as X_j[16 b +
+// c][16 b + k]); the padded row stride kUiLd spreads the fragment loads of
+// four rows over the shared-memory banks.
 // The blocks of U_jj are at most as ill-conditioned as U_jj (cond(U_bb) <=
 // cond(U_jj)), and the blocked solve stays backward stable blockwise.  No
 // shuffles (a 64-bit shuffle costs two of the SM's one-per-clock shuffle
-// slots): operands come from shared memory.  The right-hand side is C = rows
-// - sig2 up (one rounding), formed first.
+// slots): operands come from shared memory.  With up, the right-hand side is C =
+// rows - sig2 up (one rounding), formed first.
 __device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *sU,
                                                    const double *sUi, int lane,
                                                    const double *up, double sig2) {
   const int g = lane >> 2, t = lane & 3;
+  if (up) {
 #pragma unroll
-  for (int e = lane; e < 8 * TB; e += 32) {
-    const int o = (e >> 6) * LDS + (e & 63);
-    rows[o] = __fma_rn(-sig2, up[o], rows[o]);
+    for (int e = lane; e < 8 * TB; e += 32) {
+      const int o = (e >> 6) * LDS + (e & 63);
+      rows[o] = __fma_rn(-sig2, up[o], rows[o]);
+    }
+    __syncwarp();
   }
-  __syncwarp();
 #pragma unroll 1
   for (int b = 0; b < 4; ++b) {
     const int cb = 16 * b;
@@ -247,7 +252,7 @@ __device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *s
 #pragma unroll
       for (int k0 = 0; k0 < 16; k0 += 4) {
         const double av = rows[g * LDS + cb + k0 + t];
-        const double bv = sUi[b * 256 + (k0 + t) * 16 + 8 * nt + g];
+        const double bv = sUi[(cb + k0 + t) * kUiLd + 8 * nt + g];
         dmma(c0, c1, av, bv);
       }
       x[nt][0] = c0;

@@ -109,8 +109,9 @@ __device__ __forceinline__ void sync_all() { __syncthreads(); }
 // Cholesky of the 16 x 16 block D[kb.., kb..] (lower part, row stride ld,
 // overwritten by L) by one warp in registers: lane i + 16 h holds columns
 // 8 h .. 8 h + 7 of row kb + i; column c's entries reach the other lanes by
-// shuffles.  The same operations as a column-by-column right-looking
-// Cholesky of the block: L_cc = sqrt(d_cc), L_ic = d_ic (1 / L_cc), d_ij -=
+// shuffles.  A column-by-column right-looking Cholesky of the block: 1 / L_cc
+// = rsqrt(d_cc) (one operation on the chain of pivots instead of a square
+// root and a reciprocal), L_cc = d_cc / L_cc, L_ic = d_ic (1 / L_cc), d_ij -=
 // L_ic L_jc; dis[kb + c] = 1 / L_cc.  Returns true on a pivot that is not
 // > 0.
 __device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis, int lane) {
@@ -124,7 +125,7 @@ __device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis,
     const int hc = c >> 3, tc = c & 7;
     const double piv = __shfl_sync(0xffffffffu, a[tc], c + 16 * hc);
     bad |= !(piv > 0.0);
-    const double sq = sqrt(piv), rs = __drcp_rn(sq);
+    const double rs = rsqrt(piv), sq = piv * rs;
     if (h == hc) {
       if (i == c) a[tc] = sq;
       else if (i > c) a[tc] *= rs;
@@ -146,6 +147,27 @@ __device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis,
   return bad;
 }
 
+// T = L_bb^-1 of the 16 x 16 lower-triangular block at D[kb..][kb..] (row
+// stride ld) by one warp, lane j < 16 computing column j of T down the column
+// (T_jj = 1 / L_jj from dis, T_ij = -(sum_{j<=k<i} L_ik T_kj) / L_ii), stored
+// transposed: ui[j kUiLd + i] = T_ij, i.e. ui holds (L_bb^T)^-1 = U_bb^-1.
+__device__ __forceinline__ void warp_trinv16(const double *D, int ld, int kb, const double *dis,
+                                             double *ui, int lane) {
+  if (lane < 16) {
+    const int j = lane;
+    double *uj = ui + j * kUiLd;
+    for (int i = 0; i < j; ++i) uj[i] = 0.0;
+    uj[j] = dis[kb + j];
+    for (int i = j + 1; i < 16; ++i) {
+      const double *li = D + (kb + i) * ld + kb;
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s = __fma_rn(li[k], uj[k], s);
+      uj[i] = -s * dis[kb + i];
+    }
+  }
+  __syncwarp();
+}
+
 // The diagonal tile of a step, 256 threads (8 warps): the Cholesky factor
 // L_c of the 64 x 64 tile D (lower part, in shared memory at g with row stride
 // ld, overwritten), X = L_c^{-1} (to gi, row stride TB), y = X r for the first
@@ -162,7 +184,8 @@ __device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis,
 template <class Sync, bool kTensorSolve = false>
 __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int F, double *gi,
                             double *Us, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
-                            int tid, Sync sync, double *gu = nullptr, int uld = 0) {
+                            int tid, Sync sync, double *gu = nullptr, int uld = 0,
+                            double *ui = nullptr) {
   (void)cv;
   double *D = const_cast<double *>(g_in);
   const int lane = tid & 31, warp = tid >> 5;
@@ -226,11 +249,16 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     Us[p * LDS + i] = u;
     if (gu) gu[int64_t(p) * uld + i] = u;
   }
+  // With ui (and ld == LDS): the inverses of U's four 16 x 16 diagonal blocks,
+  // one warp each, for the block-inverse row solves below.
+  const bool blockinv = !kTensorSolve && ui != nullptr;
+  if (blockinv && warp < 4) warp_trinv16(D, ld, 16 * warp, dis, ui + 16 * warp * kUiLd, lane);
   sync();
   // X^T from X^T U = I: rows of the identity solved in place of D.
   for (int e = tid; e < TB * TB; e += 256) D[(e >> 6) * ld + (e & 63)] = (e >> 6) == (e & 63);
   sync();
   if (kTensorSolve) warp_rows_trsm8_tc(D + 8 * warp * ld, Us, dis, lane);
+  else if (blockinv) warp_rows_trsm8_bi(D + 8 * warp * ld, Us, ui, lane, nullptr, 0.0);
   else warp_rows_trsm8(D + 8 * warp * ld, Us, dis, lane);
   sync();
   // X (row-major, gi) and y = X r.
@@ -693,7 +721,7 @@ constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // L[j+1, j] (finisher)
 constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // row points (2 x TB), column points
 constexpr int kWsRedOff = kWsPtsOff + 2 * TB * 32 + 3 * TB * 8;  // y_j, r_i, diag_tile vectors
 constexpr int kWsUiOff = kWsRedOff + 3 * TB * kMaxF * 8;  // U_j's diagonal block inverses
-constexpr int kWsBarOff = kWsUiOff + 4 * 16 * 16 * 8;
+constexpr int kWsBarOff = kWsUiOff + 4 * 16 * kUiLd * 8;
 constexpr size_t kWsSmem = size_t(kWsBarOff) + 256;
 static_assert(kWsSmem <= 232448, "shared memory of k_col_step_ws");
 static_assert(kWsStage % 1024 == 0, "stages start on 1 KB boundaries");
@@ -1007,6 +1035,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     double *ysh = reinterpret_cast<double *>(smb + kWsRedOff);  // TB x kMaxF
     double *rsh = ysh + TB * kMaxF + 3 * TB;                     // r_i, TB x kMaxF
     double *sUi = reinterpret_cast<double *>(smb + kWsUiOff);   // [b][k][c] = U_bb^-1[k][c]
+                                                                 // (row stride kUiLd)
     volatile int *arrive_flag = &bar->arrive_flag;
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
@@ -1040,7 +1069,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           const double *xg = a.inv + sl.inv + int64_t(j) * TB * TB;
           for (int e = etid; e < 4 * 256; e += 256) {
             const int b = e >> 8, k = (e >> 4) & 15, c = e & 15;
-            cp_async8(sUi + e, xg + (16 * b + c) * TB + 16 * b + k);
+            cp_async8(sUi + (16 * b + k) * kUiLd + c, xg + (16 * b + c) * TB + 16 * b + k);
           }
           const double *yg = rcol + int64_t(j) * TB * ld;
           for (int e = etid; e < TB * F; e += 256)
@@ -1172,7 +1201,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         const bool bad = diag_tile_t(sC, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
                                      a.inv + sl.inv + int64_t(j + 1) * TB * TB, sX, cv, dis, ysd,
                                      etid, ws_sync,
-                                     W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld);
+                                     W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, sL);
         if (etid == 0 && bad) atomicOr(&a.status[sl.k], 4);
         xq = -1;  // sX was the factor's scratch
       }

@@ -371,14 +371,40 @@ struct CandSpec {
 
 enum : unsigned char { kDead = 0, kAlive0 = 1, kSurvive = 2, kPending = 3 };
 
+// Calls fn(point_id) for the points in the 3^3 cells around q that fall to
+// this lane: the warp's 32 lanes split every cell's points between them.
+template <typename Fn>
+__device__ __forceinline__ void for_neighbors_lanes(const GridView &g, double qx, double qy,
+                                                    double qz, int lane, Fn &&fn) {
+  const int cx = cell_coord(qx, g.lo[0], g.inv_h, g.nc[0]);
+  const int cy = cell_coord(qy, g.lo[1], g.inv_h, g.nc[1]);
+  const int cz = cell_coord(qz, g.lo[2], g.inv_h, g.nc[2]);
+  const int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nc[0] - 1);
+  const int y0 = max(cy - 1, 0), y1 = min(cy + 1, g.nc[1] - 1);
+  const int z0 = max(cz - 1, 0), z1 = min(cz + 1, g.nc[2] - 1);
+  for (int a = x0; a <= x1; ++a)
+    for (int b = y0; b <= y1; ++b) {
+      const int base = (a * g.nc[1] + b) * g.nc[2];
+      const int s = g.start[base + z0];
+      const int e = g.start[base + z1 + 1];
+      for (int i = s + lane; i < e; i += 32) fn(g.items[i]);
+    }
+}
+
 // Steps 5-8: candidate coordinates (row-major storage, last axis fastest),
 // source and target emptiness tags (nearest within r, i.e. squared distance
 // <= r*r), snap to the nearest source (lowest id on ties).
+// One warp per candidate centre (dense blobs put thousands of sources in a
+// candidate's 3^3 cells, too many for one thread): the lanes split the
+// neighbourhood, the nearest source is the lexicographic minimum of (squared
+// distance, index) over the warp, so the result does not depend on the split.
 __global__ void k_candidates(CandSpec cs, GridView sg, const double4 *__restrict__ src,
                              GridView tg, const double4 *__restrict__ tgt, int has_targets,
                              double4 *cpos, unsigned char *state) {
-  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < cs.nb;
-       s += (long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long s = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); s < cs.nb;
+       s += nw) {
     long long t = s;
     int coords[3] = {0, 0, 0};
     for (int a = cs.dim - 1; a >= 0; --a) {
@@ -389,7 +415,7 @@ __global__ void k_candidates(CandSpec cs, GridView sg, const double4 *__restrict
     for (int a = 0; a < cs.dim; ++a) q[a] = __fma_rn(cs.dist[a], double(coords[a]), cs.lo[a]);
     double best = INFINITY;
     int bi = 0x7fffffff;
-    for_neighbors(sg, q[0], q[1], q[2], [&](int i) {
+    for_neighbors_lanes(sg, q[0], q[1], q[2], lane, [&](int i) {
       const double4 p = src[i];
       const double d2 = sqdist3(q[0], q[1], q[2], p.x, p.y, p.z);
       if (d2 < best || (d2 == best && i < bi)) {
@@ -397,19 +423,29 @@ __global__ void k_candidates(CandSpec cs, GridView sg, const double4 *__restrict
         bi = i;
       }
     });
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob < best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
     bool alive = (bi != 0x7fffffff) && (best <= cs.r2);
     if (alive && has_targets) {
       bool any = false;
-      for_neighbors(tg, q[0], q[1], q[2], [&](int i) {
+      for_neighbors_lanes(tg, q[0], q[1], q[2], lane, [&](int i) {
         if (!any) {
           const double4 p = tgt[i];
           any = sqdist3(q[0], q[1], q[2], p.x, p.y, p.z) <= cs.r2;
         }
       });
-      alive = any;
+      alive = __any_sync(0xffffffffu, any);
     }
-    state[s] = alive ? kAlive0 : kDead;
-    cpos[s] = alive ? src[bi] : make_double4(q[0], q[1], q[2], 0.0);
+    if (lane == 0) {
+      state[s] = alive ? kAlive0 : kDead;
+      cpos[s] = alive ? src[bi] : make_double4(q[0], q[1], q[2], 0.0);
+    }
   }
 }
 
@@ -863,7 +899,7 @@ void build_geometry(Plan &p, const double *src_dev, const double *tgt_dev) {
   long long off_h[26];
   const int noff = neighbor_offsets(dim, cs.shape, off_h);
   PB_CUDA(cudaMemcpyAsync(offs.p, off_h, sizeof(long long) * noff, cudaMemcpyHostToDevice, st));
-  k_candidates<<<grid_for(nb), kThreads, 0, st>>>(cs, sgrid.view, p.src4.as<double4>(),
+  k_candidates<<<grid_for(nb * 32), kThreads, 0, st>>>(cs, sgrid.view, p.src4.as<double4>(),
                                                   tgrid.view, p.tgt4.as<double4>(), m > 0 ? 1 : 0,
                                                   cpos.as<double4>(), s0.as<unsigned char>());
   note_launch();

@@ -85,7 +85,8 @@ struct DevGrid {
 // Every use joins them back into the plan's stream with events before the
 // call returns.
 struct AuxStreams {
-  static constexpr int kN = 4;      // slot groups of the large-patch engine
+  static constexpr int kN = 8;      // slot groups of the large-patch engine (at most)
+  static constexpr int kDefaultGroups = 4;  // without a tuned or given count
   static constexpr int kSmall = kN; // index of the small-patch stream
   cudaStream_t s[kN + 1] = {};
   cudaEvent_t ev[kN + 3] = {};      // per group, fork, small fork, small join

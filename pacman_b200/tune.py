@@ -29,7 +29,7 @@ import sys
 
 SPACE = {
     "PACMAN_B200_INT8_FROM": ["2", "3", "4", "5", "6"],
-    "PACMAN_B200_GROUPS": ["1", "2", "3", "4"],
+    "PACMAN_B200_GROUPS": ["1", "2", "3", "4", "6", "8"],
     "PACMAN_B200_BIG_N": ["32", "48", "64"],
 }
 DEFAULTS = {"PACMAN_B200_INT8_FROM": "4", "PACMAN_B200_GROUPS": "4",
