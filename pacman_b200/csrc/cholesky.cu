@@ -794,7 +794,7 @@ __device__ __forceinline__ void ws_mma_half(uint32_t tmem, uint32_t sA, uint32_t
 // are merged in int64 first: |level| < 2^31, so the top three shifted by 7
 // bits each stay below 2^53 and convert exactly, and the lower four or five
 // (below 2^60 in units of 128^-9) round to within 2^-57; then two FP64
-// terms (in units of sigma^2).  8 columns at a time, one TMEM wait per 8 columns.  Lanes 0..63
+// terms (in units of sigma^2).  Lanes 0..63
 // subtract sig2 x their sum from sC (which holds A); lanes 64..127 store
 // theirs in sUp, which the caller subtracts after a barrier.
 __device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *sC, double *sUp,
@@ -803,35 +803,40 @@ __device__ __forceinline__ void ws_drain(uint32_t tmem, int qd, int h, double *s
   const uint32_t lane_base = uint32_t(32 * qd) << 16;
   const bool up = qd >= 2;
   const int ng = up ? kG - 1 : kG;  // upper lanes: group 7 holds a partial level 10
-#pragma unroll
-  for (int cb = 0; cb < 4; ++cb) {
-    uint32_t z[kG][8];
+  // Four columns per step: the levels are merged into (hi, lo), the loads of
+  // step cb + 1 are issued, and the conversions and stores of step cb run
+  // while they are in flight.
+  uint32_t z[kG][4];
+  auto issue = [&](int cb) {
 #pragma unroll
     for (int g = 0; g < kG; ++g) {
       if (g >= ng) break;
-      const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h + 8 * cb);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-          : "=r"(z[g][0]), "=r"(z[g][1]), "=r"(z[g][2]), "=r"(z[g][3]), "=r"(z[g][4]),
-            "=r"(z[g][5]), "=r"(z[g][6]), "=r"(z[g][7])
-          : "r"(addr));
+      const uint32_t addr = tmem + lane_base + uint32_t(64 * g + 32 * h + 4 * cb);
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                   : "=r"(z[g][0]), "=r"(z[g][1]), "=r"(z[g][2]), "=r"(z[g][3])
+                   : "r"(addr));
     }
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+  };
+  issue(0);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+  for (int cb = 0; cb < 8; ++cb) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+    long long hi[4], lo[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
       const long long z0 = int32_t(z[0][c]), z1 = int32_t(z[1][c]), z2 = int32_t(z[2][c]);
       const long long z3 = int32_t(z[3][c]), z4 = int32_t(z[4][c]), z5 = int32_t(z[5][c]);
       const long long z6 = int32_t(z[6][c]);
-      const long long hi = (z0 * 128 + z1) * 128 + z2;
-      double val;
-      if (!up) {
-        const long long lo = (((z3 * 128 + z4) * 128 + z5) * 128 + z6) * 128 + int32_t(z[7][c]);
-        val = __fma_rn(double(hi), 0x1p-28, double(lo) * 0x1p-63);  // levels 2..4, 5..9
-      } else {
-        const long long lo = ((z3 * 128 + z4) * 128 + z5) * 128 + z6;
-        val = __fma_rn(double(hi), 0x1p-35, double(lo) * 0x1p-63);  // levels 3..5, 6..9
-      }
-      const int col = 32 * h + 8 * cb + c;
+      hi[c] = (z0 * 128 + z1) * 128 + z2;
+      lo[c] = up ? ((z3 * 128 + z4) * 128 + z5) * 128 + z6
+                 : (((z3 * 128 + z4) * 128 + z5) * 128 + z6) * 128 + int32_t(z[7][c]);
+    }
+    if (cb < 7) issue(cb + 1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      // Lower lanes: levels 2..4 and 5..9; upper lanes: 3..5 and 6..9.
+      const double val = __fma_rn(double(hi[c]), up ? 0x1p-35 : 0x1p-28, double(lo[c]) * 0x1p-63);
+      const int col = 32 * h + 4 * cb + c;
       if (!up) {
         double *cr = sC + (32 * qd + lane) * LDS + col;
         *cr = __fma_rn(-sig2, val, *cr);
@@ -863,6 +868,29 @@ __device__ __forceinline__ void ws_point_copy(const BigArgs &a, double4 *prow, i
     prow[e] = make_double4(0.0, 0.0, 0.0, 0.0);
   }
 }
+// The evaluation loop of ws_gen_tile for one basis, without branches: thread
+// t takes column c = t % 64 of rows t / 64 + 4 m, m = 0..15, and the identity
+// padding past n is selected, so that the unrolled evaluations form one block
+// whose FP64 chains (23-cycle FMA latency on this GPU) overlap.
+template <int B>
+__device__ __forceinline__ void ws_gen_rows(const BigArgs &a, const BigSlot &sl, int ti, int tj,
+                                            double *sT, const double4 *prow, const double *cpts,
+                                            int t) {
+  const double *cx = cpts, *cy = cx + TB, *cz = cy + TB;
+  const int c = t & 63, gj = tj * TB + c;
+  const double px = cx[c], py = cy[c], pz = cz[c];
+#pragma unroll 8
+  for (int m = 0; m < TB * TB / 256; ++m) {
+    const int r = (t >> 6) + 4 * m;
+    const int gi = ti * TB + r;
+    const double4 pr = prow[r];
+    const double w =
+        wendland<double>(B, __dsqrt_rn(sqdist3(pr.x, pr.y, pr.z, px, py, pz)), a.rinv);
+    const double pad = (gi == gj) ? 1.0 : 0.0;
+    sT[r * LDS + c] = (gi < sl.n && gj < sl.n) ? w : pad;
+  }
+}
+
 // A[ti, tj] of the slot (gen_tile) into sT, by the 256 epilogue threads, from
 // the row points in prow (staged and waited for by the caller) and the
 // column points in cpts (3 x TB, reloaded when load_cols).
@@ -880,22 +908,12 @@ __device__ __forceinline__ void ws_gen_tile(const BigArgs &a, const BigSlot &sl,
       cz[e] = p.z;
     }
   ws_sync();
-  // Thread t: column c = t % 64 of rows t / 64 + 4 m, m = 0..15 (unrolled by
-  // four for independent evaluations in flight).
-  const int c = t & 63, gj = tj * TB + c;
-  const double px = cx[c], py = cy[c], pz = cz[c];
-#pragma unroll 4
-  for (int m = 0; m < TB * TB / 256; ++m) {
-    const int r = (t >> 6) + 4 * m;
-    const int gi = ti * TB + r;
-    double v;
-    if (gi < sl.n && gj < sl.n) {
-      const double4 pr = prow[r];
-      v = wendland<double>(a.basis, __dsqrt_rn(sqdist3(pr.x, pr.y, pr.z, px, py, pz)), a.rinv);
-    } else {
-      v = (gi == gj) ? 1.0 : 0.0;
-    }
-    sT[r * LDS + c] = v;
+  switch (a.basis) {
+  case kWendlandC0: ws_gen_rows<kWendlandC0>(a, sl, ti, tj, sT, prow, cpts, t); break;
+  case kWendlandC2: ws_gen_rows<kWendlandC2>(a, sl, ti, tj, sT, prow, cpts, t); break;
+  case kWendlandC4: ws_gen_rows<kWendlandC4>(a, sl, ti, tj, sT, prow, cpts, t); break;
+  case kWendlandC6: ws_gen_rows<kWendlandC6>(a, sl, ti, tj, sT, prow, cpts, t); break;
+  default: ws_gen_rows<kWendlandC8>(a, sl, ti, tj, sT, prow, cpts, t); break;
   }
 }
 
