@@ -241,7 +241,7 @@ __device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *s
     }
     __syncwarp();
   }
-#pragma unroll 1
+#pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int cb = 16 * b;
     // X_b = R_b Ui_b, two 8-column halves.
@@ -265,7 +265,9 @@ __device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *s
       rows[g * LDS + cb + 8 * nt + 2 * t + 1] = x[nt][1];
     }
     __syncwarp();
-    // Columns to the right: R[:, n] -= X_b U[b, n], 8-column tiles.
+    // Columns to the right: R[:, n] -= X_b U[b, n], 8-column tiles (b is a
+    // constant here, so the tiles' product chains are interleaved).
+#pragma unroll
     for (int nt = 2 * b + 2; nt < 8; ++nt) {
       double c0 = rows[g * LDS + 8 * nt + 2 * t], c1 = rows[g * LDS + 8 * nt + 2 * t + 1];
 #pragma unroll

@@ -112,58 +112,69 @@ __device__ __forceinline__ void sync_all() { __syncthreads(); }
 // shuffles.  A column-by-column right-looking Cholesky of the block: 1 / L_cc
 // = rsqrt(d_cc) (one operation on the chain of pivots instead of a square
 // root and a reciprocal), L_cc = d_cc / L_cc, L_ic = d_ic (1 / L_cc), d_ij -=
-// L_ic L_jc; dis[kb + c] = 1 / L_cc.  Returns true on a pivot that is not
-// > 0.
+// L_ic L_jc; dis[kb + c] = 1 / L_cc.  Written without branches (selects; lane
+// c keeps 1 / L_cc and stores it after the loop) so that the sixteen unrolled
+// steps form one block the compiler can schedule across: FP64 operations
+// and shuffles each take ~25 cycles to complete on this GPU, and a step is a
+// chain of five of them.  Returns true on a pivot that is not > 0.
 __device__ __noinline__ bool warp_chol16(double *D, int ld, int kb, double *dis, int lane) {
   const int i = lane & 15, h = lane >> 4;
-  bool bad = false;
   double a[8];
 #pragma unroll
   for (int t = 0; t < 8; ++t) a[t] = 8 * h + t <= i ? D[(kb + i) * ld + kb + 8 * h + t] : 0.0;
+  double myrs = 0.0;
+  bool ok = true;
 #pragma unroll
   for (int c = 0; c < 16; ++c) {
     const int hc = c >> 3, tc = c & 7;
     const double piv = __shfl_sync(0xffffffffu, a[tc], c + 16 * hc);
-    bad |= !(piv > 0.0);
-    const double rs = rsqrt(piv), sq = piv * rs;
-    if (h == hc) {
-      if (i == c) a[tc] = sq;
-      else if (i > c) a[tc] *= rs;
-    }
-    if (lane == 0) dis[kb + c] = rs;
+    ok = ok && piv > 0.0;
+    const double rs = rsqrt(piv);
+    const double sc = a[tc] * rs;
+    const bool mine = h == hc;
+    a[tc] = mine ? (i == c ? piv * rs : (i > c ? sc : a[tc])) : a[tc];
+    myrs = lane == c ? rs : myrs;
     const double oth = __shfl_xor_sync(0xffffffffu, a[tc], 16);
-    const double lic = h == hc ? a[tc] : oth;  // L[i][c]
+    const double lic = mine ? a[tc] : oth;  // L[i][c]
 #pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-      if (jj <= c) continue;
+    for (int jj = c + 1; jj < 16; ++jj) {
       const double ljc = __shfl_sync(0xffffffffu, a[tc], jj + 16 * hc);  // L[jj][c]
-      if (h == (jj >> 3) && i >= jj) a[jj & 7] = __fma_rn(-lic, ljc, a[jj & 7]);
+      const bool upd = h == (jj >> 3) && i >= jj;
+      const double nv = __fma_rn(-lic, ljc, a[jj & 7]);
+      a[jj & 7] = upd ? nv : a[jj & 7];
     }
   }
+  if (lane < 16) dis[kb + lane] = myrs;
 #pragma unroll
   for (int t = 0; t < 8; ++t)
     if (8 * h + t <= i) D[(kb + i) * ld + kb + 8 * h + t] = a[t];
   __syncwarp();
-  return bad;
+  return !ok;
 }
 
 // T = L_bb^-1 of the 16 x 16 lower-triangular block at D[kb..][kb..] (row
-// stride ld) by one warp, lane j < 16 computing column j of T down the column
-// (T_jj = 1 / L_jj from dis, T_ij = -(sum_{j<=k<i} L_ik T_kj) / L_ii), stored
-// transposed: ui[j kUiLd + i] = T_ij, i.e. ui holds (L_bb^T)^-1 = U_bb^-1.
-__device__ __forceinline__ void warp_trinv16(const double *D, int ld, int kb, const double *dis,
-                                             double *ui, int lane) {
-  if (lane < 16) {
-    const int j = lane;
-    double *uj = ui + j * kUiLd;
-    for (int i = 0; i < j; ++i) uj[i] = 0.0;
-    uj[j] = dis[kb + j];
-    for (int i = j + 1; i < 16; ++i) {
-      const double *li = D + (kb + i) * ld + kb;
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s = __fma_rn(li[k], uj[k], s);
-      uj[i] = -s * dis[kb + i];
+// stride ld) by one warp in registers, lane j (and j + 16) computing column j
+// of T down the column (T_jj = 1 / L_jj from dis, T_ij = -(sum_{j<=k<i} L_ik
+// T_kj) / L_ii), unrolled and without branches; stored transposed:
+// ui[j kUiLd + i] = T_ij, i.e. ui holds (L_bb^T)^-1 = U_bb^-1.
+__device__ __noinline__ void warp_trinv16(const double *D, int ld, int kb, const double *dis,
+                                          double *ui, int lane) {
+  const int j = lane & 15;
+  double t[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; ++k) {
+      const double v = __fma_rn(D[(kb + i) * ld + kb + k], t[k], s);
+      s = k >= j ? v : s;
     }
+    const double di = dis[kb + i];
+    t[i] = i < j ? 0.0 : (i == j ? di : -s * di);
+  }
+  if (lane < 16) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) ui[j * kUiLd + i] = t[i];
   }
   __syncwarp();
 }
@@ -196,13 +207,40 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     const int r = e / kMaxF, f = e % kMaxF;
     ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
   }
+  const bool blockinv = !kTensorSolve && ui != nullptr;
   for (int kb = 0; kb < TB; kb += 16) {
-    // (a) the diagonal block, warp 0 (warp_chol16).
-    if (warp == 0) bad |= warp_chol16(D, ld, kb, dis, lane);
+    // (a) the diagonal block, warp 0 (warp_chol16); with ui also the inverse
+    // of its transpose, U_kk^-1, for the panel below and the row solves of X.
+    if (warp == 0) {
+      bad |= warp_chol16(D, ld, kb, dis, lane);
+      if (blockinv) warp_trinv16(D, ld, kb, dis, ui + kb * kUiLd, lane);
+    }
     sync();
-    // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d.
+    // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d, with ui as
+    // x = d U_kk^-1 on the FP64 tensor cores (warp: 8 rows), else by
+    // substitution.
     const int r0 = kb + 16 + 8 * warp;
-    if (r0 < TB) {
+    if (blockinv && r0 < TB) {
+      double x[2][2];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+        for (int k0 = 0; k0 < 16; k0 += 4) {
+          const double av = D[(r0 + gq) * ld + kb + k0 + tq];
+          const double bv = ui[(kb + k0 + tq) * kUiLd + 8 * nt + gq];
+          dmma(c0, c1, av, bv);
+        }
+        x[nt][0] = c0;
+        x[nt][1] = c1;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        D[(r0 + gq) * ld + kb + 8 * nt + 2 * tq] = x[nt][0];
+        D[(r0 + gq) * ld + kb + 8 * nt + 2 * tq + 1] = x[nt][1];
+      }
+    } else if (r0 < TB) {
       double acc[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[q] = D[(r0 + rsel + 2 * q) * ld + kb + col16];
@@ -249,10 +287,6 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     Us[p * LDS + i] = u;
     if (gu) gu[int64_t(p) * uld + i] = u;
   }
-  // With ui (and ld == LDS): the inverses of U's four 16 x 16 diagonal blocks,
-  // one warp each, for the block-inverse row solves below.
-  const bool blockinv = !kTensorSolve && ui != nullptr;
-  if (blockinv && warp < 4) warp_trinv16(D, ld, 16 * warp, dis, ui + 16 * warp * kUiLd, lane);
   sync();
   // X^T from X^T U = I: rows of the identity solved in place of D.
   for (int e = tid; e < TB * TB; e += 256) D[(e >> 6) * ld + (e & 63)] = (e >> 6) == (e & 63);

@@ -28,7 +28,7 @@ import statistics
 import sys
 
 SPACE = {
-    "PACMAN_B200_INT8_FROM": ["2", "3", "4", "5", "6"],
+    "PACMAN_B200_INT8_FROM": ["1", "2", "3", "4", "5", "6"],
     "PACMAN_B200_GROUPS": ["1", "2", "3", "4", "6", "8"],
     "PACMAN_B200_BIG_N": ["32", "48", "64"],
 }
