@@ -109,7 +109,13 @@ def cpu_baseline(w, seconds_budget: float, threads: int | None = None):
     off, _ = plan.src_csr()
     toff, _ = plan.tgt_csr()
     n = np.diff(off)
-    live = np.diff(toff) > 0
+    mt = np.diff(toff)
+    live = mt > 0
+    # Work proxy of a patch (factorisation ~n^3, evaluation ~m n): within a
+    # stratum the sampled time is scaled by the proxy's sum rather than by
+    # the patch count, which cuts the variance of small samples of large
+    # patches (their time grows as n^3 across the stratum).
+    cost = n.astype(np.float64) ** 3 + 3.0 * n.astype(np.float64) * mt
     K = int(live.sum())
     rng = np.random.default_rng(0)
     edges = [0, 64, 128, 256, 512, 1024, 2048, 1 << 30]
@@ -120,26 +126,36 @@ def cpu_baseline(w, seconds_budget: float, threads: int | None = None):
     # Every solve call also makes one partition-of-unity pass over all targets
     # (and zeroes the output): timed once with no patches, it is taken off
     # each sampled call and counted once per transfer below.
-    t1 = time.perf_counter()
-    plan.solve(w["basis"], vals, patch_list=np.zeros(0, dtype=np.int64))
-    t_call = time.perf_counter() - t1
+    calls0 = []
+    for _ in range(3):
+        t1 = time.perf_counter()
+        plan.solve(w["basis"], vals, patch_list=np.zeros(0, dtype=np.int64))
+        calls0.append(time.perf_counter() - t1)
+    t_call = float(np.median(calls0))
     for lo, hi in zip(edges[:-1], edges[1:]):
         ids = np.where((n > lo) & (n <= hi) & live)[0]
         if len(ids) == 0:
             continue
         rng.shuffle(ids)
-        # Grow the sample until the stratum's time budget is used.
-        take = 1
-        spent = 0.0
+        # Grow the sample until the stratum's time budget is used; the calls'
+        # fixed cost is taken off the stratum's sum (not per call, so that
+        # its noise averages out).
+        # At least one patch per thread per call: the restatement runs the
+        # patches of a call in parallel, one per thread, as the full
+        # transfer does.
+        take = min(len(ids), max(threads, min(len(ids) // 64, 64) if lo < 512 else 1))
+        raw = 0.0
+        calls = 0
         done = 0
-        while done < len(ids) and spent < budget_each:
+        while done < len(ids) and raw - calls * t_call < budget_each:
             chunk = ids[done:done + take]
             t1 = time.perf_counter()
             plan.solve(w["basis"], vals, patch_list=chunk)
-            spent += max(time.perf_counter() - t1 - t_call, 0.0)
+            raw += time.perf_counter() - t1
+            calls += 1
             done += len(chunk)
             take = min(take * 2, len(ids) - done) if done < len(ids) else take
-        total += spent * len(ids) / done
+        total += max(raw - calls * t_call, 0.0) * cost[ids].sum() / cost[ids[:done]].sum()
         sampled += done
     t_pu = t_call
     est = t_geom + total + t_pu

@@ -209,38 +209,12 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
   }
   const bool blockinv = !kTensorSolve && ui != nullptr;
   for (int kb = 0; kb < TB; kb += 16) {
-    // (a) the diagonal block, warp 0 (warp_chol16); with ui also the inverse
-    // of its transpose, U_kk^-1, for the panel below and the row solves of X.
-    if (warp == 0) {
-      bad |= warp_chol16(D, ld, kb, dis, lane);
-      if (blockinv) warp_trinv16(D, ld, kb, dis, ui + kb * kUiLd, lane);
-    }
+    // (a) the diagonal block, warp 0 (warp_chol16).
+    if (warp == 0) bad |= warp_chol16(D, ld, kb, dis, lane);
     sync();
-    // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d, with ui as
-    // x = d U_kk^-1 on the FP64 tensor cores (warp: 8 rows), else by
-    // substitution.
+    // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d.
     const int r0 = kb + 16 + 8 * warp;
-    if (blockinv && r0 < TB) {
-      double x[2][2];
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) {
-        double c0 = 0.0, c1 = 0.0;
-#pragma unroll
-        for (int k0 = 0; k0 < 16; k0 += 4) {
-          const double av = D[(r0 + gq) * ld + kb + k0 + tq];
-          const double bv = ui[(kb + k0 + tq) * kUiLd + 8 * nt + gq];
-          dmma(c0, c1, av, bv);
-        }
-        x[nt][0] = c0;
-        x[nt][1] = c1;
-      }
-      __syncwarp();
-#pragma unroll
-      for (int nt = 0; nt < 2; ++nt) {
-        D[(r0 + gq) * ld + kb + 8 * nt + 2 * tq] = x[nt][0];
-        D[(r0 + gq) * ld + kb + 8 * nt + 2 * tq + 1] = x[nt][1];
-      }
-    } else if (r0 < TB) {
+    if (r0 < TB) {
       double acc[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[q] = D[(r0 + rsel + 2 * q) * ld + kb + col16];
@@ -287,6 +261,9 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     Us[p * LDS + i] = u;
     if (gu) gu[int64_t(p) * uld + i] = u;
   }
+  // With ui: the inverses of U's four 16 x 16 diagonal blocks, one warp each,
+  // for the block-inverse row solves of X below.
+  if (blockinv && warp < 4) warp_trinv16(D, ld, 16 * warp, dis, ui + 16 * warp * kUiLd, lane);
   sync();
   // X^T from X^T U = I: rows of the identity solved in place of D.
   for (int e = tid; e < TB * TB; e += 256) D[(e >> 6) * ld + (e & 63)] = (e >> 6) == (e & 63);
