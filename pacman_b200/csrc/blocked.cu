@@ -840,19 +840,14 @@ void solve_big(Plan &p, int basis, const double *vals, int F, bool lu,
     }
     a.slices = nullptr;
     a.dpart = nullptr;
-    a.dcount = nullptr;
     DevMem ddiag;
     if (oz && tot_sl > 0) {
       dsl.alloc(size_t(tot_sl), st);
       a.slices = dsl.as<uint8_t>();
-      // The int8 steps' diagonal-tile hand-over: a TB x TB part and an
-      // arrival counter per slot (counters start at zero, the finishing CTA
-      // of each step puts its slot's back to zero).
-      const size_t part_bytes = sizeof(double) * TB * TB * size_t(ns);
-      ddiag.alloc(part_bytes + sizeof(int) * size_t(ns), st);
+      // The int8 steps' next diagonal tile: D' (TB x TB per slot), written by
+      // the step's diagonal item and factored by k_diag_next.
+      ddiag.alloc(sizeof(double) * TB * TB * size_t(ns), st);
       a.dpart = ddiag.as<double>();
-      a.dcount = reinterpret_cast<int *>(ddiag.as<char>() + part_bytes);
-      PB_CUDA(cudaMemsetAsync(a.dcount, 0, sizeof(int) * size_t(ns), st));
     }
     const size_t n_inv = lu ? size_t(2) * TB * TB * ns : size_t(tot_inv);
     const size_t n_beta = size_t(4) * kMaxF * ns;

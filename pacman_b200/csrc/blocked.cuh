@@ -389,8 +389,7 @@ struct BigArgs {
   double oz_mul;       // 128 / sigma (sigma bounds |L|)
   double oz_sig2;      // sigma^2
   int wait_limit;      // polls of a tensor-core pipeline wait before it gives up
-  double *dpart;       // mixed forward: per slot, the diagonal CTA's part of the next diagonal tile (TB x TB)
-  int *dcount;         // mixed forward: per slot, arrivals at the next diagonal tile (zero between steps)
+  double *dpart;       // mixed forward: per slot, D' of the next diagonal tile (TB x TB)
 };
 
 // Polls of a tensor-core pipeline wait (mbarrier) before the step gives up

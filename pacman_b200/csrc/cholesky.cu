@@ -321,6 +321,58 @@ __global__ void __launch_bounds__(256, 4) k_diag_chol(BigArgs a, const BigSlot *
   if (threadIdx.x == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
+// The next diagonal tile after an int8 step j, one CTA per slot with
+// T > j + 1 (the first cnt slots): D = D' - L[j+1, j] L[j+1, j]^T, with D'
+// (the tile minus the products of columns p < j) written by the step's
+// diagonal item to dpart and L[j+1, j] by its row item j + 1; then
+// diag_tile_t with block-inverse row solves (X_{j+1}, U_{j+1}, y_{j+1}).  A
+// separate launch rather than a hand-over inside the step: the factorisation
+// of a 64 x 64 tile is a chain of 64 pivots that keeps one warp busy for tens
+// of microseconds, and here two CTAs per SM overlap their chains while the
+// step kernel's CTAs go on with their items.
+constexpr size_t kDiagNextSmem =
+    (size_t(2) * TB * LDS + size_t(4) * 16 * kUiLd + 3 * TB + TB * kMaxF) * sizeof(double);
+__global__ void __launch_bounds__(256, 2) k_diag_next(BigArgs a, const BigSlot *__restrict__ slots,
+                                                      int j) {
+  extern __shared__ __align__(16) double smn[];
+  double *D = smn;                  // D' and then D (TB x LDS)
+  double *Ls = D + TB * LDS;        // L[j+1, j], then U scratch
+  double *ui = Ls + TB * LDS;       // U's 16 x 16 diagonal block inverses
+  double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(ui + 4 * 16 * kUiLd);
+  double *dis = ui + 4 * 16 * kUiLd + 2 * TB;
+  double(*ys)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(dis + TB);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const BigSlot sl = slots[blockIdx.x];
+  const int ld = sl.ld;
+  double *W = a.W + sl.base;
+  const double *dp = a.dpart + int64_t(sl.q) * TB * TB;
+  const double *lg = W + int64_t(j + 1) * TB * ld + int64_t(j) * TB;
+  for (int idx = tid; idx < TB * TB / 2; idx += 256) {
+    const int r = idx >> 5, c2 = idx & 31;
+    cp_async16(D + r * LDS + 2 * c2, dp + r * TB + 2 * c2);
+    cp_async16(Ls + r * LDS + 2 * c2, lg + int64_t(r) * ld + 2 * c2);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  {
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+    double acc[4][4][2];
+    if (warp < 4) {
+      acc_load(acc, D, LDS, wr, wc, lane);
+      mma64<false, true>(Ls, Ls, acc, -1.0, wr, wc, lane);
+    }
+    __syncthreads();
+    if (warp < 4) acc_store(acc, D, LDS, wr, wc, lane);
+  }
+  __syncthreads();
+  auto sync = [] { __syncthreads(); };
+  const bool bad = diag_tile_t(D, LDS, W + int64_t(j + 1) * TB * ld + int64_t(sl.T) * TB, ld, a.F,
+                               a.inv + sl.inv + int64_t(j + 1) * TB * TB, Ls, cv, dis, ys, tid,
+                               sync, W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, ui);
+  if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
+}
+
 // Phase 2 of a factorisation step (256 threads, warp w: rows 16 w .. + 15,
 // in two passes of 8).  sC holds C (row tiles i0, and i0 + 1 when arows =
 // 2 TB; kColRows x LDS).  L[i, j] solves L[i, j] U_j = C with U_j = L_jj^T
@@ -698,8 +750,8 @@ __global__ void __launch_bounds__(kColThreads, 2)
 // row tile i of column j (C = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T, then
 // L[i, j] U_j = C solved against the diagonal tile's factor, the forward
 // substitution and the int8 slices of L[i, j]), or the diagonal item of a
-// slot (D' of tile j + 1).  Each CTA takes a contiguous range of the step's
-// items.
+// slot (D' of tile j + 1, left in dpart for k_diag_next).  Each CTA takes a
+// contiguous range of the step's items; nothing waits on another CTA.
 //   warp 0 (one thread): bulk copies of the slice half-tiles (K = 32) of the
 //     item's row tile and of the column tile row through a kWsStages ring;
 //   warp 1 (one thread): the tcgen05 MMAs into one TMEM accumulator;
@@ -727,8 +779,8 @@ constexpr int kWsHalfA = 2 * kWsChunkA;                  // 16384
 constexpr int kWsStage = kWsHalfA + kWsHalf;             // row half + column half
 constexpr int kWsThreads = 320;                          // 2 issue warps + 8 epilogue warps
 constexpr int kWsCOff = kWsStages * kWsStage;            // C / D (TB x LDS doubles)
-constexpr int kWsXOff = kWsCOff + TB * LDS * 8;          // X_j, or diag_tile scratch
-constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // L[j+1, j] (finisher)
+constexpr int kWsXOff = kWsCOff + TB * LDS * 8;          // U_j, the diagonal tile's factor
+constexpr int kWsLOff = kWsXOff + TB * LDS * 8;          // upper TMEM lanes' level sums
 constexpr int kWsPtsOff = kWsLOff + TB * LDS * 8;        // row points (2 x TB), column points
 constexpr int kWsRedOff = kWsPtsOff + 2 * TB * 32 + 3 * TB * 8;  // y_j, r_i, diag_tile vectors
 constexpr int kWsUiOff = kWsRedOff + 3 * TB * kMaxF * 8;  // U_j's diagonal block inverses
@@ -742,7 +794,7 @@ static_assert(2 * TB * kMaxF + 3 * TB <= 3 * TB * kMaxF, "residual rows after th
 
 struct WsBars {
   uint64_t full[kWsStages], empty[kWsStages], acc_full, acc_empty, done;
-  int abort_flag, arrive_flag, ep_stop;
+  int abort_flag, ep_stop;
   uint32_t tmem;
 };
 static_assert(sizeof(WsBars) <= 256, "barrier area");
@@ -928,21 +980,6 @@ __device__ __forceinline__ void ws_gen_tile(const BigArgs &a, const BigSlot &sl,
   }
 }
 
-// oz_diag_arrive for the 256 epilogue threads (etid 0 arrives).
-__device__ __forceinline__ bool ws_diag_arrive(int *count, volatile int *flag, int etid) {
-  __threadfence();
-  ws_sync();
-  if (etid == 0) {
-    const int old = atomicAdd(count, 1);
-    *flag = old;
-    if (old == 1) *count = 0;
-  }
-  ws_sync();
-  const bool last = *flag == 1;
-  if (last) __threadfence();
-  return last;
-}
-
 __global__ void __launch_bounds__(kWsThreads, 1)
     k_col_step_ws(BigArgs a, const BigSlot *__restrict__ slots, const int *__restrict__ ipre,
                   int cnt, int j) {
@@ -1055,7 +1092,6 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     // Epilogue: 8 warps, etid 0..255.
     const int etid = tid - 64, ew = warp - 2;
     const int qd = warp & 3, h = ew >> 2;
-    const int wr = (ew >> 1) * 32, wc = (ew & 1) * 32;  // trsm blocks (ew < 4)
     double *sC = reinterpret_cast<double *>(smb + kWsCOff);
     double *sX = reinterpret_cast<double *>(smb + kWsXOff);
     double *sL = reinterpret_cast<double *>(smb + kWsLOff);
@@ -1065,7 +1101,6 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     double *rsh = ysh + TB * kMaxF + 3 * TB;                     // r_i, TB x kMaxF
     double *sUi = reinterpret_cast<double *>(smb + kWsUiOff);   // [b][k][c] = U_bb^-1[k][c]
                                                                  // (row stride kUiLd)
-    volatile int *arrive_flag = &bar->arrive_flag;
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
     ws_sync();
@@ -1090,7 +1125,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       const bool diag = w.r == 0;
       const int i = diag ? j + 1 : j + w.r;
       if (!diag) {
-        // U_j and y_j once per slot (the finisher reuses their buffers), the
+        // U_j (and its block inverses) and y_j once per slot, the
         // residual rows r_i of every item: copied while the tile is made.
         if (xq != w.q) {
           load_factor_async(sX, W + int64_t(j) * TB * ld + int64_t(j) * TB, ld, etid, 256);
@@ -1131,8 +1166,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
       tc_fence_after();
       // C = A - sigma^2 (lower-lane levels + upper-lane levels): sC gets A
-      // minus the lower lanes' sums, sL (free until the finisher) the upper
-      // lanes' sums.
+      // minus the lower lanes' sums, sL the upper lanes' sums.
       ws_drain(tmem, qd, h, sC, sL, a.oz_sig2, lane);
       tc_fence_before();
       __syncwarp();
@@ -1144,9 +1178,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         nidx = ws_point_index(a, nxt.sl, nxt.s0, wn.r == 0 ? j + 1 : j + wn.r, etid);
       }
       // C = sC - sigma^2 sL is formed where it is read: by the diagonal
-      // item's copy, or by the triangular solve's loads.
-      bool finish = false;
-      // The copies of the next item's row points (one commit group per item).
+      // item's copy, or by the triangular solve's loads.  The copies of the
+      // next item's row points go out as one commit group per item.
       auto next_points = [&]() {
         if (it + 1 < it1) {
           if (etid < TB) ws_point_copy(a, prows + ((k + 1) & 1) * TB, etid, nidx);
@@ -1154,22 +1187,17 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         }
       };
       if (diag) {
-        // D' into sC (this CTA may finish the tile) and to dpart (for the
-        // other producer, if it arrives last).
+        // D' to dpart, where the next launch (k_diag_next) factors D.
         double *dst = a.dpart + int64_t(sl.q) * TB * TB;
         for (int e = etid; e < TB * TB; e += 256) {
           const int o = (e >> 6) * LDS + (e & 63);
-          const double d = __fma_rn(-a.oz_sig2, sL[o], sC[o]);
-          sC[o] = d;
-          dst[e] = d;
+          dst[e] = __fma_rn(-a.oz_sig2, sL[o], sC[o]);
         }
         next_points();
-        finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
       } else {
         // L[i, j] U_j = C by blocked row solves (warp ew: rows 8 ew .. + 7),
         // stored; forward substitution; int8 slices.
         cp_async_wait<0>();
-        ws_sync();
         ws_sync();
         const int r0 = 8 * ew;
         warp_rows_trsm8_bi(sC + r0 * LDS, sX, sUi, lane, sL + r0 * LDS, a.oz_sig2);
@@ -1203,36 +1231,6 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           uint8_t *dst = slice_row(sl, i) + int64_t(j) * kOzTileBytes;
           slice_tile_smem(sC, TB, a.oz_mul, dst, dst, etid, 256);
         }
-        if (i == j + 1) finish = ws_diag_arrive(a.dcount + sl.q, arrive_flag, etid);
-        else ws_sync();
-        if (finish) {
-          const double *src = a.dpart + int64_t(sl.q) * TB * TB;
-          for (int e = etid; e < TB * TB; e += 256) sC[(e >> 6) * LDS + (e & 63)] = __ldcg(src + e);
-        }
-      }
-      if (finish) {
-        // D = D' - L[j+1, j] L[j+1, j]^T, factored: X_{j+1}, y_{j+1}.
-        const double *lg = W + int64_t(j + 1) * TB * ld + int64_t(j) * TB;
-        for (int e = etid; e < TB * TB; e += 256)
-          sL[(e >> 6) * LDS + (e & 63)] = __ldcg(lg + int64_t(e >> 6) * ld + (e & 63));
-        ws_sync();
-        double acc[4][4][2];
-        if (ew < 4) {
-          acc_load(acc, sC, LDS, wr, wc, lane);
-          mma64<false, true>(sL, sL, acc, -1.0, wr, wc, lane);
-        }
-        ws_sync();
-        if (ew < 4) acc_store(acc, sC, LDS, wr, wc, lane);
-        ws_sync();
-        double(*ysd)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(ysh);
-        double(*cv)[TB] = reinterpret_cast<double(*)[TB]>(ysh + TB * kMaxF);
-        double *dis = ysh + TB * kMaxF + 2 * TB;
-        const bool bad = diag_tile_t(sC, LDS, rcol + int64_t(j + 1) * TB * ld, ld, F,
-                                     a.inv + sl.inv + int64_t(j + 1) * TB * TB, sX, cv, dis, ysd,
-                                     etid, ws_sync,
-                                     W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, sL);
-        if (etid == 0 && bad) atomicOr(&a.status[sl.k], 4);
-        xq = -1;  // sX was the factor's scratch
       }
       ws_sync();
     }
@@ -1243,8 +1241,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   tc_fence_after();
   __syncthreads();
   // After a time-out, the patches of every item of this CTA's range are
-  // marked for the FP64 LU (a slot whose diagonal hand-over this CTA did not
-  // complete is among them).
+  // marked for the FP64 LU.
   if (*abort_flag)
     for (int it = it0 + tid; it < it1; it += kWsThreads)
       atomicOr(&a.status[slots[ws_item(ipre, cnt, it).q].k], 8);
@@ -1756,6 +1753,8 @@ void chol_set_smem_attributes() {
                                int(kWsSmem)));
   PB_CUDA(cudaFuncSetAttribute(k_diag_chol, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(kDiagSmem)));
+  PB_CUDA(cudaFuncSetAttribute(k_diag_next, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kDiagNextSmem)));
   {
 #define PB_SWEEP_ATTR(K, F)                                                                   \
   PB_CUDA(cudaFuncSetAttribute(K<F, bk_stages(F)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
@@ -1809,6 +1808,8 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       const int items = cp.pre[cp.ioff[j] + c];
       k_col_step_ws<<<std::min(items, sms), kWsThreads, kWsSmem, st>>>(a, ds, dpre + cp.ioff[j],
                                                                        c, j);
+      note_launch();
+      k_diag_next<<<c, 256, kDiagNextSmem, st>>>(a, ds, j);
     }
     note_launch();
     if (rep.time_kernels) {
