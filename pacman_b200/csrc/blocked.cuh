@@ -233,54 +233,60 @@ __device__ __forceinline__ void warp_rows_trsm8_bi(double *rows, const double *s
                                                    const double *sUi, int lane,
                                                    const double *up, double sig2) {
   const int g = lane >> 2, t = lane & 3;
-  if (up) {
+  // The warp's 8 x 64 right-hand side stays in registers in the tensor
+  // cores' accumulator layout (lane: row g, columns 8 nt + 2 t, + 1); only
+  // the 8 x 16 block being solved goes through shared memory, once to be
+  // read as the products' A operand and once as the result.
+  double c[8][2];
 #pragma unroll
-    for (int e = lane; e < 8 * TB; e += 32) {
-      const int o = (e >> 6) * LDS + (e & 63);
-      rows[o] = __fma_rn(-sig2, up[o], rows[o]);
+  for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int o = g * LDS + 8 * nt + 2 * t + e;
+      c[nt][e] = up ? __fma_rn(-sig2, up[o], rows[o]) : rows[o];
     }
-    __syncwarp();
-  }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int cb = 16 * b;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      rows[g * LDS + cb + 8 * h + 2 * t] = c[2 * b + h][0];
+      rows[g * LDS + cb + 8 * h + 2 * t + 1] = c[2 * b + h][1];
+    }
+    __syncwarp();
+    double af[4];
+#pragma unroll
+    for (int k4 = 0; k4 < 4; ++k4) af[k4] = rows[g * LDS + cb + 4 * k4 + t];
     // X_b = R_b Ui_b, two 8-column halves.
     double x[2][2];
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
+    for (int h = 0; h < 2; ++h) {
       double c0 = 0.0, c1 = 0.0;
 #pragma unroll
-      for (int k0 = 0; k0 < 16; k0 += 4) {
-        const double av = rows[g * LDS + cb + k0 + t];
-        const double bv = sUi[(cb + k0 + t) * kUiLd + 8 * nt + g];
-        dmma(c0, c1, av, bv);
-      }
-      x[nt][0] = c0;
-      x[nt][1] = c1;
+      for (int k4 = 0; k4 < 4; ++k4)
+        dmma(c0, c1, af[k4], sUi[(cb + 4 * k4 + t) * kUiLd + 8 * h + g]);
+      x[h][0] = c0;
+      x[h][1] = c1;
     }
     __syncwarp();
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-      rows[g * LDS + cb + 8 * nt + 2 * t] = x[nt][0];
-      rows[g * LDS + cb + 8 * nt + 2 * t + 1] = x[nt][1];
+    for (int h = 0; h < 2; ++h) {
+      rows[g * LDS + cb + 8 * h + 2 * t] = x[h][0];
+      rows[g * LDS + cb + 8 * h + 2 * t + 1] = x[h][1];
     }
-    __syncwarp();
-    // Columns to the right: R[:, n] -= X_b U[b, n], 8-column tiles (b is a
-    // constant here, so the tiles' product chains are interleaved).
+    if (b < 3) {
+      __syncwarp();
 #pragma unroll
-    for (int nt = 2 * b + 2; nt < 8; ++nt) {
-      double c0 = rows[g * LDS + 8 * nt + 2 * t], c1 = rows[g * LDS + 8 * nt + 2 * t + 1];
+      for (int k4 = 0; k4 < 4; ++k4) af[k4] = -rows[g * LDS + cb + 4 * k4 + t];
+      // Columns to the right: R[:, n] -= X_b U[b, n], 8-column tiles.
 #pragma unroll
-      for (int k0 = 0; k0 < 16; k0 += 4) {
-        const double av = -rows[g * LDS + cb + k0 + t];
-        const double bv = sU[(cb + k0 + t) * LDS + 8 * nt + g];
-        dmma(c0, c1, av, bv);
-      }
-      rows[g * LDS + 8 * nt + 2 * t] = c0;
-      rows[g * LDS + 8 * nt + 2 * t + 1] = c1;
+      for (int nt = 2 * b + 2; nt < 8; ++nt)
+#pragma unroll
+        for (int k4 = 0; k4 < 4; ++k4)
+          dmma(c[nt][0], c[nt][1], af[k4], sU[(cb + 4 * k4 + t) * LDS + 8 * nt + g]);
     }
-    __syncwarp();
   }
+  __syncwarp();
 }
 
 // warp_rows_trsm8 with the off-diagonal block products on the FP64 tensor
