@@ -598,7 +598,9 @@ def main():
     # Plain FP64 path (the reference's unpivoted-LU algorithm) over the same
     # number of timed steps, and the agreement of the two paths.
     extra = {"ms_per_step_median": statistics.median(times),
-             "e2e_ms_per_step_median": statistics.median(e2e_times)}
+             "e2e_ms_per_step_median": statistics.median(e2e_times),
+             "step_ms": [round(t, 3) for t in times],
+             "e2e_step_ms": [round(t, 3) for t in e2e_times]}
     if not args.no_fp64_compare:
         out_mixed = step(args.precision).cpu().numpy()
         f64_stats = {}
