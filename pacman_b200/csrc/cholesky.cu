@@ -1166,8 +1166,9 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       }
       tc_fence_after();
       // C = A - sigma^2 (lower-lane levels + upper-lane levels): sC gets A
-      // minus the lower lanes' sums, sL the upper lanes' sums.
-      ws_drain(tmem, qd, h, sC, sL, a.oz_sig2, lane);
+      // minus the lower lanes' sums, sL the upper lanes' sums.  At j = 0
+      // there are no products (no MMAs were issued) and C = A.
+      if (j > 0) ws_drain(tmem, qd, h, sC, sL, a.oz_sig2, lane);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cnt(&bar->acc_empty, 1);
@@ -1191,7 +1192,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         double *dst = a.dpart + int64_t(sl.q) * TB * TB;
         for (int e = etid; e < TB * TB; e += 256) {
           const int o = (e >> 6) * LDS + (e & 63);
-          dst[e] = __fma_rn(-a.oz_sig2, sL[o], sC[o]);
+          dst[e] = j > 0 ? __fma_rn(-a.oz_sig2, sL[o], sC[o]) : sC[o];
         }
         next_points();
       } else {
@@ -1200,7 +1201,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         cp_async_wait<0>();
         ws_sync();
         const int r0 = 8 * ew;
-        warp_rows_trsm8_bi(sC + r0 * LDS, sX, sUi, lane, sL + r0 * LDS, a.oz_sig2);
+        warp_rows_trsm8_bi(sC + r0 * LDS, sX, sUi, lane, j > 0 ? sL + r0 * LDS : nullptr,
+                           a.oz_sig2);
         next_points();
         double lo[8], hi[8];
 #pragma unroll
@@ -1274,11 +1276,16 @@ constexpr int kBkTile = TB * TB * 8;  // bytes of one stage
 // SM, for more fields (registers).
 constexpr int bk_stages(int F) { return F <= 2 ? 3 : 5; }
 
-size_t chol_back_smem(int F) {
+size_t chol_back_smem(int F, int S = 0) {
   // stages, part, accs, full/empty barriers, abort flag and issue counter
-  const int S = bk_stages(F);
+  if (S == 0) S = bk_stages(F);
   return size_t(S) * kBkTile + size_t(8 * TB * F + TB * F) * 8 + 2 * S * 8 + 16;
 }
+// The deep ring of the one-field backward sweep (one CTA per SM, twice the
+// tiles in flight): a slot's sweep streams its T (T - 1) / 2 tiles through
+// one SM, so the largest slots' sweeps are set by the bytes one SM keeps in
+// flight (PACMAN_B200_BACK_STAGES = 6 selects it).
+constexpr int kBkDeep = 6;
 
 
 // Bounded wait for a phase that gives up early once the CTA has aborted.
@@ -1760,6 +1767,9 @@ void chol_set_smem_attributes() {
   PB_CUDA(cudaFuncSetAttribute(K<F, bk_stages(F)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                int(std::max(chol_back_smem(F), chol_fwd_smem(F)))))
     PB_SWEEP_ATTR(k_chol_back, 1);
+    PB_CUDA(cudaFuncSetAttribute(k_chol_back<1, kBkDeep>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(chol_back_smem(1, kBkDeep))));
     PB_SWEEP_ATTR(k_chol_back, 2);
     PB_SWEEP_ATTR(k_chol_back, 4);
     PB_SWEEP_ATTR(k_chol_back, kMaxF);
@@ -1782,7 +1792,7 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
   const Tuning &tu = tuning_for_current_device();
   const int sms = tu.sms;
   // First step on the int8 tensor cores: tuned, PACMAN_B200_INT8_FROM overrides.
-  const int oz_from = std::max(1, tuned_int("PACMAN_B200_INT8_FROM", tu.int8_from));
+  const int oz_from = std::max(0, tuned_int("PACMAN_B200_INT8_FROM", tu.int8_from));
   bool tail = tail_event == nullptr;
   for (int j = 0; j < steps; ++j) {
     const int c = cp.cnt[j];
@@ -1873,7 +1883,11 @@ void finish_kernel_timing(SolveReport &rep, cudaEvent_t ref) {
 void chol_launch_finish(const BigArgs &a, const BigSlot *ds, int ns, bool adjoint,
                         cudaStream_t st) {
   const size_t smem = chol_back_smem(a.F);
-  if (a.F == 1) k_chol_back<1, bk_stages(1)><<<ns, 288, smem, st>>>(a, ds);
+  const bool deep = tuned_int("PACMAN_B200_BACK_STAGES", tuning_for_current_device().back_stages) ==
+                    kBkDeep;
+  if (a.F == 1 && deep)
+    k_chol_back<1, kBkDeep><<<ns, 288, chol_back_smem(1, kBkDeep), st>>>(a, ds);
+  else if (a.F == 1) k_chol_back<1, bk_stages(1)><<<ns, 288, smem, st>>>(a, ds);
   else if (a.F <= 2) k_chol_back<2, bk_stages(2)><<<ns, 288, smem, st>>>(a, ds);
   else if (a.F <= 4) k_chol_back<4, bk_stages(4)><<<ns, 288, smem, st>>>(a, ds);
   else k_chol_back<kMaxF, bk_stages(kMaxF)><<<ns, 288, smem, st>>>(a, ds);

@@ -209,6 +209,7 @@ struct Tuning {
   int big_n_chol = 64;  // patches above this size use the tiled Cholesky (mixed)
   int int8_from = 4;    // first tile column updated on the int8 tensor cores
   int groups = 0;       // slot groups of the tiled engine (0: min(4, slots / 8))
+  int back_stages = 3;  // ring depth of the one-field backward sweep (3 or 6)
   int sms = 148;
   std::string source = "built-in defaults";
 };

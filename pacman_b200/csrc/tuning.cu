@@ -64,6 +64,7 @@ void parse(const std::string &path, Tuning &t) {
     if (key == "PACMAN_B200_BIG_N") t.big_n_chol = v;
     else if (key == "PACMAN_B200_INT8_FROM") t.int8_from = v;
     else if (key == "PACMAN_B200_GROUPS") t.groups = v;
+    else if (key == "PACMAN_B200_BACK_STAGES") t.back_stages = v;
   }
 }
 

@@ -9,7 +9,9 @@ defaults:
 * ``PACMAN_B200_GROUPS``: slot groups of the tiled engine, each stepping on
   its own stream;
 * ``PACMAN_B200_BIG_N``: patches above this size use the tiled Cholesky
-  instead of the register kernels (at most 64).
+  instead of the register kernels (at most 64);
+* ``PACMAN_B200_BACK_STAGES``: ring depth (3 or 6) of the one-field
+  backward sweep.
 
 The library reads each parameter per call from the environment, so the
 tuner sets them there.  With ``--write`` the best choice goes to
@@ -28,12 +30,13 @@ import statistics
 import sys
 
 SPACE = {
-    "PACMAN_B200_INT8_FROM": ["1", "2", "3", "4", "5", "6"],
+    "PACMAN_B200_INT8_FROM": ["0", "1", "2", "3", "4", "5", "6"],
     "PACMAN_B200_GROUPS": ["1", "2", "3", "4", "6", "8"],
     "PACMAN_B200_BIG_N": ["32", "48", "64"],
+    "PACMAN_B200_BACK_STAGES": ["3", "6"],
 }
 DEFAULTS = {"PACMAN_B200_INT8_FROM": "4", "PACMAN_B200_GROUPS": "4",
-            "PACMAN_B200_BIG_N": "64"}
+            "PACMAN_B200_BIG_N": "64", "PACMAN_B200_BACK_STAGES": "3"}
 
 
 def conf_path(device_name: str) -> str:
