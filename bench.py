@@ -700,7 +700,8 @@ def main():
         "ms_span_per_step": ms_i8,
         "share_of_step": ms_i8 / ms_per_step if ms_per_step else None,
         "fp64_steps": {
-            "kernel": "k_col_step<1> (steps 0-3: column update on the FP64 tensor cores, "
+            "kernel": "k_col_step<1> (the tile columns below PACMAN_B200_INT8_FROM, none "
+                      "with the tuned B200 setting: column update on the FP64 tensor cores, "
                       "mma.sync f64)",
             "achieved": kst.get("update_flops_f64", 0.0) / (ms_f64 * 1e-3) / 1e12 if ms_f64 else 0,
             "peak": dgemm, "unit": "TFLOP/s",

@@ -208,10 +208,10 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
   }
   const bool blockinv = !kTensorSolve && ui != nullptr;
-  for (int kb = 0; kb < TB; kb += 16) {
-    // (a) the diagonal block, warp 0 (warp_chol16).
-    if (warp == 0) bad |= warp_chol16(D, ld, kb, dis, lane);
-    sync();
+  // (a) the first diagonal block, warp 0 (warp_chol16).
+  if (warp == 0) bad |= warp_chol16(D, ld, 0, dis, lane);
+  sync();
+  for (int kb = 0; kb + 16 < TB; kb += 16) {
     // (b) the panel below: rows kb + 16 .. 63 solve x L_kk^T = d.
     const int r0 = kb + 16 + 8 * warp;
     if (r0 < TB) {
@@ -234,22 +234,34 @@ __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int
     }
     sync();
     // (c) trailing blocks: D[i, j] -= P_i P_j^T (P: the panel columns), 8 x 8
-    // output tiles (ti, tj) with kb + 16 <= 8 tj <= 8 ti, four per warp step.
-    {
-      const int base = (kb + 16) / 8, nt = 8 - base;
-      for (int u = warp; u < nt * nt; u += 8) {
-        const int ti = base + u / nt, tj = base + u % nt;
-        if (tj > ti) continue;
-        double c0 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq];
-        double c1 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1];
+    // output tiles (ti, tj) with kb + 16 <= 8 tj <= 8 ti.  Warp 0 updates
+    // the next diagonal block's three tiles first and factors that block
+    // (look-ahead) while warps 1..7 update the rest: the chain of diagonal
+    // blocks does not wait for the whole trailing update.
+    const int base = (kb + 16) / 8, nt = 8 - base;
+    auto tile = [&](int ti, int tj) {
+      double c0 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq];
+      double c1 = D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1];
 #pragma unroll
-        for (int k0 = 0; k0 < 16; k0 += 4) {
-          const double av = -D[(8 * ti + gq) * ld + kb + k0 + tq];
-          const double bv = D[(8 * tj + gq) * ld + kb + k0 + tq];
-          dmma(c0, c1, av, bv);
-        }
-        D[(8 * ti + gq) * ld + 8 * tj + 2 * tq] = c0;
-        D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1] = c1;
+      for (int k0 = 0; k0 < 16; k0 += 4) {
+        const double av = -D[(8 * ti + gq) * ld + kb + k0 + tq];
+        const double bv = D[(8 * tj + gq) * ld + kb + k0 + tq];
+        dmma(c0, c1, av, bv);
+      }
+      D[(8 * ti + gq) * ld + 8 * tj + 2 * tq] = c0;
+      D[(8 * ti + gq) * ld + 8 * tj + 2 * tq + 1] = c1;
+    };
+    if (warp == 0) {
+      tile(base, base);
+      tile(base + 1, base);
+      tile(base + 1, base + 1);
+      __syncwarp();
+      bad |= warp_chol16(D, ld, kb + 16, dis, lane);
+    } else {
+      for (int u = warp - 1; u < nt * nt; u += 7) {
+        const int ti = base + u / nt, tj = base + u % nt;
+        if (tj > ti || (ti < base + 2 && tj < base + 2)) continue;
+        tile(ti, tj);
       }
     }
     sync();
