@@ -354,6 +354,8 @@ __global__ void __launch_bounds__(256, 2) k_diag_next(BigArgs a, const BigSlot *
   double *dis = ui + 4 * 16 * kUiLd + 2 * TB;
   double(*ys)[kMaxF] = reinterpret_cast<double(*)[kMaxF]>(dis + TB);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // The next step's launch may start now (its epilogue waits for this grid).
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   const BigSlot sl = slots[blockIdx.x];
   const int ld = sl.ld;
   double *W = a.W + sl.base;
@@ -1115,6 +1117,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
                                                                  // (row stride kUiLd)
     volatile int *ep_stop = &bar->ep_stop;  // written by epilogue threads only
     if (etid == 0) *ep_stop = 0;
+    // The step may be launched while the previous launch (k_diag_next of
+    // step j - 1, which writes U_j, X_j and y_j and reads dpart) still runs:
+    // the copy and MMA warps need only the slices of earlier steps, which
+    // the launch before that wrote, but the epilogue waits for it here.
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
     ws_sync();
     int xq = -1;  // slot whose U_j (factor of the diagonal tile, transposed) is in sX
     int pq = -1, ptj = -1;  // slot and column tile whose points are in cpts
@@ -1828,8 +1835,20 @@ void chol_launch_steps(const BigArgs &a, const BigSlot *ds, const std::vector<Bi
       k_col_step<true><<<n, kColThreads, kColSmem, st>>>(a, ds, dpre + cp.off[j], c, j);
     else {
       const int items = cp.pre[cp.ioff[j] + c];
-      k_col_step_ws<<<std::min(items, sms), kWsThreads, kWsSmem, st>>>(a, ds, dpre + cp.ioff[j],
-                                                                       c, j);
+      // Programmatic dependent launch: the step's copies and MMAs overlap
+      // the tail of the previous k_diag_next (see griddepcontrol.wait in the
+      // kernel); without kernel timing, where events separate the launches.
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(std::min(items, sms));
+      cfg.blockDim = dim3(kWsThreads);
+      cfg.dynamicSmemBytes = kWsSmem;
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = rep.time_kernels ? 0 : 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      PB_CUDA(cudaLaunchKernelEx(&cfg, k_col_step_ws, a, ds, static_cast<const int *>(dpre + cp.ioff[j]), c, j));
       note_launch();
       k_diag_next<<<c, 256, kDiagNextSmem, st>>>(a, ds, j);
     }
