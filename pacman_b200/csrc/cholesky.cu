@@ -196,17 +196,18 @@ template <class Sync, bool kTensorSolve = false>
 __device__ bool diag_tile_t(const double *g_in, int ld, double *rg, int rld, int F, double *gi,
                             double *Us, double (*cv)[TB], double *dis, double (*ys)[kMaxF],
                             int tid, Sync sync, double *gu = nullptr, int uld = 0,
-                            double *ui = nullptr) {
+                            double *ui = nullptr, bool ys_loaded = false) {
   (void)cv;
   double *D = const_cast<double *>(g_in);
   const int lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int col16 = lane & 15, half = lane & 16, rsel = lane >> 4;
   bool bad = false;
-  for (int e = tid; e < TB * kMaxF; e += 256) {
-    const int r = e / kMaxF, f = e % kMaxF;
-    ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
-  }
+  if (!ys_loaded)
+    for (int e = tid; e < TB * kMaxF; e += 256) {
+      const int r = e / kMaxF, f = e % kMaxF;
+      ys[r][f] = f < F ? __ldcg(rg + int64_t(r) * rld + f) : 0.0;
+    }
   const bool blockinv = !kTensorSolve && ui != nullptr;
   // (a) the first diagonal block, warp 0 (warp_chol16).
   if (warp == 0) bad |= warp_chol16(D, ld, 0, dis, lane);
@@ -366,6 +367,10 @@ __global__ void __launch_bounds__(256, 2) k_diag_next(BigArgs a, const BigSlot *
     cp_async16(D + r * LDS + 2 * c2, dp + r * TB + 2 * c2);
     cp_async16(Ls + r * LDS + 2 * c2, lg + int64_t(r) * ld + 2 * c2);
   }
+  // r_{j+1} (the first F columns of the residual tile), for y = X r.
+  double *rg = W + int64_t(j + 1) * TB * ld + int64_t(sl.T) * TB;
+  for (int e = tid; e < TB * a.F; e += 256)
+    cp_async8(&ys[e / a.F][e % a.F], rg + int64_t(e / a.F) * ld + e % a.F);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -381,9 +386,9 @@ __global__ void __launch_bounds__(256, 2) k_diag_next(BigArgs a, const BigSlot *
   }
   __syncthreads();
   auto sync = [] { __syncthreads(); };
-  const bool bad = diag_tile_t(D, LDS, W + int64_t(j + 1) * TB * ld + int64_t(sl.T) * TB, ld, a.F,
-                               a.inv + sl.inv + int64_t(j + 1) * TB * TB, Ls, cv, dis, ys, tid,
-                               sync, W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, ui);
+  const bool bad = diag_tile_t(D, LDS, rg, ld, a.F, a.inv + sl.inv + int64_t(j + 1) * TB * TB, Ls,
+                               cv, dis, ys, tid, sync,
+                               W + int64_t(j + 1) * TB * ld + int64_t(j + 1) * TB, ld, ui, true);
   if (tid == 0 && bad) atomicOr(&a.status[sl.k], 4);
 }
 
