@@ -5,17 +5,18 @@
 // thread (src/rbf_pum/solver/solver.hpp:422-490, KokkosBatched
 // SerialLU<Unblocked>).  A is symmetric positive definite, so here it is
 // factored as L L^T in 64 x 64 tiles, all large patches in lockstep, one tile
-// column j per step and one launch per step (k_col_step):
-//   C[i, j] = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T for every i > j, with the
-//   accumulator in registers for the whole K loop and the L panels streaming
-//   through a cp.async pipeline; then L[i, j] = C X_j^T (X_j = L[j, j]^{-1},
-//   formed one step earlier) and the forward substitution r_i -= L[i, j] y_j;
-//   the CTA of row tile j + 1 also forms, factors and inverts the next
-//   diagonal tile (X_{j+1}, y_{j+1} = X_{j+1} r_{j+1}).
-// k_diag_chol does the diagonal tile of step 0.  Afterwards k_chol_back solves
-// L^T alpha = y (with the kept tile inverses) and k_chol_eval evaluates
-// local = E alpha + V beta (solver.hpp:270-273).  The tile products run on
-// the FP64 tensor cores (mma.sync m8n8k4 f64).
+// column j per step:
+//   C[i, j] = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T for every i > j, then
+//   L[i, j] U_j = C solved against the diagonal tile's factor (U_j = L_jj^T,
+//   made one step earlier) and the forward substitution r_i -= L[i, j] y_j.
+// The column update runs on the int8 tensor cores as split-integer products
+// (k_col_step_ws, with k_diag_next factoring the next diagonal tile after
+// each step) or, for the columns before PACMAN_B200_INT8_FROM and without
+// int8 slices, on the FP64 tensor cores (k_col_step, whose CTA of row tile
+// j + 1 also forms and factors the next diagonal tile).  k_diag_chol does
+// the diagonal tile of step 0.  Afterwards k_chol_back solves L^T alpha = y
+// (with the kept tile inverses X_s = L_ss^-1) and k_chol_eval evaluates
+// local = E alpha + V beta (solver.hpp:270-273).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -601,9 +602,9 @@ __device__ void slice_tile_smem(const double *sL, int nrows, double mul, uint8_t
 //  1. C = A[i, j] - sum_{p<j} L[i, p] L[j, p]^T: eight warps hold 32 x 32
 //     accumulators (starting at -A) for the whole K loop, the L panels stream
 //     through a cp.async pipeline;
-//  2. L[i, j] = C X_j^T, the triangular solve with the inverse factor of the
-//     diagonal tile (made one step earlier), stored; then the forward
-//     substitution r_i -= L[i, j] y_j from the accumulator registers;
+//  2. L[i, j] U_j = C, the triangular solve against the diagonal tile's
+//     factor (made one step earlier), stored; then the forward
+//     substitution r_i -= L[i, j] y_j;
 //  3. CTA 0 (i0 = j + 1) forms the next diagonal tile
 //     D = A[j+1, j+1] - sum_{p<=j} L[j+1, p] L[j+1, p]^T and factors it:
 //     X_{j+1} and y_{j+1} = X_{j+1} r_{j+1} for step j + 1.
