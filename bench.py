@@ -67,6 +67,11 @@ def parse():
     ap.add_argument("--with-fe", action="store_true",
                     help="with --kernels-only: each step also runs the NEAREST_NEAREST "
                          "finite-element transfer of the same points")
+    ap.add_argument("--with-mls", action="store_true",
+                    help="with --kernels-only: each step also runs the moving least squares "
+                         "transfer of the same points")
+    ap.add_argument("--mls-only", action="store_true",
+                    help="with --kernels-only: run only the moving least squares transfers")
     ap.add_argument("--configs", action="store_true",
                     help="one line per configuration of the baseline table (GPU in both "
                          "precisions, the CPU restatement in Serial and OpenMP, errors)")
@@ -478,6 +483,18 @@ def run_configs(args):
     print(json.dumps(line), flush=True)
 
 
+def measure_mls(pacman, S, V0, T, timed, steps):
+    """Moving least squares transfer of device-resident points and one field:
+    one warm call, then the median of `steps` timed calls."""
+    pacman.MLS.interpolate(3, pacman.execspaces.CUDA, S, V0, T)
+    mt = timed(lambda: pacman.MLS.interpolate(3, pacman.execspaces.CUDA, S, V0, T), steps)
+    mms = statistics.median(mt)
+    return {"value": T.shape[0] / (mms * 1e-3), "unit": UNIT, "ms_per_call": mms,
+            "what": "pacman.MLS.interpolate, same sources, targets and first field, "
+                    "device-resident (k_mls: 10-nearest search, Jacobi pseudo-inverse of the "
+                    "10 x 10 moment matrix)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -544,7 +561,12 @@ def main():
         if args.with_adjoint:
             plan = pacman.rbf.Plan(3, S, T, precision=args.precision, **kw)
             G = torch.ones_like(V)
+        V0 = V if V.dim() == 1 else V[:, 0].contiguous()
         for _ in range(args.steps):
+            if args.with_mls or args.mls_only:
+                pacman.MLS.interpolate(3, pacman.execspaces.CUDA, S, V0, T)
+            if args.mls_only:
+                continue
             step(args.precision, st)
             if plan is not None:
                 plan.execute(w["basis"], V, save_for_adjoint=True)
@@ -655,6 +677,13 @@ def main():
             bms = sum(bt) / len(bt)
             batch[prec] = {"value": btot / (bms * 1e-3), "ms_per_call": bms}
         extra["many_uneven_256"] = batch
+
+    # Moving least squares (pacman.MLS.interpolate) over the same points and
+    # the first field, device-resident: K = 10 nearest sources, a quadratic
+    # weighted least-squares fit per target.
+    if world == 1 and not args.no_batch and args.scale == 1.0:
+        extra["mls"] = measure_mls(pacman, S, V if V.dim() == 1 else V[:, 0].contiguous(), T,
+                                   timed, max(3, args.steps))
 
     # Roofline of the dominant kernel: the int8 step kernel of the large-patch
     # Cholesky (k_col_step_ws).  One extra transfer after the timed region,

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define PACMAN_B200_ABI_VERSION 5
+#define PACMAN_B200_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define PACMAN_B200_API __attribute__((visibility("default")))
@@ -259,6 +259,26 @@ PACMAN_B200_API int pacman_b200_fe_interpolate(int32_t dim, int32_t method,
                                                const double *target_points, int64_t n_target,
                                                double *target_values, int32_t *target_status,
                                                const pacman_b200_options *opts);
+
+/*
+ * Moving least squares transfer of the reference's PACMAN::MLS_interpolate
+ * (src/interface.hpp:148-170, src/mls_interface.cpp; the arithmetic of
+ * ArborX 2.1's Interpolation::MovingLeastSquares with its defaults, called at
+ * src/mls/interpolator.hpp:49-77): for each target the K nearest sources
+ * (K = 3, 6, 10 in 1D, 2D, 3D; lowest index on ties; all sources when fewer),
+ * Wendland C0 weights over 1.1 x the farthest neighbour's distance, and the
+ * value at the target of the weighted least-squares quadratic (pseudo-inverse
+ * of the moment matrix, eigenvalues below 1e-13 of the largest dropped).
+ * One scalar field; 0 at every target without sources.  Arrays may be host or
+ * device memory of opts->device; opts (device, stream) may be NULL.  Errors:
+ * PACMAN_B200_ERR_INVALID (null pointer with a non-zero count, negative
+ * count), PACMAN_B200_ERR_DIMENSION, PACMAN_B200_ERR_LIMIT (counts >= 2^31).
+ */
+PACMAN_B200_API int pacman_b200_mls_interpolate(int32_t dim, const double *source_points,
+                                                int64_t n_source, const double *source_values,
+                                                const double *target_points, int64_t n_target,
+                                                double *target_values,
+                                                const pacman_b200_options *opts);
 
 /*
  * Target sharding of one transfer over `world` GPUs, one process per GPU

@@ -55,6 +55,15 @@ PACMAN_SHIM_API int pacman_fe_interpolate_c(int spaceDimension, int execSpace, i
                                             int nTargetPoints, double *targetValues,
                                             int *targetStatus);
 
+/* src/fortran_interface.h:175-179: PACMAN::MLS_interpolate with plain C
+ * types; targetValues is caller-allocated, nTargetPoints entries.
+ * 0 on success, -1 on a std::exception, -2 otherwise. */
+PACMAN_SHIM_API int pacman_mls_interpolate_c(int spaceDimension, int execSpace,
+                                             const double *sourcePoints, int nSourcePoints,
+                                             const double *sourceValues,
+                                             const double *targetPoints, int nTargetPoints,
+                                             double *targetValues);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,4 +87,21 @@ __attribute__((visibility("default"))) FeInterpolateResult fe_interpolate(
     offset_t *connOff, int_t connOffSize, cell_t *cellTypes, coordinates_t *targetPoints,
     int_t nTargetPoints, bool fortranIndexing = false);
 
+// src/interface.hpp:143-146.
+struct MLSInterpolateResult {
+  std::vector<fp_t> targetValues;  ///< Interpolated scalar value per target point.
+};
+
+/// Moving least squares interpolation (src/interface.hpp:166-170): the
+/// K = 3, 6, 10 (1D, 2D, 3D) nearest sources of each target, Wendland C0
+/// weights, a weighted quadratic least-squares fit evaluated at the target
+/// (ArborX's MovingLeastSquares defaults, which the reference calls).
+/// @throws std::invalid_argument on null pointers with non-zero counts.
+/// @throws std::runtime_error if spaceDimension is not 1, 2 or 3, or on a
+///         device error.
+__attribute__((visibility("default"))) MLSInterpolateResult MLS_interpolate(
+    int_t spaceDimension, unsigned char execSpace, coordinates_t *sourcePoints,
+    int_t nSourcePoints, fp_t *sourceValues, coordinates_t *targetPoints,
+    int_t nTargetPoints);
+
 }  // namespace PACMAN

@@ -10,6 +10,7 @@ from .oracle import (  # noqa: F401
     ensure_built,
     fe_nearest,
     interpolate,
+    mls_interpolate,
     set_threads,
     wendland,
 )

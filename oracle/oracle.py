@@ -65,6 +65,9 @@ def _load():
         lib.orc_fe_nearest.argtypes = [ctypes.c_int, _f64p, ctypes.c_int64, _f64p, _f64p,
                                        ctypes.c_int64, _f64p, _i32p]
         lib.orc_fe_nearest.restype = ctypes.c_int
+        lib.orc_mls_interpolate.argtypes = [ctypes.c_int, _f64p, ctypes.c_int64, _f64p, _f64p,
+                                            ctypes.c_int64, _f64p, _i32p]
+        lib.orc_mls_interpolate.restype = ctypes.c_int
         _lib = lib
         return lib
 
@@ -208,3 +211,22 @@ def fe_nearest(dim, src, values, tgt):
     if rc != 0:
         raise RuntimeError(f"oracle fe_nearest failed ({rc}): {lib.orc_last_error().decode()}")
     return out, idx[: tgt.shape[0]]
+
+
+def mls_interpolate(dim, src, values, tgt, with_sweeps=False):
+    """Moving least squares transfer (src/mls/interpolator.hpp:49-77 over
+    ArborX's MovingLeastSquares defaults): values at the targets, and with
+    ``with_sweeps`` the Jacobi sweep count of each target."""
+    lib = _load()
+    src = np.ascontiguousarray(src, dtype=np.float64).reshape(-1, dim)
+    tgt = np.ascontiguousarray(tgt, dtype=np.float64).reshape(-1, dim)
+    vals = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+    out = np.zeros(tgt.shape[0], dtype=np.float64)
+    sw = np.zeros(max(tgt.shape[0], 1), dtype=np.int32)
+    rc = lib.orc_mls_interpolate(int(dim), _ptr(src) if src.size else None, src.shape[0],
+                                 _ptr(vals) if vals.size else None,
+                                 _ptr(tgt) if tgt.size else None, tgt.shape[0],
+                                 _ptr(out) if out.size else None, _ptr(sw, _i32p))
+    if rc != 0:
+        raise RuntimeError(f"oracle mls_interpolate failed ({rc}): {lib.orc_last_error().decode()}")
+    return (out, sw[: tgt.shape[0]]) if with_sweeps else out

@@ -1038,3 +1038,199 @@ int orc_fe_nearest(int dim, const double *src, int64_t n, const double *vals,
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Moving least squares (src/mls/interpolator.hpp:49-77, src/mls_interface.cpp):
+ * the reference constructs ArborX 2.1's Interpolation::MovingLeastSquares
+ * (un-vendored dependency) with its defaults and interpolates one scalar
+ * field.  Restated from that published algorithm:
+ *  - neighbours: the K nearest sources of each target, K = the size of the
+ *    quadratic polynomial basis (3, 6, 10 in 1D, 2D, 3D); fewer when there
+ *    are fewer sources.  Order and ties: ascending (squared distance, source
+ *    index), squared distances formed as sqdist() above;
+ *  - radius: 1.1 x the largest neighbour distance (at least 10 x DBL_EPSILON),
+ *    so that the farthest neighbour keeps a non-zero weight;
+ *  - weights: Wendland C0 of rho = distance / radius, (1 - rho)^2;
+ *  - basis: the monomials of degree <= 2 of x = (source - target) / radius
+ *    (1D: 1, x, x^2; 2D: 1, x, y, x^2, xy, y^2; 3D: 1, x, y, z, x^2, xy, xz,
+ *    y^2, yz, z^2), so that the value at the target is the constant
+ *    coefficient.  ArborX uses source - target unscaled; the division by the
+ *    radius changes no value where A is invertible (exact arithmetic) and
+ *    takes the radius^4 spread out of A's eigenvalues, so the eigenvalue
+ *    cut-off below is relative to a well-scaled matrix;
+ *  - moment matrix A = sum_j w_j p_j p_j^T and b = sum_j w_j f_j p_j; the
+ *    value is e_0^T A^+ b with A^+ the Moore-Penrose pseudo-inverse of the
+ *    symmetric A.
+ * A^+ comes from a cyclic Jacobi eigen-decomposition A = V L V^T (Rutishauser's
+ * rotation formulas) whose rotations are applied to u = V^T e_0 and
+ * v = V^T b; eigenvalues |l_k| <= 1e-13 max |l| count as zero, and the value
+ * is sum_k u_k v_k / l_k over the others.  ArborX's eigenvalue cut-off and
+ * tie order are not reproducible here (parity with ArborX is unpinned; the
+ * reference's own MLS tests are the pins).  In exact arithmetic the value
+ * equals ArborX's whenever A is invertible, and whenever A's null space is
+ * orthogonal to e_0 (sources on a line or plane through the target); with
+ * fewer sources than basis functions, or a degenerate neighbour set that
+ * misses the target, the two pseudo-inverse fits differ by the basis scaling.  Targets keep 0 without sources
+ * (SetupTransferClass zero-fills, common/transfer.hxx:100-110).
+ * No fused multiply-add outside sqdist(): every product and sum below is
+ * rounded on its own, and the CUDA kernel is compiled the same way.
+ * ---------------------------------------------------------------------- */
+#define MLS_KMAX 10
+#define MLS_SWEEPS 64
+
+int orc_mls_basis_size(int dim) { return dim == 1 ? 3 : (dim == 2 ? 6 : 10); }
+
+static void mls_basis(int dim, const double *x, double *p) {
+  p[0] = 1.0;
+  if (dim == 1) {
+    p[1] = x[0];
+    p[2] = x[0] * x[0];
+  } else if (dim == 2) {
+    p[1] = x[0]; p[2] = x[1];
+    p[3] = x[0] * x[0]; p[4] = x[0] * x[1]; p[5] = x[1] * x[1];
+  } else {
+    p[1] = x[0]; p[2] = x[1]; p[3] = x[2];
+    p[4] = x[0] * x[0]; p[5] = x[0] * x[1]; p[6] = x[0] * x[2];
+    p[7] = x[1] * x[1]; p[8] = x[1] * x[2]; p[9] = x[2] * x[2];
+  }
+}
+
+/* One Jacobi rotation annihilating a[p][q] (p < q) of the symmetric M x M
+ * matrix a (both triangles kept), applied to the vectors u and v as well. */
+static void mls_rotate(int M, double a[MLS_KMAX][MLS_KMAX], double *u, double *v, int p, int q) {
+  const double apq = a[p][q];
+  if (apq == 0.0) return;
+  const double app = a[p][p], aqq = a[q][q];
+  const double g = 100.0 * fabs(apq);
+  if (fabs(app) + g == fabs(app) && fabs(aqq) + g == fabs(aqq)) {
+    a[p][q] = a[q][p] = 0.0;  /* below the rounding of both diagonal entries */
+    return;
+  }
+  const double h = aqq - app;
+  double t;
+  if (fabs(h) + g == fabs(h)) {
+    t = apq / h;
+  } else {
+    const double theta = 0.5 * h / apq;
+    t = 1.0 / (fabs(theta) + sqrt(1.0 + theta * theta));
+    if (theta < 0.0) t = -t;
+  }
+  const double c = 1.0 / sqrt(1.0 + t * t);
+  const double s = t * c;
+  const double tau = s / (1.0 + c);
+  a[p][p] = app - t * apq;
+  a[q][q] = aqq + t * apq;
+  a[p][q] = a[q][p] = 0.0;
+  for (int r = 0; r < M; ++r) {
+    if (r == p || r == q) continue;
+    const double arp = a[r][p], arq = a[r][q];
+    const double np_ = arp - s * (arq + tau * arp);
+    const double nq_ = arq + s * (arp - tau * arq);
+    a[r][p] = a[p][r] = np_;
+    a[r][q] = a[q][r] = nq_;
+  }
+  const double up = u[p], uq = u[q];
+  u[p] = up - s * (uq + tau * up);
+  u[q] = uq + s * (up - tau * uq);
+  const double vp = v[p], vq = v[q];
+  v[p] = vp - s * (vq + tau * vp);
+  v[q] = vq + s * (vp - tau * vq);
+}
+
+/* e_0^T A^+ b for the symmetric M x M moment matrix a (destroyed). */
+static double mls_pinv_value(int M, double a[MLS_KMAX][MLS_KMAX], const double *b, int *sweeps) {
+  double u[MLS_KMAX], v[MLS_KMAX];
+  for (int i = 0; i < M; ++i) {
+    u[i] = i == 0 ? 1.0 : 0.0;
+    v[i] = b[i];
+  }
+  int sw = 0;
+  for (; sw < MLS_SWEEPS; ++sw) {
+    int off = 0;
+    for (int p = 0; p < M; ++p)
+      for (int q = p + 1; q < M; ++q) off |= a[p][q] != 0.0;
+    if (!off) break;
+    for (int p = 0; p < M; ++p)
+      for (int q = p + 1; q < M; ++q) mls_rotate(M, a, u, v, p, q);
+  }
+  if (sweeps) *sweeps = sw;
+  double lmax = 0.0;
+  for (int k = 0; k < M; ++k) lmax = fmax(lmax, fabs(a[k][k]));
+  const double cut = 1e-13 * lmax;
+  double val = 0.0;
+  for (int k = 0; k < M; ++k)
+    if (fabs(a[k][k]) > cut) val = val + (u[k] * v[k]) / a[k][k];
+  return val;
+}
+
+int orc_mls_interpolate(int dim, const double *src, int64_t n, const double *vals,
+                        const double *tgt, int64_t m, double *out, int32_t *sweeps_out) {
+  if (dim < 1 || dim > 3) {
+    set_err("dimension must be 1, 2 or 3");
+    return -2;
+  }
+  const int K = orc_mls_basis_size(dim);
+  const int kk = n < K ? (int)n : K;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t t = 0; t < m; ++t) {
+    double y[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < dim; ++d) y[d] = tgt[t * dim + d];
+    double bd[MLS_KMAX];
+    int64_t bi[MLS_KMAX];
+    int cnt = 0;
+    /* Ascending source index: an equal distance never displaces a kept one. */
+    for (int64_t i = 0; i < n; ++i) {
+      double x[3] = {0.0, 0.0, 0.0};
+      for (int d = 0; d < dim; ++d) x[d] = src[i * dim + d];
+      const double tx = x[0] - y[0], ty = x[1] - y[1], tz = x[2] - y[2];
+      double acc = tx * tx;
+      acc = fma(ty, ty, acc);
+      acc = fma(tz, tz, acc);
+      if (cnt == kk && !(acc < bd[kk - 1])) continue;
+      int pos = cnt < kk ? cnt++ : kk - 1;
+      while (pos > 0 && acc < bd[pos - 1]) {
+        bd[pos] = bd[pos - 1];
+        bi[pos] = bi[pos - 1];
+        --pos;
+      }
+      bd[pos] = acc;
+      bi[pos] = i;
+    }
+    if (kk == 0) {
+      out[t] = 0.0;
+      if (sweeps_out) sweeps_out[t] = 0;
+      continue;
+    }
+    double dist[MLS_KMAX];
+    double rmax = 10.0 * DBL_EPSILON;
+    for (int j = 0; j < kk; ++j) {
+      dist[j] = sqrt(bd[j]);
+      rmax = fmax(rmax, dist[j]);
+    }
+    const double radius = 1.1 * rmax;
+    double a[MLS_KMAX][MLS_KMAX], b[MLS_KMAX];
+    for (int i = 0; i < K; ++i) {
+      b[i] = 0.0;
+      for (int k = 0; k < K; ++k) a[i][k] = 0.0;
+    }
+    for (int j = 0; j < kk; ++j) {
+      double x[3] = {0.0, 0.0, 0.0}, p[MLS_KMAX];
+      for (int d = 0; d < dim; ++d) x[d] = (src[bi[j] * dim + d] - y[d]) / radius;
+      mls_basis(dim, x, p);
+      const double rho = dist[j] / radius;
+      const double w = (1.0 - rho) * (1.0 - rho);
+      const double wf = w * vals[bi[j]];
+      for (int r = 0; r < K; ++r) {
+        const double wr = w * p[r];
+        for (int c = r; c < K; ++c) a[r][c] = a[r][c] + wr * p[c];
+        b[r] = b[r] + wf * p[r];
+      }
+    }
+    for (int r = 0; r < K; ++r)
+      for (int c = 0; c < r; ++c) a[r][c] = a[c][r];
+    int sw = 0;
+    out[t] = mls_pinv_value(K, a, b, &sw);
+    if (sweeps_out) sweeps_out[t] = sw;
+  }
+  return 0;
+}

@@ -87,6 +87,14 @@ const char *orc_last_error(void);
 int orc_fe_nearest(int dim, const double *src, int64_t n, const double *vals,
                    const double *tgt, int64_t m, double *out, int32_t *nearest);
 
+/* Moving least squares (ArborX MovingLeastSquares defaults: quadratic basis,
+ * Wendland C0 weights, K = basis-size nearest sources): out[t] = value at
+ * target t, 0 without sources; sweeps (may be NULL) receives the Jacobi sweep
+ * count per target. */
+int orc_mls_basis_size(int dim);
+int orc_mls_interpolate(int dim, const double *src, int64_t n, const double *vals,
+                        const double *tgt, int64_t m, double *out, int32_t *sweeps);
+
 #ifdef __cplusplus
 }
 #endif

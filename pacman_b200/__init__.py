@@ -5,10 +5,12 @@ reference's arguments (src/pybindings/bindings.cpp:38-93).  The computation
 runs in hand-written sm_100a CUDA kernels behind the C ABI of
 ``include/pacman_b200.h``; there is no CPU fallback.
 """
-from . import distributed, execspaces, fe, rbf  # noqa: F401
+from . import distributed, execspaces, fe, mls, rbf  # noqa: F401
+from . import mls as MLS  # noqa: F401  (the reference's submodule name)
 from ._lib import load as _load_library
 
-__all__ = ["distributed", "execspaces", "fe", "rbf", "initialize", "finalize", "library_path"]
+__all__ = ["MLS", "distributed", "execspaces", "fe", "mls", "rbf", "initialize", "finalize",
+           "library_path"]
 
 
 def initialize():

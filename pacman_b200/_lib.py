@@ -121,6 +121,9 @@ SIGNATURES = {
     "pacman_b200_fe_interpolate": (ctypes.c_int, [
         ctypes.c_int32, ctypes.c_int32, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_int64, _VP, _VP,
         ctypes.POINTER(Options)]),
+    "pacman_b200_mls_interpolate": (ctypes.c_int, [
+        ctypes.c_int32, _VP, ctypes.c_int64, _VP, _VP, ctypes.c_int64, _VP,
+        ctypes.POINTER(Options)]),
     "pacman_b200_plan_owned_targets": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), _VP]),
     "pacman_b200_patch_radius_noalloc": (ctypes.c_int, [
         ctypes.c_int32, _VP, ctypes.c_int64, ctypes.c_int32, _VP, _VP]),

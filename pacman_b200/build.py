@@ -25,6 +25,9 @@ NVCC_FLAGS = ARCH + [
     f"-I{os.path.join(ROOT, 'include')}",
 ]
 
+# mls.cu rounds every product and sum on its own, as the CPU restatement does.
+FILE_FLAGS = {"mls.cu": ["-fmad=false"]}
+
 
 def _nvcc() -> str:
     cand = [os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")]
@@ -51,6 +54,7 @@ def _compile(src: str, extra: list[str], verbose: bool) -> str:
     newest = max([os.path.getmtime(path)] + [os.path.getmtime(h) for h in _headers()])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj
+    extra = extra + FILE_FLAGS.get(src, [])
     cmd = [_nvcc()] + NVCC_FLAGS + extra + ["-c", path, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [_nvcc()] + NVCC_FLAGS + extra + ["-x", "c++", "-c", path, "-o", obj]

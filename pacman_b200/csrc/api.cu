@@ -945,6 +945,68 @@ int pacman_b200_fe_interpolate(int32_t dim, int32_t method, const double *src, i
   return 0;
 }
 
+int pacman_b200_mls_interpolate(int32_t dim, const double *src, int64_t n, const double *vals,
+                                const double *tgt, int64_t m, double *out,
+                                const pacman_b200_options *opts) {
+  g_last_error.clear();
+  if (src == nullptr && n > 0)
+    return fail(PACMAN_B200_ERR_INVALID, "sourcePoints is null but nSourcePoints > 0");
+  if (tgt == nullptr && m > 0)
+    return fail(PACMAN_B200_ERR_INVALID, "targetPoints is null but nTargetPoints > 0");
+  if (vals == nullptr && n > 0)
+    return fail(PACMAN_B200_ERR_INVALID, "sourceValues is null but nSourcePoints > 0");
+  if (dim < 1 || dim > 3)
+    return fail(PACMAN_B200_ERR_DIMENSION, "The dimension of the points can only be: 1, 2 or 3.");
+  if (n < 0 || m < 0) return fail(PACMAN_B200_ERR_INVALID, "negative point count");
+  if (n > 0x7fffffffll || m > 0x7fffffffll)
+    return fail(PACMAN_B200_ERR_LIMIT, "point counts are limited to 2^31 - 1");
+  if (out == nullptr && m > 0) return fail(PACMAN_B200_ERR_INVALID, "target_values is null");
+  pacman_b200_options o;
+  pacman_b200_options_init(&o);
+  if (opts) o = *opts;
+  if (m == 0) return 0;
+  cudaStream_t own = nullptr;
+  try {
+    DeviceScope ds(o.device);
+    tune_pool(ds.dev);
+    HostArena::get().reset();
+    cudaStream_t st = static_cast<cudaStream_t>(o.stream);
+    if (!st) {
+      PB_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+      st = own;
+    }
+    {
+      InBuf s, v, t;
+      s.stage(src, size_t(n) * dim, ds.dev, st);
+      v.stage(vals, size_t(n), ds.dev, st);
+      t.stage(tgt, size_t(m) * dim, ds.dev, st);
+      const bool out_dev = is_device_ptr(out, ds.dev);
+      DevMem obuf;
+      double *o_dev = out;
+      if (!out_dev) {
+        obuf.alloc(sizeof(double) * size_t(m), st);
+        o_dev = obuf.as<double>();
+      }
+      mls_interpolate(dim, s.ptr, n, v.ptr, t.ptr, m, o_dev, st);
+      if (!out_dev)
+        PB_CUDA(cudaMemcpyAsync(out, o_dev, sizeof(double) * size_t(m), cudaMemcpyDeviceToHost,
+                                st));
+      PB_CUDA(host_sync(st));
+    }
+    if (own) {
+      cudaStreamDestroy(own);
+      own = nullptr;
+    }
+  } catch (const Error &e) {
+    if (own) {
+      cudaStreamSynchronize(own);
+      cudaStreamDestroy(own);
+    }
+    return fail(e.code, e.msg);
+  }
+  return 0;
+}
+
 int pacman_b200_plan_shard(pacman_b200_plan *plan, int32_t rank, int32_t world) {
   if (!plan) return fail(PACMAN_B200_ERR_INVALID, "plan is null");
   try {

@@ -82,4 +82,28 @@ int pacman_fe_interpolate_c(int spaceDimension, int execSpace, int method,
   }
 }
 
+int pacman_mls_interpolate_c(int spaceDimension, int execSpace, const double *sourcePoints,
+                             int nSourcePoints, const double *sourceValues,
+                             const double *targetPoints, int nTargetPoints,
+                             double *targetValues) {
+  try {
+    if (targetValues == nullptr && nTargetPoints > 0)
+      throw std::invalid_argument("targetValues is null but nTargetPoints > 0");
+    PACMAN::MLSInterpolateResult r = PACMAN::MLS_interpolate(
+        static_cast<PACMAN::int_t>(spaceDimension), static_cast<unsigned char>(execSpace),
+        const_cast<PACMAN::coordinates_t *>(sourcePoints),
+        static_cast<PACMAN::int_t>(nSourcePoints), const_cast<PACMAN::fp_t *>(sourceValues),
+        const_cast<PACMAN::coordinates_t *>(targetPoints),
+        static_cast<PACMAN::int_t>(nTargetPoints));
+    for (int i = 0; i < nTargetPoints; ++i) targetValues[i] = r.targetValues[std::size_t(i)];
+    return 0;
+  } catch (const std::exception &e) {
+    std::cerr << "pacman_mls_interpolate_c: " << e.what() << "\n";
+    return -1;
+  } catch (...) {
+    std::cerr << "pacman_mls_interpolate_c: unknown exception\n";
+    return -2;
+  }
+}
+
 }  // extern "C"

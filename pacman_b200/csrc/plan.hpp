@@ -247,6 +247,9 @@ void build_point_grid(DevGrid &out, const double4 *pts, int64_t n, int dim, cons
 // Finite-element NEAREST_NEAREST transfer (nearest.cu).
 void fe_nearest(int dim, const double *src_dev, int64_t n, const double *vals_dev,
                 const double *tgt_dev, int64_t m, double *out_dev, cudaStream_t st);
+// Moving least squares transfer (mls.cu).
+void mls_interpolate(int dim, const double *src_dev, int64_t n, const double *vals_dev,
+                     const double *tgt_dev, int64_t m, double *out_dev, cudaStream_t st);
 // Restricts the plan to target shard `rank` of `world` (shard.cu).
 void shard_plan(Plan &p, int rank, int world);
 

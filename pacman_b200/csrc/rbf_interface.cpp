@@ -78,4 +78,32 @@ FeInterpolateResult fe_interpolate(int_t spaceDimension, unsigned char execSpace
   return result;
 }
 
+// PACMAN::MLS_interpolate (src/mls_interface.cpp): the reference's null and
+// dimension checks, then the moving least squares transfer.
+MLSInterpolateResult MLS_interpolate(int_t spaceDimension, unsigned char execSpace,
+                                     coordinates_t *sourcePoints, int_t nSourcePoints,
+                                     fp_t *sourceValues, coordinates_t *targetPoints,
+                                     int_t nTargetPoints) {
+  if (sourcePoints == nullptr && nSourcePoints > 0)
+    throw std::invalid_argument("sourcePoints is null but nSourcePoints > 0");
+  if (targetPoints == nullptr && nTargetPoints > 0)
+    throw std::invalid_argument("targetPoints is null but nTargetPoints > 0");
+  if (sourceValues == nullptr && nSourcePoints > 0)
+    throw std::invalid_argument("sourceValues is null but nSourcePoints > 0");
+  if (spaceDimension < 1 || spaceDimension > 3)
+    throw std::runtime_error("The dimension of the points can only be: 1, 2 or 3.\n");
+  if (execSpace > ExecSpaces::SYCL)
+    throw std::invalid_argument("execspace: Serial, OpenMP, Threads, Cuda, HIP, SYCL");
+  MLSInterpolateResult result;
+  const size_t m = nTargetPoints > 0 ? size_t(nTargetPoints) : 0;
+  result.targetValues.assign(m, 0.0);
+  if (m == 0) return result;
+  const int rc = pacman_b200_mls_interpolate(
+      spaceDimension, sourcePoints, nSourcePoints > 0 ? nSourcePoints : 0, sourceValues,
+      targetPoints, int64_t(m), result.targetValues.data(), nullptr);
+  if (rc == PACMAN_B200_ERR_INVALID) throw std::invalid_argument(pacman_b200_last_error());
+  if (rc != 0) throw std::runtime_error(pacman_b200_last_error());
+  return result;
+}
+
 }  // namespace PACMAN

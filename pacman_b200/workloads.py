@@ -34,6 +34,30 @@ def franke_3d(p: np.ndarray) -> np.ndarray:
             - 0.2 * np.exp(-((9 * x - 4) ** 2 + (9 * y - 7) ** 2 + (9 * z - 5) ** 2)))
 
 
+def franke_2d(p: np.ndarray) -> np.ndarray:
+    """Franke's 2D test function (tests/franke_functions.py:71-116 of the reference)."""
+    x, y = p[:, 0], p[:, 1]
+    return (0.75 * np.exp(-((9 * x - 2) ** 2 + (9 * y - 2) ** 2) / 4.0)
+            + 0.75 * np.exp(-((9 * x + 1) ** 2 / 49.0 + (9 * y + 1) / 10.0))
+            + 0.5 * np.exp(-((9 * x - 7) ** 2 + (9 * y - 3) ** 2) / 4.0)
+            - 0.2 * np.exp(-((9 * x - 4) ** 2 + (9 * y - 7) ** 2)))
+
+
+def franke_1d(p: np.ndarray) -> np.ndarray:
+    """The reference's 1D Franke function (tests/franke_functions.py:29-69, the
+    later of its two definitions, which is the one Python keeps)."""
+    x = p[:, 0]
+    return (0.75 * np.exp(-((9 * x - 2) ** 2) / 4.0)
+            + 0.75 * np.exp(-((9 * x + 1) ** 2) / 49.0)
+            + 0.5 * np.exp(-((9 * x - 7) ** 2) / 4.0)
+            - 0.2 * np.exp(-((9 * x - 4) ** 2)))
+
+
+def franke(p: np.ndarray) -> np.ndarray:
+    """franke_1d, franke_2d or franke_3d by the points' dimension."""
+    return {1: franke_1d, 2: franke_2d, 3: franke_3d}[p.shape[1]](p)
+
+
 def fourier_fields(p: np.ndarray, nfields: int, seed: int, modes: int = 16, kmax: int = 4) -> np.ndarray:
     """nfields random Fourier series sum_j a_j cos(2 pi k_j.x) + b_j sin(2 pi k_j.x),
     a, b ~ N(0,1), integer wavenumbers with |k|_inf <= kmax."""

@@ -24,7 +24,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for name in names:
         assert hasattr(lib, name), name
     assert set(names) == set(_lib.SIGNATURES)
-    assert _lib.load().pacman_b200_abi_version() == 5
+    assert _lib.load().pacman_b200_abi_version() == 6
 
 
 def test_cpp_dropin_symbol_exported():

@@ -1,10 +1,10 @@
 """The C entry points of the reference's Fortran module
 (src/fortran_interface.h:69-151) exported by libpacman_b200.so.
 
-The Fortran module calls pacman_rbf_interpolate_c / pacman_fe_interpolate_c
-through ISO_C_BINDING and reads their integer return code: 0, or -1 when the
-C++ call threw a std::exception, -2 for anything else
-(src/fortran_interface.cpp:84-90).  gfortran is not in this image, so these
+The Fortran module calls pacman_rbf_interpolate_c, pacman_fe_interpolate_c
+and pacman_mls_interpolate_c through ISO_C_BINDING and reads their integer
+return code: 0, or -1 when the C++ call threw a std::exception, -2 for
+anything else (src/fortran_interface.cpp:84-90).  gfortran is not in this image, so these
 tests bind the same C signatures through ctypes, which is what the module's
 interface blocks do.  The GPU cases repeat the reference's Fortran known-answer
 test (tests/test_fortran_rbf_interface.f90: 20^3 grid onto itself, rel-L2 <
@@ -33,6 +33,9 @@ def _shim():
     lib.pacman_fe_interpolate_c.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D,
                                             ctypes.c_int, _D, _I, ctypes.c_int, _I, ctypes.c_int,
                                             _I, _D, ctypes.c_int, _D, _I]
+    lib.pacman_mls_interpolate_c.restype = ctypes.c_int
+    lib.pacman_mls_interpolate_c.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D,
+                                             _D, ctypes.c_int, _D]
     lib.pacman_best_execspace_c.restype = ctypes.c_int
     return lib
 
@@ -51,7 +54,7 @@ def test_shim_symbols_exported_with_c_linkage():
     names = re.findall(r"PACMAN_SHIM_API\s+[\w\s\*]*?\b(pacman_\w+_c)\s*\(", src)
     assert set(names) == {"pacman_kokkos_initialize_c", "pacman_kokkos_finalize_c",
                           "pacman_best_execspace_c", "pacman_rbf_interpolate_c",
-                          "pacman_fe_interpolate_c"}
+                          "pacman_fe_interpolate_c", "pacman_mls_interpolate_c"}
     out = os.popen(f"nm -D --defined-only {_lib.LIB_PATH}").read()
     for n in names:
         assert re.search(r"\bT " + n + r"$", out, re.M), n  # unmangled: extern "C"
@@ -86,6 +89,13 @@ def test_shim_maps_exceptions_to_minus_one(capfd):
     rc = lib.pacman_fe_interpolate_c(3, 3, 0xF1, _dp(p), 4, _dp(v), None, 0, None, 0, None,
                                      _dp(p), 4, _dp(out), st.ctypes.data_as(_I))
     assert rc == -1 and "NEAREST_NEAREST" in capfd.readouterr().err
+    # MLS (src/fortran_interface.cpp:138-164): the same -1 mapping.
+    assert lib.pacman_mls_interpolate_c(4, 3, _dp(p), 4, _dp(v), _dp(p), 4, _dp(out)) == -1
+    assert "pacman_mls_interpolate_c: The dimension" in capfd.readouterr().err
+    assert lib.pacman_mls_interpolate_c(3, 3, _dp(p), 4, None, _dp(p), 4, _dp(out)) == -1
+    assert "sourceValues is null" in capfd.readouterr().err
+    assert lib.pacman_mls_interpolate_c(3, 3, _dp(p), 4, _dp(v), _dp(p), 4, None) == -1
+    assert lib.pacman_mls_interpolate_c(3, 3, _dp(p), 4, _dp(v), _dp(p), 0, None) == 0
 
 
 @pytest.mark.gpu
@@ -133,3 +143,16 @@ def test_shim_fe_nearest_nearest():
     assert rc == 0
     assert np.array_equal(out, oracle.fe_nearest(3, sp, sv, tp)[0])
     assert (st == 0).all()
+
+
+@pytest.mark.gpu
+def test_shim_mls_matches_oracle():
+    rng = np.random.default_rng(7)
+    sp = rng.random((3000, 3))
+    tp = rng.random((2000, 3))
+    sv = np.cos(4 * sp[:, 0]) * sp[:, 1]
+    out = np.zeros(len(tp))
+    rc = _shim().pacman_mls_interpolate_c(3, 3, _dp(sp), len(sp), _dp(sv), _dp(tp), len(tp),
+                                          _dp(out))
+    assert rc == 0
+    assert np.array_equal(out, oracle.mls_interpolate(3, sp, sv, tp))
