@@ -495,6 +495,19 @@ def measure_mls(pacman, S, V0, T, timed, steps):
                     "10 x 10 moment matrix)"}
 
 
+def mls_cpu_baseline(w):
+    """The CPU restatement of the moving least squares transfer (cell-grid
+    neighbour search, the same fit per target) over the whole workload with
+    every host thread."""
+    import oracle
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    oracle.mls_interpolate(3, w["src"], w["values"][:, 0], w["tgt"])
+    sec = time.perf_counter() - t0
+    return {"value": w["tgt"].shape[0] / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the whole transfer, {sec:.2f} s"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -766,6 +779,8 @@ def main():
         v1, desc1, _, _, _ = cpu_baseline(w, args.cpu_seconds / 2, threads=1)
         line["cpu_baseline_serial"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
                                        "sample": desc1}
+        if "mls" in line:
+            line["mls"]["cpu_baseline"] = mls_cpu_baseline(w)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -66,7 +66,7 @@ def _load():
                                        ctypes.c_int64, _f64p, _i32p]
         lib.orc_fe_nearest.restype = ctypes.c_int
         lib.orc_mls_interpolate.argtypes = [ctypes.c_int, _f64p, ctypes.c_int64, _f64p, _f64p,
-                                            ctypes.c_int64, _f64p, _i32p]
+                                            ctypes.c_int64, _f64p, _i32p, ctypes.c_int]
         lib.orc_mls_interpolate.restype = ctypes.c_int
         _lib = lib
         return lib
@@ -213,10 +213,12 @@ def fe_nearest(dim, src, values, tgt):
     return out, idx[: tgt.shape[0]]
 
 
-def mls_interpolate(dim, src, values, tgt, with_sweeps=False):
+def mls_interpolate(dim, src, values, tgt, with_sweeps=False, knn="auto"):
     """Moving least squares transfer (src/mls/interpolator.hpp:49-77 over
     ArborX's MovingLeastSquares defaults): values at the targets, and with
-    ``with_sweeps`` the Jacobi sweep count of each target."""
+    ``with_sweeps`` the Jacobi sweep count of each target.  ``knn``: "brute"
+    (every source per target), "grid" (a cell grid) or "auto" (the grid from
+    4,096 sources on); the neighbours, and so the values, are the same."""
     lib = _load()
     src = np.ascontiguousarray(src, dtype=np.float64).reshape(-1, dim)
     tgt = np.ascontiguousarray(tgt, dtype=np.float64).reshape(-1, dim)
@@ -226,7 +228,8 @@ def mls_interpolate(dim, src, values, tgt, with_sweeps=False):
     rc = lib.orc_mls_interpolate(int(dim), _ptr(src) if src.size else None, src.shape[0],
                                  _ptr(vals) if vals.size else None,
                                  _ptr(tgt) if tgt.size else None, tgt.shape[0],
-                                 _ptr(out) if out.size else None, _ptr(sw, _i32p))
+                                 _ptr(out) if out.size else None, _ptr(sw, _i32p),
+                                 {"auto": 0, "brute": 1, "grid": 2}[knn])
     if rc != 0:
         raise RuntimeError(f"oracle mls_interpolate failed ({rc}): {lib.orc_last_error().decode()}")
     return (out, sw[: tgt.shape[0]]) if with_sweeps else out

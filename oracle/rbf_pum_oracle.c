@@ -1163,38 +1163,164 @@ static double mls_pinv_value(int M, double a[MLS_KMAX][MLS_KMAX], const double *
   return val;
 }
 
+static inline double mls_sqdist(int dim, const double *src, int64_t i, const double *y) {
+  double x[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < dim; ++d) x[d] = src[i * dim + d];
+  const double tx = x[0] - y[0], ty = x[1] - y[1], tz = x[2] - y[2];
+  double acc = tx * tx;
+  acc = fma(ty, ty, acc);
+  acc = fma(tz, tz, acc);
+  return acc;
+}
+
+/* Keeps the kk smallest (squared distance, index) pairs, sorted. */
+static inline void mls_keep(double acc, int64_t i, int kk, double *bd, int64_t *bi, int *cnt) {
+  if (*cnt == kk && !(acc < bd[kk - 1] || (acc == bd[kk - 1] && i < bi[kk - 1]))) return;
+  int pos = *cnt < kk ? (*cnt)++ : kk - 1;
+  while (pos > 0 && (acc < bd[pos - 1] || (acc == bd[pos - 1] && i < bi[pos - 1]))) {
+    bd[pos] = bd[pos - 1];
+    bi[pos] = bi[pos - 1];
+    --pos;
+  }
+  bd[pos] = acc;
+  bi[pos] = i;
+}
+
+/* Source cell grid of the neighbour search: about two sources per cell over
+ * the sources' bounding box. */
+typedef struct {
+  int dim;
+  double lo[3], inv_h, h;
+  int64_t nc[3];
+  int64_t *start;
+  int64_t *items;
+} mls_grid_t;
+
+static int64_t mls_cell(const mls_grid_t *g, int d, double x) {
+  const double f = floor((x - g->lo[d]) * g->inv_h);
+  if (!(f >= 0.0)) return 0;
+  if (f > (double)(g->nc[d] - 1)) return g->nc[d] - 1;
+  return (int64_t)f;
+}
+
+static int mls_grid_build(mls_grid_t *g, int dim, const double *src, int64_t n) {
+  memset(g, 0, sizeof(*g));
+  g->dim = dim;
+  double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {0.0, 0.0, 0.0}, ext = 0.0;
+  for (int d = 0; d < dim; ++d) {
+    lo[d] = INFINITY;
+    hi[d] = -INFINITY;
+    for (int64_t i = 0; i < n; ++i) {
+      lo[d] = fmin(lo[d], src[i * dim + d]);
+      hi[d] = fmax(hi[d], src[i * dim + d]);
+    }
+    ext = fmax(ext, hi[d] - lo[d]);
+  }
+  const double per_axis = ceil(pow(fmax((double)n / 2.0, 1.0), 1.0 / dim));
+  g->h = ext > 0.0 ? ext / per_axis : 1.0;
+  g->inv_h = 1.0 / g->h;
+  int64_t cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    g->lo[d] = lo[d];
+    g->nc[d] = d < dim ? (int64_t)floor((hi[d] - lo[d]) * g->inv_h) + 1 : 1;
+    if (g->nc[d] < 1 || g->nc[d] > (1 << 21)) {
+      set_err("mls: could not size the neighbour grid");
+      return -3;
+    }
+    cells *= g->nc[d];
+  }
+  g->start = (int64_t *)calloc((size_t)cells + 1, sizeof(int64_t));
+  g->items = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+  int64_t *cell = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+  if (!g->start || !g->items || !cell) {
+    free(cell);
+    set_err("mls: out of memory");
+    return -4;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c = 0;
+    for (int d = 0; d < 3; ++d)
+      c = c * g->nc[d] + (d < dim ? mls_cell(g, d, src[i * dim + d]) : 0);
+    cell[i] = c;
+    g->start[c + 1]++;
+  }
+  for (int64_t c = 0; c < cells; ++c) g->start[c + 1] += g->start[c];
+  for (int64_t i = 0; i < n; ++i) g->items[g->start[cell[i]]++] = i;
+  for (int64_t c = cells; c > 0; --c) g->start[c] = g->start[c - 1];
+  g->start[0] = 0;
+  free(cell);
+  return 0;
+}
+
+/* The kk nearest sources of y: shells of cells at Chebyshev cell distance
+ * R = 0, 1, ... around y's (clamped) cell.  After shell R every unscanned
+ * source lies at least R cell widths away (one less for rounding at cell
+ * borders), so the scan stops once the kk-th best squared distance is below
+ * ((R - 1) h)^2. */
+static void mls_knn_grid(const mls_grid_t *g, const double *src, const double *y, int kk,
+                         double *bd, int64_t *bi) {
+  int cnt = 0;
+  int64_t c[3], rmax = 0;
+  for (int d = 0; d < 3; ++d) {
+    c[d] = d < g->dim ? mls_cell(g, d, y[d]) : 0;
+    if (g->nc[d] > rmax) rmax = g->nc[d];
+  }
+  for (int64_t R = 0; R <= rmax; ++R) {
+    for (int64_t a = c[0] - R; a <= c[0] + R; ++a) {
+      if (a < 0 || a >= g->nc[0]) continue;
+      for (int64_t b = c[1] - R; b <= c[1] + R; ++b) {
+        if (b < 0 || b >= g->nc[1]) continue;
+        for (int64_t e = c[2] - R; e <= c[2] + R; ++e) {
+          if (e < 0 || e >= g->nc[2]) continue;
+          const int64_t da = llabs(a - c[0]), db = llabs(b - c[1]), de = llabs(e - c[2]);
+          if (da != R && db != R && de != R) continue;  /* inside: scanned before */
+          const int64_t cid = (a * g->nc[1] + b) * g->nc[2] + e;
+          for (int64_t s = g->start[cid]; s < g->start[cid + 1]; ++s) {
+            const int64_t i = g->items[s];
+            mls_keep(mls_sqdist(g->dim, src, i, y), i, kk, bd, bi, &cnt);
+          }
+        }
+      }
+    }
+    if (cnt == kk && R >= 1) {
+      const double lim = (double)(R - 1) * g->h;
+      if (bd[kk - 1] < lim * lim) break;
+    }
+  }
+}
+
 int orc_mls_interpolate(int dim, const double *src, int64_t n, const double *vals,
-                        const double *tgt, int64_t m, double *out, int32_t *sweeps_out) {
+                        const double *tgt, int64_t m, double *out, int32_t *sweeps_out,
+                        int knn_mode) {
   if (dim < 1 || dim > 3) {
     set_err("dimension must be 1, 2 or 3");
     return -2;
   }
   const int K = orc_mls_basis_size(dim);
   const int kk = n < K ? (int)n : K;
+  /* knn_mode: 1 brute force, 2 cell grid, 0 the grid from 4,096 sources on. */
+  const int use_grid = knn_mode == 2 || (knn_mode == 0 && n >= 4096);
+  mls_grid_t grid;
+  memset(&grid, 0, sizeof(grid));
+  if (use_grid && n > 0) {
+    const int rc = mls_grid_build(&grid, dim, src, n);
+    if (rc) {
+      free(grid.start);
+      free(grid.items);
+      return rc;
+    }
+  }
 #pragma omp parallel for schedule(dynamic, 64)
   for (int64_t t = 0; t < m; ++t) {
     double y[3] = {0.0, 0.0, 0.0};
     for (int d = 0; d < dim; ++d) y[d] = tgt[t * dim + d];
     double bd[MLS_KMAX];
     int64_t bi[MLS_KMAX];
-    int cnt = 0;
-    /* Ascending source index: an equal distance never displaces a kept one. */
-    for (int64_t i = 0; i < n; ++i) {
-      double x[3] = {0.0, 0.0, 0.0};
-      for (int d = 0; d < dim; ++d) x[d] = src[i * dim + d];
-      const double tx = x[0] - y[0], ty = x[1] - y[1], tz = x[2] - y[2];
-      double acc = tx * tx;
-      acc = fma(ty, ty, acc);
-      acc = fma(tz, tz, acc);
-      if (cnt == kk && !(acc < bd[kk - 1])) continue;
-      int pos = cnt < kk ? cnt++ : kk - 1;
-      while (pos > 0 && acc < bd[pos - 1]) {
-        bd[pos] = bd[pos - 1];
-        bi[pos] = bi[pos - 1];
-        --pos;
-      }
-      bd[pos] = acc;
-      bi[pos] = i;
+    if (use_grid && n > 0) {
+      mls_knn_grid(&grid, src, y, kk, bd, bi);
+    } else {
+      int cnt = 0;
+      for (int64_t i = 0; i < n; ++i) mls_keep(mls_sqdist(dim, src, i, y), i, kk, bd, bi, &cnt);
     }
     if (kk == 0) {
       out[t] = 0.0;
@@ -1232,5 +1358,7 @@ int orc_mls_interpolate(int dim, const double *src, int64_t n, const double *val
     out[t] = mls_pinv_value(K, a, b, &sw);
     if (sweeps_out) sweeps_out[t] = sw;
   }
+  free(grid.start);
+  free(grid.items);
   return 0;
 }

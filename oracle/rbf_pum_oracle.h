@@ -90,10 +90,12 @@ int orc_fe_nearest(int dim, const double *src, int64_t n, const double *vals,
 /* Moving least squares (ArborX MovingLeastSquares defaults: quadratic basis,
  * Wendland C0 weights, K = basis-size nearest sources): out[t] = value at
  * target t, 0 without sources; sweeps (may be NULL) receives the Jacobi sweep
- * count per target. */
+ * count per target.  knn_mode: 1 brute-force neighbours, 2 a cell grid, 0 the
+ * grid from 4,096 sources on (same neighbours either way). */
 int orc_mls_basis_size(int dim);
 int orc_mls_interpolate(int dim, const double *src, int64_t n, const double *vals,
-                        const double *tgt, int64_t m, double *out, int32_t *sweeps);
+                        const double *tgt, int64_t m, double *out, int32_t *sweeps,
+                        int knn_mode);
 
 #ifdef __cplusplus
 }

@@ -99,6 +99,36 @@ def test_quadratics_are_reproduced(dim):
     _agree(out, q(T), cond)
 
 
+def _neighbour_cases():
+    rng = np.random.default_rng(50)
+    cases = []
+    for dim in (1, 2, 3):
+        S = rng.random((6000, dim))
+        cases.append((dim, S, W.franke(S), rng.random((2000, dim))))
+    g = _grid(20, 3)
+    cases.append((3, g, W.franke(g), g))                       # exact distance ties
+    c = rng.random((8, 3))
+    S = c[rng.integers(0, 8, 20000)] + rng.normal(0.0, 0.02, size=(20000, 3))
+    T = np.concatenate([rng.random((2000, 3)), rng.random((200, 3)) * 4.0 + 2.0])
+    cases.append((3, S, S[:, 0], T))                           # clusters, far targets
+    b = rng.random((1500, 3))
+    S = np.concatenate([b, b[:700]])
+    cases.append((3, S, rng.standard_normal(len(S)), rng.random((1500, 3))))  # duplicates
+    P = np.c_[rng.random((3000, 2)), np.zeros(3000)]
+    cases.append((3, P, W.franke(P), np.c_[rng.random((1000, 2)), rng.choice([0.0, 0.05], 1000)]))
+    return cases
+
+
+def test_grid_neighbour_search_equals_brute_force():
+    """The oracle's cell-grid neighbour search (used from 4,096 sources on)
+    finds the same neighbours in the same order as the all-pairs scan, so the
+    values are identical."""
+    for dim, S, f, T in _neighbour_cases():
+        a = oracle.mls_interpolate(dim, S, f, T, knn="brute")
+        b = oracle.mls_interpolate(dim, S, f, T, knn="grid")
+        assert np.array_equal(a, b), (dim, len(S))
+
+
 def test_fewer_sources_than_the_basis_and_none():
     rng = np.random.default_rng(3)
     T = rng.random((50, 3))
