@@ -96,8 +96,8 @@ def test_torch_device_inputs_match_host_inputs():
 
 
 def test_million_points_sampled_against_the_oracle():
-    """1M uniform sources -> 1M uniform targets in 3D; the oracle (brute-force
-    neighbours) recomputes 2,000 sampled targets, which must match exactly.
+    """1M uniform sources -> 1M uniform targets in 3D; the oracle recomputes
+    2,000 sampled targets, which must match exactly.
     The fit's own error against Franke's function is ~7e-3 rel-L2 here (ten
     neighbours for ten basis functions interpolate, and some random
     neighbour sets are close to singular), so the last check is a loose
