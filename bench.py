@@ -336,7 +336,7 @@ def measured_peaks():
     except (OSError, ValueError):
         pass
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
-            "source": "fallback (earlier measurement on this pool: 6.65 TB/s copy, 1.59 PFLOP/s "
+            "source": "fallback (an earlier B200 measurement: 6.65 TB/s copy, 1.59 PFLOP/s "
                       "bf16 burst, ~1.4 sustained)"}
 
 
