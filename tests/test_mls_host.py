@@ -160,3 +160,13 @@ def test_python_dimension_and_empty_targets():
         pacman.MLS.interpolate(4, 3, np.zeros((5, 4)), np.zeros(5), np.zeros((2, 4)))
     out = pacman.MLS.interpolate(3, 3, np.zeros((5, 3)), np.zeros(5), np.zeros((0, 3)))
     assert out.shape == (0,)
+
+
+def test_kernel_is_built_without_contraction():
+    """The GPU values equal the oracle's bit for bit only while mls.cu is
+    compiled without fused multiply-adds (the oracle uses -ffp-contract=off)."""
+    from pacman_b200 import build
+    assert "-fmad=false" in build.FILE_FLAGS["mls.cu"]
+    import os
+    mk = open(os.path.join(os.path.dirname(oracle.__file__), "Makefile")).read()
+    assert "-ffp-contract=off" in mk
